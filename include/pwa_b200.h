@@ -1,0 +1,106 @@
+/* pwa_b200.h -- C ABI of the B200 likelihood library (libpwa_b200.so).
+ *
+ * The hot path replaced here is the reference's GPU likelihood boundary
+ * (RooTDalitz/kernel_calEva.h:20-27, implemented in src/kernel_calEva.cu and
+ * src/cu_DPFPropogator.cu).  The reference exposes it with C++ linkage, std::vector arguments,
+ * file-scope device buffers and abort-on-error; this ABI carries the same data (the reference's SoA
+ * planes and float parameter block, unchanged) through plain pointers, an explicit context and int
+ * status codes.  The C++ functions with the reference's exact signatures are declared in
+ * kernel_calEva_compat.h and implemented on top of this ABI.
+ *
+ * Data layout (identical to the reference, src/RooDalitzAmplitude.cxx:548-770):
+ *   events are columns, planes are rows, plane stride n_size = (n / 32 + 1) * 32 floats.
+ *   pp  : 111 planes  0 mKp, 1 m(J/psi p), 2 weight (<= -1000 marks data), 3..50 Lambda* angular
+ *         factors (Re/Im interleaved), 51..110 Lambda* d-functions
+ *   pp1 :  96 planes  Pc angular factors (Re/Im interleaved)
+ *   pp2 :  96 planes  Pc d-functions
+ *   sw  :  n_size floats, data sWeights for events [0, nda)
+ * Events [0, nda) are data, sorted into m(J/psi p) bands; [nda, n) are MC.
+ *
+ * Parameter block ("h_paraList"): the reference's float layout (cu_init_data,
+ * src/RooDalitzAmplitude.cxx:3141-3210): 6 floats per resonance, then (Re, Im) helicity couplings,
+ * spline coefficients, and 4 x 32 K-matrix floats.
+ *
+ * Threading: a context is used by one host thread at a time; distinct contexts are independent
+ * (no global device state besides read-only constant tables).
+ */
+#ifndef PWA_B200_H
+#define PWA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PWA_OK = 0,
+  PWA_E_CUDA = 1,        /* a CUDA runtime call failed (see pwa_last_cuda_error) */
+  PWA_E_ARG = 2,         /* null pointer or negative size */
+  PWA_E_LAYOUT = 3,      /* parameter block sizes inconsistent with the resonance table */
+  PWA_E_SIZE = 4,        /* a model size exceeds the compiled maximum */
+  PWA_E_UNSUPPORTED = 5, /* lineshape type or chain not built (spline, revised K-matrix, Zcs) */
+  PWA_E_PARAM = 6,       /* invalid resonance parameters (spin, K-matrix channel) */
+  PWA_E_STATE = 7,       /* no events uploaded */
+  PWA_E_NOMEM = 8        /* device allocation failed */
+};
+
+typedef struct pwa_ctx pwa_ctx;
+
+typedef struct {
+  double nll;       /* NLL_SHIFT + sumW_data ln(sumint / sumW_mc) - sum sw ln fx (+1000 guard) */
+  double sumint;    /* sum over MC of w |A|^2 (host_store_fx's return value) */
+  double sum_noint; /* same without Pc / Lambda* interference */
+  double data_term; /* sum over data of sw ln |A|^2 */
+  int64_t n_nonpos; /* events whose |A|^2 was <= 0 or not finite */
+} pwa_result;
+
+/* Context on CUDA device `device` (its own stream and buffers).  Replaces the file-scope state of
+ * kernel_calEva.cu:76-80. */
+int pwa_ctx_create(int device, pwa_ctx** out);
+int pwa_ctx_destroy(pwa_ctx* ctx);
+
+/* Copies events from host planes (reference layout) to the device (cu_malloc_h_pp,
+ * kernel_calEva.cu:1447-1457, for all planes at once).  nda_smr / nda_fine are the band arguments
+ * host_store_fx receives (IntegralMethod2 passes its first band count minus one). */
+int pwa_ctx_upload_events(pwa_ctx* ctx, const float* pp, const float* pp1, const float* pp2, const float* sw,
+                          int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr, int64_t nda_fine);
+
+/* Uses caller-owned device planes instead (the reference's d_float_pp* vectors); the context does
+ * not free them. */
+int pwa_ctx_set_device_events(pwa_ctx* ctx, const float* d_pp, const float* d_pp1, const float* d_pp2,
+                              const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
+                              int64_t nda_fine);
+
+/* One likelihood evaluation (host_store_fx, kernel_calEva.cu:1186-1363): parameter block from host
+ * memory in, result out; h_fx (optional, n doubles) receives per-event fx like the reference's
+ * store_h_fx copy.  Blocks until the result is on the host. */
+int pwa_ctx_eval_nll(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size,
+                     int NR, int NZ, int NX, float FFR, float FFB, double sum_w_mc, double sum_w_data,
+                     double nll_shift, pwa_result* out, double* h_fx);
+
+/* Per-event unsmeared |A|^2 for toy weights (host_store_amp2s, kernel_calEva.cu:1376-1419). */
+int pwa_ctx_amp2(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR,
+                 int NZ, int NX, float FFR, float FFB, double* h_amp2);
+
+/* Device time of the last pwa_ctx_eval_nll kernels in milliseconds (CUDA events). */
+double pwa_ctx_last_kernel_ms(pwa_ctx* ctx);
+
+/* Number of kernels launched by the last pwa_ctx_eval_nll. */
+int pwa_ctx_last_launches(pwa_ctx* ctx);
+
+/* Host-side diagnostic, no GPU needed: decodes the parameter block as the kernels do and evaluates
+ * each Lambda* lineshape times its Lambda_b barrier at mkp (lstar: 2*NR doubles, Re/Im) and each Pc
+ * lineshape times its barrier at mz (pc: 2*NZ doubles).  Plays the role of the reference's
+ * host_store_lineshapeLsKM diagnostic (kernel_calEva.cu:1545-1584) for the Breit-Wigner and
+ * K-matrix lineshapes. */
+int pwa_host_lineshapes(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                        int NX, float FFR, float FFB, double mkp, double mz, double* lstar, double* pc);
+
+const char* pwa_error_string(int code);
+const char* pwa_last_cuda_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PWA_B200_H */

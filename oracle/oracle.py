@@ -1,0 +1,178 @@
+"""TEST INFRASTRUCTURE ONLY -- Python bindings of the FP64 oracle (oracle/pwa_oracle.cpp) and of the
+reference's own code built for host cores (oracle/build_ref.py).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, as the
+checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+NLL_SHIFT = 10000000.0
+
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+
+
+def build(force: bool = False) -> Path:
+    src = HERE / "pwa_oracle.cpp"
+    if force or not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["g++", "-std=c++17", "-O2", "-fopenmp", "-fPIC", "-shared", str(src), "-o", str(LIB)],
+                       check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.oracle_eval_fx.restype = C.c_int
+        L.oracle_eval_fx.argtypes = [_fp, _fp, _fp, C.c_long, C.c_long, C.c_long, C.c_long, _fp, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, _dp, _dp,
+                                     C.c_int]
+        L.oracle_amp2.restype = C.c_int
+        L.oracle_amp2.argtypes = [_fp, _fp, _fp, C.c_long, C.c_long, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, C.c_float, C.c_float, _dp, C.c_int]
+        L.oracle_assemble_nll.restype = C.c_double
+        L.oracle_assemble_nll.argtypes = [_dp, _dp, _fp, C.c_long, C.c_long, C.c_double, C.c_double, C.c_double, _dp]
+        for f in ("oracle_bw_lstar", "oracle_bw_pc"):
+            getattr(L, f).argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, _dp]
+        for f in ("oracle_barrier_lb_lstar", "oracle_barrier_lb_pc"):
+            getattr(L, f).restype = C.c_double
+            getattr(L, f).argtypes = [C.c_double] * 4
+        L.oracle_kmatrix.restype = C.c_int
+        L.oracle_kmatrix.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_int, _dp]
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return np.ascontiguousarray(a, np.float32).ctypes.data_as(_fp)
+
+
+def eval_fx(sample, block, nda_smr: int, nda_fine: int, swap_coupling_parts: bool = False,
+            threads: int | None = None):
+    """Per-event |A|^2 (fx) and non-interfering w|A|^2 with the reference's band dispatch."""
+    fx = np.zeros(sample.n, np.float64)
+    fxn = np.zeros(sample.n, np.float64)
+    pl = np.ascontiguousarray(block.data, np.float32)
+    keep = (sample.pp, sample.pp1, sample.pp2, pl)
+    rc = lib().oracle_eval_fx(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), sample.n_size, sample.n, nda_smr,
+                              nda_fine, pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size,
+                              block.NR, block.NZ, block.NX, block.ffr, block.ffb, int(swap_coupling_parts),
+                              fx.ctypes.data_as(_dp), fxn.ctypes.data_as(_dp), threads or os.cpu_count())
+    del keep
+    if rc != 0:
+        raise RuntimeError(f"oracle_eval_fx failed: {rc}")
+    return fx, fxn
+
+
+def amp2(sample, block, threads: int | None = None) -> np.ndarray:
+    """Unsmeared, unweighted coherent |A|^2 per event (host_store_amp2s semantics)."""
+    out = np.zeros(sample.n, np.float64)
+    pl = np.ascontiguousarray(block.data, np.float32)
+    rc = lib().oracle_amp2(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), sample.n_size, sample.n,
+                           pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size, block.NR,
+                           block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp), threads or os.cpu_count())
+    if rc != 0:
+        raise RuntimeError(f"oracle_amp2 failed: {rc}")
+    return out
+
+
+def assemble_nll(sample, fx, fxn) -> tuple:
+    out = C.c_double()
+    sw = np.ascontiguousarray(sample.sw, np.float32)
+    s = lib().oracle_assemble_nll(fx.ctypes.data_as(_dp), fxn.ctypes.data_as(_dp), sw.ctypes.data_as(_fp),
+                                  sample.nda, sample.n, sample.sum_w_mc, sample.sum_w_data, NLL_SHIFT, C.byref(out))
+    return out.value, s
+
+
+def nll(sample, block, swap_coupling_parts: bool = False) -> tuple:
+    """(NLL, MC normalisation sum, fx, fx_noint) as host_store_fx would return them, for the band
+    arguments RooDalitzAmplitude::IntegralMethod2 passes."""
+    a, b = sample.reference_band_args()
+    fx, fxn = eval_fx(sample, block, a, b, swap_coupling_parts)
+    v, s = assemble_nll(sample, fx, fxn)
+    return v, s, fx, fxn
+
+
+# ------------------------------------------------------------------ reference built for host cores
+_ref_libs = {}
+
+
+def ref_lib(NR: int, NZ: int, NX: int = 0, ikm: int = 6, build_if_missing: bool = True):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("pwa_build_ref", HERE / "build_ref.py")
+    br = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(br)
+    path = br.lib_path(NR, NZ, NX, ikm)
+    if not path.exists():
+        if not (build_if_missing and br.available()):
+            return None
+        br.build_bucket(NR, NZ, NX, ikm)
+    key = str(path)
+    if key not in _ref_libs:
+        L = C.CDLL(key)
+        L.ref_configure.argtypes = [_fp, C.c_int]
+        L.ref_reset.argtypes = []
+        L.ref_host_store_fx.restype = C.c_double
+        L.ref_host_store_fx.argtypes = [_fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int, _dp, C.c_int,
+                                        C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp,
+                                        C.c_double, C.c_double, C.c_float, C.c_float, C.c_int, C.c_int]
+        L.ref_host_store_amp2s.argtypes = [_fp, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int, _dp, C.c_int,
+                                           C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
+        _ref_libs[key] = L
+    return _ref_libs[key]
+
+
+class RefHost:
+    """The reference's host_store_fx on host cores for one sample (SoA buffers set once)."""
+
+    def __init__(self, sample, block):
+        self.L = ref_lib(block.NR, block.NZ, block.NX)
+        if self.L is None:
+            raise FileNotFoundError("reference host build unavailable")
+        self.s = sample
+        self.pp = np.ascontiguousarray(sample.pp, np.float32)
+        self.pp1 = np.ascontiguousarray(sample.pp1, np.float32)
+        self.pp2 = np.ascontiguousarray(sample.pp2, np.float32)
+        self.pp3 = np.zeros(16, np.float32)
+        self.sw = np.ascontiguousarray(sample.sw, np.float32)
+        self.L.ref_reset()
+        pl = np.ascontiguousarray(block.data, np.float32)
+        self.L.ref_configure(pl.ctypes.data_as(_fp), block.para_size)
+        self.fx = np.zeros(sample.n, np.float64)
+
+    def store_fx(self, block, store_h_fx: bool = True) -> tuple:
+        s = self.s
+        pl = np.ascontiguousarray(block.data, np.float32)
+        out = C.c_double()
+        a, b = s.reference_band_args()
+        sumint = self.L.ref_host_store_fx(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp3),
+                                          _f(self.sw), pl.ctypes.data_as(_fp), block.para_size, block.vamp_size,
+                                          block.spline_size, self.fx.ctypes.data_as(_dp), s.n, 0, s.nda, a, b,
+                                          block.NR, block.NZ, block.NX, C.byref(out), s.sum_w_mc, s.sum_w_data,
+                                          block.ffr, block.ffb, int(store_h_fx), 1)
+        return out.value, sumint
+
+    def amp2s(self, block) -> np.ndarray:
+        out = np.zeros(self.s.n, np.float64)
+        pl = np.ascontiguousarray(block.data, np.float32)
+        self.L.ref_host_store_amp2s(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp3),
+                                    pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size,
+                                    out.ctypes.data_as(_dp), self.s.n, block.NR, block.NZ, block.NX, block.ffr,
+                                    block.ffb)
+        return out

@@ -1,0 +1,717 @@
+// TEST INFRASTRUCTURE ONLY -- the FP64 CPU oracle for the unbinned amplitude likelihood.
+//
+// This file restates, in double precision and in plain scalar C++, the reference's GPU likelihood
+// path (reference files src/kernel_calEva.cu and src/cu_DPFPropogator.cu).  It is used only by the
+// tests, by __graft_entry__.smoke() and by bench.py's cpu_baseline leg, always as the checker; the
+// product path never links or calls it.
+//
+// Inputs are exactly the reference's: the float SoA planes pp/pp1/pp2 (stride n_size), the float
+// parameter block h_paraList, and the band counts.  Every float input and every float constant of
+// the reference is promoted to double unchanged, so a difference between this oracle and a float
+// implementation is arithmetic precision only.
+//
+// Parity is pinned against the reference's own code built for host cores (oracle/build_ref.py),
+// see tests/test_oracle_vs_ref.py.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+using cd = std::complex<double>;
+
+// A float literal of the reference promoted to double (the reference computes with floats).
+constexpr double F(float x) { return (double)x; }
+
+// Masses (cu_DPFPropogator.cu:11-14).
+constexpr double M_LB = F(5.61951f);
+constexpr double M_K = F(0.493677f);
+constexpr double M_P = F(0.938272046f);
+constexpr double M_JPSI = F(3.096916f);
+
+// K-matrix channel masses, averaged isospin partners (cu_DPFPropogator.cu:590-595).
+constexpr double KM_D = F(1.86719f);
+constexpr double KM_DST = F(2.008555f);
+constexpr double KM_SC = F(2.453435f);
+constexpr double KM_SCST = F(2.517955f);
+constexpr double KM_SC_HW = F(-0.00105f);
+constexpr double KM_SCST_HW = F(-0.00800f);
+
+// Resolution model (Resonances.h:56-58).
+constexpr double MRES0 = F(-0.134064f);
+constexpr double MRES1 = F(0.0599014f);
+constexpr double MRES2 = F(-0.00655841f);
+
+// Parameter table layout (Resonances.h:97-112).
+constexpr int NSET = 6;
+enum { P_MASS = 0, P_WIDTH, P_SPIN, P_LRESON, P_TYPE, P_PARITY };
+enum { T_BREITWIGNER = 1, T_KMATRIX = 240, T_NONRESONANT = 361 };
+constexpr int NPMAX = 4;
+constexpr int NKMC = 4;
+
+// Offsets of the reference smearing schemes (Resonances.h:31-54); the values are data of the
+// reference (rounded normal quantiles, not all symmetric) and are reproduced exactly.
+const float kSmear30[30] = {-2.128f, -1.645f, -1.383f, -1.192f, -1.036f, -0.903f, -0.783f, -0.674f,
+                            -0.573f, -0.477f, -0.385f, -0.297f, -0.210f, -0.126f, -0.042f, 0.042f,
+                            0.126f,  0.210f,  0.297f,  0.385f,  0.477f,  0.573f,  0.675f,  0.784f,
+                            0.903f,  1.037f,  1.192f,  1.383f,  1.645f,  2.128f};
+const float kSmear20[20] = {-1.960f, -1.440f, -1.150f, -0.934f, -0.755f, -0.598f, -0.454f,
+                            -0.319f, -0.189f, -0.063f, 0.063f,  0.189f,  0.319f,  0.454f,
+                            0.598f,  0.755f,  0.935f,  1.150f,  1.440f,  1.960f};
+const float kSmear150[150] = {
+    -2.713f, -2.326f, -2.128f, -1.989f, -1.881f, -1.791f, -1.713f, -1.645f, -1.583f, -1.527f,
+    -1.476f, -1.428f, -1.383f, -1.341f, -1.301f, -1.263f, -1.226f, -1.192f, -1.158f, -1.126f,
+    -1.095f, -1.065f, -1.036f, -1.008f, -0.981f, -0.954f, -0.928f, -0.903f, -0.878f, -0.854f,
+    -0.830f, -0.806f, -0.783f, -0.761f, -0.739f, -0.717f, -0.696f, -0.674f, -0.654f, -0.633f,
+    -0.613f, -0.593f, -0.573f, -0.553f, -0.534f, -0.515f, -0.496f, -0.477f, -0.458f, -0.440f,
+    -0.421f, -0.403f, -0.385f, -0.367f, -0.349f, -0.332f, -0.314f, -0.297f, -0.279f, -0.262f,
+    -0.245f, -0.227f, -0.210f, -0.193f, -0.176f, -0.160f, -0.142f, -0.126f, -0.109f, -0.092f,
+    -0.075f, -0.058f, -0.042f, -0.025f, -0.008f, 0.008f, 0.025f, 0.042f, 0.059f, 0.075f,
+    0.092f, 0.109f, 0.126f, 0.143f, 0.160f, 0.176f, 0.193f, 0.210f, 0.228f, 0.245f,
+    0.262f, 0.279f, 0.297f, 0.314f, 0.332f, 0.350f, 0.367f, 0.385f, 0.403f, 0.422f,
+    0.440f, 0.458f, 0.477f, 0.496f, 0.515f, 0.534f, 0.553f, 0.573f, 0.593f, 0.613f,
+    0.633f, 0.654f, 0.675f, 0.696f, 0.717f, 0.739f, 0.761f, 0.784f, 0.806f, 0.830f,
+    0.854f, 0.878f, 0.903f, 0.928f, 0.954f, 0.981f, 1.008f, 1.037f, 1.066f, 1.096f,
+    1.126f, 1.159f, 1.192f, 1.226f, 1.263f, 1.301f, 1.341f, 1.383f, 1.428f, 1.476f,
+    1.527f, 1.583f, 1.645f, 1.713f, 1.791f, 1.881f, 1.989f, 2.128f, 2.326f, 2.713f,
+};
+
+inline double sq(double x) { return x * x; }
+
+// ---------------------------------------------------------------- kinematics (cu_DPFPropogator.cu:33-153)
+double two_body_p(double M, double m1, double m2) {  // getp
+  const double M2 = M * M;
+  return std::sqrt(std::fabs((M2 - sq(m1 + m2)) * (M2 - sq(m1 - m2)))) / 2.0 / M;
+}
+
+double bw_poly(int L, double z) {
+  switch (L) {
+    case 1: return 1.0 + z;
+    case 2: return z * z + 3.0 * z + 9.0;
+    case 3: return z * z * z + 6.0 * z * z + 45.0 * z + 225.0;
+    case 4: return std::pow(z, 4) + 10.0 * std::pow(z, 3) + 135.0 * z * z + 1575.0 * z + 11025.0;
+    case 5:
+      return std::pow(z, 5) + 15.0 * std::pow(z, 4) + 315.0 * std::pow(z, 3) + 6300.0 * z * z +
+             99225.0 * z + 893025.0;
+  }
+  return 1.0;
+}
+
+// Blatt-Weisskopf ratio F_L(p)/F_L(p0) (F_BW, cu_DPFPropogator.cu:69-97).
+double barrier_ratio(double r, int L, double p, double p0) {
+  if (L < 1 || L > 5) return 1.0;
+  const double z = sq(r * p), z0 = sq(r * p0);
+  return std::sqrt(bw_poly(L, z0) / bw_poly(L, z));
+}
+
+// Squared ratio with z from p^2 directly (F_BW2, cu_DPFPropogator.cu:99-127).
+double barrier_ratio2(double r, int L, double p2, double p20) {
+  if (L < 1 || L > 5) return 1.0;
+  const double z = r * r * p2, z0 = r * r * std::fabs(p20);
+  return bw_poly(L, z0) / bw_poly(L, z);
+}
+
+double channel_barrier(double M2, double m1, double m2, int L, double ffb) {  // getFBW2
+  if (L == 0) return 1.0;
+  const double p2 = (M2 - sq(m1 + m2)) * (M2 - sq(m1 - m2)) / M2 / 4.0;
+  const double M20 = 25.0;
+  const double p20 = (M20 - sq(m1 + m2)) * (M20 - sq(m1 - m2)) / M20 / 4.0;
+  return std::pow(p2 / p20, L) * barrier_ratio2(ffb, L, p2, p20);
+}
+
+cd rho_real(double M2, double m1, double m2, int L, double ffb) {  // getrho
+  const double rho2 = (M2 - sq(m1 + m2)) * (M2 - sq(m1 - m2));
+  const double rho = std::sqrt(std::fabs(rho2)) / M2 * channel_barrier(M2, m1, m2, L, ffb);
+  return rho2 >= 0 ? cd(rho, 0) : cd(0, rho);
+}
+
+// The reference's own complex square root (RooTDalitz/cuComplex.h:641-657): zero for tiny inputs,
+// and the imaginary part takes the input's sign only when |Im/Re| > 1e-3.
+cd csqrt_branch(cd x) {
+  if (std::fabs(x.real()) < F(0.000001f) && std::fabs(x.imag()) < F(0.000001f)) return cd(0, 0);
+  const double radius = std::abs(x);
+  const double cosA = x.real() / radius;
+  double re = std::sqrt(radius * (cosA + 1.0) / 2.0);
+  double im = std::sqrt(radius * (1.0 - cosA) / 2.0);
+  if (std::signbit(x.imag()) && std::fabs(x.imag() / x.real()) > F(0.001f)) im = -im;
+  return cd(re, im);
+}
+
+cd rho_complex(double M2, cd m1, cd m2) {  // getrho_complexMass (barrier factor is 1 there)
+  const cd part1 = (m1 + m2) * (m1 + m2) - M2;
+  const cd part2 = (m1 - m2) * (m1 - m2) - M2;
+  return csqrt_branch(part1 * part2) * (1.0 / M2);
+}
+
+// ---------------------------------------------------------------- production barriers (cu_DPFPropogator.cu:155-217)
+double barrier_lb_lstar(double J, double mpp, double mr, double ffb) {  // BTerm
+  const int LB = (J <= 1) ? 0 : (int)(J - 1.5);
+  const double pB = two_body_p(M_LB, M_JPSI, mpp);
+  double pB0 = pB;
+  const double mmin = M_K + M_P, mmax = M_LB - M_JPSI;
+  if (mr < 0) pB0 = two_body_p(M_LB, M_JPSI, (mmin + mmax) / 2.0);
+  if (mr > 1e-10 && mr + M_JPSI < M_LB) pB0 = two_body_p(M_LB, M_JPSI, mr);
+  if (mr + M_JPSI > M_LB) {
+    const double mreff =
+        mmin + 0.5 * (mmax - mmin) * (1.0 + std::tanh((mr - (mmin + mmax) / 2.0) / (mmax - mmin)));
+    pB0 = two_body_p(M_LB, M_JPSI, mreff);
+  }
+  return barrier_ratio(ffb, LB, pB, pB0) * std::pow(pB / M_LB, LB) * std::pow(M_LB / pB0, LB);
+}
+
+double barrier_lb_pc(double J, double mpp, double mr, double ffb) {  // BTermZ
+  const int LB = (int)(J - 0.5);
+  const double pB = two_body_p(M_LB, M_K, mpp);
+  double pB0 = pB;
+  if (mr < 0) pB0 = two_body_p(M_LB, M_K, (M_JPSI + M_P + M_LB - M_K) / 2.0);
+  if (mr > 1e-10 && mr + M_K < M_LB) pB0 = two_body_p(M_LB, M_K, mr);
+  return barrier_ratio(ffb, LB, pB, pB0) * std::pow(pB / M_LB, LB);
+}
+
+// ---------------------------------------------------------------- Breit-Wigners (cu_DPFPropogator.cu:219-336)
+cd breit_wigner(double m, double gamma, double e2) {
+  const double de2 = m * m - e2, gm = gamma * m, d = de2 * de2 + gm * gm;
+  return cd(de2 / d, gm / d);
+}
+
+double bw_norm(double m_r, double gamma_r) {
+  const double kr = std::sqrt(m_r * m_r + gamma_r * gamma_r);
+  return F(0.948850f) * m_r * std::sqrt(gamma_r * kr / std::sqrt(m_r * (m_r + kr)));
+}
+
+cd bw_lstar(double m_r, double gamma_r, double mpp, int LR, double ffr) {  // BW_AMP
+  const double pR = two_body_p(mpp, M_P, M_K);
+  double pR0 = pR;
+  const double mmin = M_K + M_P, mmax = M_LB - M_JPSI;
+  const double thr = F(M_P + M_K);  // float sum in the reference
+  if (m_r < 0) pR0 = two_body_p((mmin + mmax) / 2.0, M_P, M_K);
+  if (m_r > thr) pR0 = two_body_p(m_r, M_P, M_K);
+  if (m_r <= thr && m_r > 1e-10) {
+    const double mreff =
+        mmin + 0.5 * (mmax - mmin) * (1.0 + std::tanh((m_r - (mmin + mmax) / 2.0) / (mmax - mmin)));
+    pR0 = two_body_p(mreff, M_P, M_K);
+  }
+  double FR = barrier_ratio(ffr, LR, pR, pR0);
+  if (m_r < 0) return cd(std::pow(pR / pR0, LR), 0);
+  double gamma = gamma_r;
+  if (m_r > thr) {
+    gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp) * FR * FR;
+  } else if (m_r < F(1.43f) && m_r > 0) {
+    const double msig = F(1.18937f), mpi0 = F(0.13957018f);
+    const double pSP = two_body_p(mpp, msig, mpi0);
+    pR0 = two_body_p(m_r, msig, mpi0);
+    FR = 1.0;
+    gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp);
+    gamma += F(0.0505f) * std::pow(pSP / pR0, 2 * LR + 1) * (m_r / mpp);
+  }
+  const double factor = FR * std::pow(pR / pR0, LR) * bw_norm(m_r, gamma_r);
+  return factor * breit_wigner(m_r, gamma, mpp * mpp);
+}
+
+cd bw_pc(double m_r, double gamma_r, double mpp, int LR, double ffr) {  // BW_AMPZ
+  const double pR = two_body_p(mpp, M_P, M_JPSI);
+  double pR0 = pR;
+  const double thr = F(M_P + M_JPSI);
+  if (m_r > thr) pR0 = two_body_p(m_r, M_P, M_JPSI);
+  const double FR = barrier_ratio(ffr, LR, pR, pR0);
+  double gamma = gamma_r;
+  if (m_r > thr) gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp) * FR * FR;
+  const double factor = FR * std::pow(pR / pR0, LR) * bw_norm(m_r, gamma_r);
+  return factor * breit_wigner(m_r, gamma, mpp * mpp);
+}
+
+// ---------------------------------------------------------------- K-matrix (cu_DPFPropogator.cu:588-813)
+// First row of the inverse of a complex n x n matrix S, via an unpivoted LU of S^T with b = e0
+// (RooTDalitz/cuSolve4x4.h:278-353 uses this construction).
+void first_row_of_inverse(const cd* S, int n, cd* out) {
+  std::vector<cd> A(n * n), L(n * n, cd(0, 0)), U(n * n, cd(0, 0)), invU(n);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) A[r * n + c] = S[c * n + r];
+  for (int i = 0; i < n; ++i) {
+    for (int c = i; c < n; ++c) {
+      cd u = A[i * n + c];
+      for (int k = 0; k < i; ++k) u -= L[i * n + k] * U[k * n + c];
+      U[i * n + c] = u;
+    }
+    invU[i] = 1.0 / U[i * n + i];
+    for (int r = i + 1; r < n; ++r) {
+      cd l = A[r * n + i];
+      for (int k = 0; k < i; ++k) l -= L[r * n + k] * U[k * n + i];
+      L[r * n + i] = l * invU[i];
+    }
+  }
+  std::vector<cd> y(n);
+  for (int i = 0; i < n; ++i) {
+    y[i] = (i == 0) ? cd(1, 0) : cd(0, 0);
+    for (int j = 0; j < i; ++j) y[i] -= L[i * n + j] * y[j];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    cd x = y[i];
+    for (int j = i + 1; j < n; ++j) x -= U[i * n + j] * out[j];
+    out[i] = invU[i] * x;
+  }
+}
+
+struct Model {
+  const float* pl = nullptr;
+  int para_size = 0, vamp_size = 0, spline_size = 0;
+  int NR = 0, NZ = 0, NX = 0;
+  double FFR = 3, FFB = 3;
+  int kmcount = 0;
+  std::vector<int> ampcount;  // first coupling index of each resonance
+  std::vector<int> ikmslot;   // K-matrix output slot of each Pc entry
+  bool swap_coupling_parts = false;
+};
+
+// Coupling offsets (kernel_calEva.cu:1014-1098) and K-matrix output slots (:978-1010).
+void configure(Model& m) {
+  const float* pl = m.pl;
+  int cnt = m.para_size;
+  m.ampcount.assign(m.NR + m.NZ + m.NX, 0);
+  for (int r = 0; r < m.NR; ++r) {
+    m.ampcount[r] = cnt;
+    const int S2 = (int)pl[r * NSET + P_SPIN];
+    cnt += 2 * ((S2 == 1) ? 8 : 12);
+  }
+  for (int i = 0; i < m.NZ; ++i) {
+    const int r = m.NR + i;
+    m.ampcount[r] = cnt;
+    const double S = (int)pl[r * NSET + P_SPIN] / 2.0;
+    for (int k = 0; k < 2; ++k)
+      for (int hpsi = -1; hpsi <= 1; ++hpsi)
+        for (int ihz = 0; ihz < 2; ++ihz)
+          for (int ihp = 0; ihp < 2; ++ihp)
+            if (!(std::fabs(hpsi - (ihp ? 0.5 : -0.5)) > S)) cnt += 2;
+  }
+  for (int i = 0; i < m.NX; ++i) {
+    const int r = m.NR + m.NZ + i;
+    m.ampcount[r] = cnt;
+    const double S = (int)pl[r * NSET + P_SPIN] / 2.0;
+    for (int k = 0; k < 2; ++k)
+      for (int hpsi = -1; hpsi <= 1; ++hpsi) {
+        if (std::abs(hpsi) > S) continue;
+        for (int ihp = 0; ihp < 2; ++ihp) {
+          const double hp = ihp ? 0.5 : -0.5;
+          for (int ihz = 0; ihz < 2; ++ihz) {
+            const double hz = ihz ? hp + 0.5 : hp - 0.5;
+            if (std::fabs(hz) > S) continue;
+            cnt += 2;
+          }
+        }
+      }
+  }
+  int per_group[4] = {0, 0, 0, 0};
+  m.ikmslot.assign(m.NZ, 0);
+  for (int i = 0; i < m.NZ; ++i) {
+    const int r = m.NR + i;
+    const int S2 = (int)pl[r * NSET + P_SPIN], LR = (int)pl[r * NSET + P_LRESON];
+    if ((int)pl[r * NSET + P_TYPE] == T_KMATRIX) {
+      const int ik = (LR > 0) ? ((S2 == 3) ? 3 : 2) : ((S2 == 3) ? 1 : 0);
+      m.ikmslot[i] = per_group[ik]++;
+    }
+  }
+  m.kmcount = m.para_size + m.vamp_size + m.spline_size;
+}
+
+// One J^P group of the coupled-channel Pc K-matrix at invariant mass mpp.  Writes Npole + 4 P-vector
+// outputs (poles first, then the four non-resonant production terms).
+int kmatrix_group(const Model& md, double mpp, int J_r, int P_r, int ik, cd* Mtr) {
+  const float* pl = md.pl;
+  const double ffb = md.FFB;
+  const int Lna = (P_r == 1) ? 1 : 0;
+  const double s = mpp * mpp;
+  cd rho[NKMC];
+  rho[0] = rho_real(s, M_P, M_JPSI, Lna, ffb);
+  if (J_r == 1 && P_r == -1) {
+    rho[1] = rho_complex(s, cd(KM_DST, 0), cd(KM_SC, KM_SC_HW));
+    rho[3] = rho_complex(s, cd(KM_D, 0), cd(KM_SC, KM_SC_HW));
+    rho[2] = rho_complex(s, cd(KM_DST, 0), cd(KM_SCST, KM_SCST_HW));
+  } else if (J_r == 3 && P_r == -1) {
+    rho[1] = rho_complex(s, cd(KM_DST, 0), cd(KM_SC, KM_SC_HW));
+    rho[2] = rho_complex(s, cd(KM_DST, 0), cd(KM_SCST, KM_SCST_HW));
+    rho[3] = rho_complex(s, cd(KM_D, 0), cd(KM_SCST, KM_SCST_HW));
+  } else if (P_r == 1) {
+    rho[1] = rho_real(s, KM_DST, KM_SC, Lna, ffb);
+    rho[2] = rho_real(s, KM_D, KM_SC, Lna, ffb);
+    rho[3] = rho_real(s, KM_D, KM_SCST, Lna, ffb);
+  } else {
+    return -1;  // channel phase space undefined in the reference for this J^P
+  }
+  const float* g_alpha = &pl[md.kmcount + ik * (NPMAX + NKMC) * NKMC];
+  const float* f_scat = &pl[md.kmcount + NPMAX * NKMC + ik * (NPMAX + NKMC) * NKMC];
+  int Npole = 0, ikm = 1;
+  double ms[NPMAX + 1] = {1, 1, 1, 1, 1};
+  for (int r = md.NR; r < md.NR + md.NZ; ++r) {
+    const double mfit = pl[r * NSET + P_MASS];
+    const int iChannel = (int)pl[r * NSET + P_WIDTH];
+    const int S = (int)pl[r * NSET + P_SPIN];
+    const int type = (int)pl[r * NSET + P_TYPE];
+    const int parity = (int)pl[r * NSET + P_PARITY];
+    if (!(type == T_KMATRIX && S == J_r && parity == P_r && mfit > 0)) continue;
+    if (Npole >= NPMAX) return -2;
+    double m0 = mfit;
+    if (iChannel > 0) {
+      const double mfit2 = mfit * mfit;
+      cd rch;
+      if (iChannel == 1)
+        rch = rho_complex(mfit2, cd(KM_DST, 0), cd(KM_SC, KM_SC_HW));
+      else if (iChannel == 2)
+        rch = rho_complex(mfit2, cd(KM_D, 0), cd(KM_SCST, KM_SCST_HW));
+      else if (iChannel == 3)
+        rch = rho_complex(mfit2, cd(KM_D, 0), cd(KM_SC, KM_SC_HW));
+      else
+        return -3;
+      const double g = g_alpha[Npole * NKMC + iChannel];
+      const cd shift = cd(0, g * g) * rch;
+      m0 = std::sqrt(mfit2 + shift.real());
+    } else if (iChannel < 0) {
+      return -3;
+    }
+    double denorm = m0 * m0 - s;
+    if (std::fabs(denorm) < F(1e-3f)) denorm = F(1e-3f);
+    ++Npole;
+    ms[0] *= denorm;
+    for (int ip = 1; ip <= NPMAX; ++ip)
+      if (ip != ikm) ms[ip] *= denorm;
+    ++ikm;
+  }
+  double mg[NPMAX][NKMC], fs[NKMC][NKMC], kma[NKMC][NKMC];
+  for (int i = 0; i < Npole; ++i)
+    for (int j = 0; j < NKMC; ++j) mg[i][j] = g_alpha[i * NKMC + j] * ms[i + 1];
+  for (int i = 0; i < NKMC; ++i)
+    for (int j = 0; j < NKMC; ++j) fs[i][j] = f_scat[i * NKMC + j] * ms[0];
+  for (int i = 0; i < NKMC; ++i)
+    for (int j = i; j < NKMC; ++j) {
+      double v = fs[i][j];
+      for (int k = 0; k < Npole; ++k) v += (double)g_alpha[k * NKMC + i] * mg[k][j];
+      kma[i][j] = kma[j][i] = v;
+    }
+  cd KK[NKMC * NKMC];
+  for (int i = 0; i < NKMC; ++i)
+    for (int j = 0; j < NKMC; ++j) {
+      KK[i * NKMC + j] = cd(0, -1) * (kma[i][j] * rho[j]);
+      if (i == j) KK[i * NKMC + j] += ms[0];
+    }
+  cd T[NKMC];
+  first_row_of_inverse(KK, NKMC, T);
+  const double na = (Lna >= 1) ? channel_barrier(s, M_P, M_JPSI, Lna, ffb) : 1.0;
+  for (int ip = 0; ip < Npole; ++ip) {
+    cd acc(0, 0);
+    for (int i = 0; i < NKMC; ++i) acc += T[i] * mg[ip][i];
+    Mtr[ip] = acc * na;
+  }
+  for (int i = 0; i < NKMC; ++i) Mtr[Npole + i] = T[i] * (ms[0] * na);
+  return Npole + NKMC;
+}
+
+// ---------------------------------------------------------------- per-event amplitudes (kernel_calEva.cu:85-811)
+struct Ev {
+  const float *pp, *pp1, *pp2;
+  long n;  // plane stride
+  long i;  // event index
+  double p0(int plane) const { return pp[i + plane * n]; }
+  double p1(int plane) const { return pp1[i + plane * n]; }
+  double p2(int plane) const { return pp2[i + plane * n]; }
+};
+
+inline cd read_coupling(const Model& md, int& cnt) {
+  const double a = md.pl[cnt], b = md.pl[cnt + 1];
+  cnt += 2;
+  return md.swap_coupling_parts ? cd(b, a) : cd(a, b);
+}
+
+inline int pc_group(int S2, int LR) { return (LR > 0) ? ((S2 == 3) ? 3 : 2) : ((S2 == 3) ? 1 : 0); }
+
+// Lambda* chain contribution to the 8 helicity amplitudes H[4*dmu + 2*lb + p] (GetAmpLz).
+bool amp_lstar(const Model& md, const Ev& e, cd* H) {
+  const double mkp = e.p0(0);
+  for (int r = 0; r < md.NR; ++r) {
+    const float* q = &md.pl[r * NSET];
+    double m0 = q[P_MASS];
+    const double g0 = q[P_WIDTH];
+    const int S2 = (int)q[P_SPIN], LR = (int)q[P_LRESON], type = (int)q[P_TYPE];
+    const double S = 0.5 * S2;
+    cd bw(0, 0);
+    if (type == T_BREITWIGNER)
+      bw = bw_lstar(m0, g0, mkp, LR, md.FFR);
+    else if (type == T_NONRESONANT)
+      bw = cd(1, 0);
+    else
+      return false;  // spline / revised K-matrix Lambda* lineshapes are not restated here
+    bw *= barrier_lb_lstar(S, mkp, m0, md.FFB);
+    int cnt = md.ampcount[r];
+    const int s = (S2 - 1) / 2;
+    for (int k = 0; k < 2; ++k)
+      for (int m = 0; m < 6; ++m) {
+        if (S2 == 1 && m >= 4) continue;
+        const cd c = read_coupling(md, cnt);
+        if (std::abs(c) < 1e-10) continue;
+        const double dl = e.p0(51 + s * 12 + k * 6 + m);
+        for (int i = 0; i < 2; ++i)
+          for (int j = 0; j < 2; ++j) {
+            const int a = 3 + (i * 12 + j * 6 + m) * 2;
+            const cd A(e.p0(a), e.p0(a + 1));
+            H[4 * i + 2 * j + k] += dl * (A * bw) * c;
+          }
+      }
+  }
+  return true;
+}
+
+// Angular part of one Pc entry times its couplings (no lineshape), added into HZ[8].
+void amp_pc_angular(const Model& md, const Ev& e, int iPc, cd scale, cd* HZ) {
+  const int r = md.NR + iPc;
+  const int S2 = (int)md.pl[r * NSET + P_SPIN];
+  const double S = 0.5 * S2;
+  int cnt = md.ampcount[r];
+  const int s = (S2 - 1) / 2;
+  for (int k = 0; k < 2; ++k) {
+    int m = 0;
+    for (int hpsi = -1; hpsi <= 1; ++hpsi)
+      for (int ihz = 0; ihz < 2; ++ihz)
+        for (int ihp = 0; ihp < 2; ++ihp) {
+          const double hp = ihp ? 0.5 : -0.5;
+          if (std::fabs(hpsi - hp) > S) { ++m; continue; }
+          const cd c = read_coupling(md, cnt);
+          if (std::abs(c) < 1e-10) { ++m; continue; }
+          const double dz = e.p2(s * 24 + k * 12 + m);
+          for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j) {
+              const int a = (i * 24 + j * 12 + m) * 2;
+              const cd A(e.p1(a), e.p1(a + 1));
+              HZ[4 * i + 2 * j + k] += dz * (A * scale) * c;
+            }
+          ++m;
+        }
+  }
+}
+
+// Lineshapes of all Pc entries at mass mz (K-matrix groups solved once each).  Returns false if a
+// J^P group cannot be evaluated.
+bool pc_lineshapes(const Model& md, double mz, double weight, cd* bw) {
+  cd akm[4][NPMAX + NKMC];
+  bool have[4] = {false, false, false, false};
+  for (int i = 0; i < md.NZ; ++i) {
+    const float* q = &md.pl[(md.NR + i) * NSET];
+    double m0 = q[P_MASS];
+    const double g0 = q[P_WIDTH];
+    const int S2 = (int)q[P_SPIN], LR = (int)q[P_LRESON], type = (int)q[P_TYPE];
+    cd b(0, 0);
+    if (type == T_BREITWIGNER) {
+      b = bw_pc(m0, g0, mz, LR, md.FFR);
+    } else if (type == T_KMATRIX) {
+      const int ik = pc_group(S2, LR);
+      if (!have[ik]) {
+        if (kmatrix_group(md, mz, S2, (LR > 0) ? 1 : -1, ik, akm[ik]) < 0) return false;
+        have[ik] = true;
+      }
+      b = akm[ik][md.ikmslot[i]];
+    } else if (type == T_NONRESONANT) {
+      b = cd(1, 0);
+    } else {
+      return false;
+    }
+    bw[i] = b * (barrier_lb_pc(0.5 * S2, mz, m0, md.FFB) * weight);
+  }
+  return true;
+}
+
+// Unsmeared |A|^2 (GetAmp2s): coherent sum, or the sum of the chains' separate |A|^2.
+double amp2_unsmeared(const Model& md, const Ev& e, bool interference) {
+  cd HL[8] = {}, HZ[8] = {};
+  if (!amp_lstar(md, e, HL)) return std::nan("");
+  std::vector<cd> bw(std::max(md.NZ, 1));
+  if (md.NZ > 0 && !pc_lineshapes(md, e.p0(1), 1.0, bw.data())) return std::nan("");
+  for (int i = 0; i < md.NZ; ++i) amp_pc_angular(md, e, i, bw[i], HZ);
+  double tot = 0;
+  for (int h = 0; h < 8; ++h)
+    tot += interference ? std::norm(HL[h] + HZ[h]) : std::norm(HL[h]) + std::norm(HZ[h]);
+  return tot;
+}
+
+// Smeared |A|^2 (TemplateGetAmp2s): the Pc lineshapes are averaged over nbins mass offsets
+// scheme[b]*mres(m), bilinearly in the amplitude.  The per-bin weight is the float 1/nbins and the
+// Pc-Pc accumulator is rescaled by its float reciprocal, exactly as the reference does
+// (kernel_calEva.cu:676,771-783), so the effective weights match to the last bit of the constants.
+double amp2_smeared(const Model& md, const Ev& e, int nbins, const float* scheme) {
+  cd HL[8] = {};
+  if (!amp_lstar(md, e, HL)) return std::nan("");
+  const int NZ = md.NZ;
+  std::vector<cd> HZ(NZ * 8, cd(0, 0)), BW1(NZ, cd(0, 0)), BW2(NZ * NZ, cd(0, 0)), bw(std::max(NZ, 1));
+  for (int i = 0; i < NZ; ++i) amp_pc_angular(md, e, i, cd(1, 0), &HZ[i * 8]);
+  const double mz = e.p0(1);
+  const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
+  const float wf = (float)(1.0 / nbins);
+  const double w = wf;
+  const double unscale = (double)(1.f / wf);
+  for (int b = 0; b < nbins; ++b) {
+    const double off = (double)scheme[b] * mres;
+    if (NZ > 0 && !pc_lineshapes(md, mz + off, w, bw.data())) return std::nan("");
+    for (int i = 0; i < NZ; ++i) {
+      BW1[i] += bw[i];
+      for (int j = 0; j < NZ; ++j) BW2[i * NZ + j] += bw[i] * std::conj(bw[j] * unscale);
+    }
+  }
+  double tot = 0;
+  for (int h = 0; h < 8; ++h) {
+    tot += std::norm(HL[h]);
+    for (int i = 0; i < NZ; ++i) {
+      tot += 2.0 * (std::conj(HL[h]) * (BW1[i] * HZ[i * 8 + h])).real();
+      for (int j = 0; j < NZ; ++j) tot += (BW2[i * NZ + j] * HZ[i * 8 + h] * std::conj(HZ[j * 8 + h])).real();
+    }
+  }
+  return tot;
+}
+
+// In the reference the 3/2-band and 20-bin windows are tested on the float mass.
+bool in_mc_smear_window(float mz) { return (mz > 4.4 && mz < 4.48) || (mz > 4.27 && mz < 4.34); }
+
+}  // namespace
+
+extern "C" {
+
+// Per-event |A|^2 with the reference's band dispatch (kernel_calEva.cu:819-961):
+//   [0, nda_smr)                     30-offset smearing
+//   [nda_smr, nda_smr + nda_fine)    150-offset smearing
+//   [nda_smr + nda_fine, n_events)   20-offset smearing inside the MC windows, else unsmeared,
+//                                    times the event weight w unless w <= -1000 (data sentinel).
+// fx_noint receives w*|A|^2 without Pc/Lambda* interference (0 for data).  Returns 0 on success.
+int oracle_eval_fx(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
+                   long nda_smr, long nda_fine, const float* paraList, int para_size, int vamp_size,
+                   int spline_size, int NR, int NZ, int NX, float FFR, float FFB, int swap_coupling_parts,
+                   double* fx, double* fx_noint, int nthreads) {
+  if (NX != 0) return -10;  // the Zcs chain is not part of this oracle
+  Model md;
+  md.pl = paraList;
+  md.para_size = para_size;
+  md.vamp_size = vamp_size;
+  md.spline_size = spline_size;
+  md.NR = NR;
+  md.NZ = NZ;
+  md.NX = NX;
+  md.FFR = FFR;
+  md.FFB = FFB;
+  md.swap_coupling_parts = swap_coupling_parts != 0;
+  configure(md);
+  const long b1 = std::max(0L, nda_smr);
+  const long b2 = std::max(0L, nda_smr + nda_fine);
+  int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(| : err)
+  for (long i = 0; i < n_events; ++i) {
+    Ev e{pp, pp1, pp2, n_size, i};
+    double v;
+    if (i < b1) {
+      v = amp2_smeared(md, e, 30, kSmear30);
+      fx[i] = v;
+      if (fx_noint) fx_noint[i] = 0;
+    } else if (i < b2) {
+      v = amp2_smeared(md, e, 150, kSmear150);
+      fx[i] = v;
+      if (fx_noint) fx_noint[i] = 0;
+    } else {
+      const float mz = pp[i + n_size];
+      v = in_mc_smear_window(mz) ? amp2_smeared(md, e, 20, kSmear20) : amp2_unsmeared(md, e, true);
+      const double w = pp[i + 2 * n_size];
+      const bool data = pp[i + 2 * n_size] <= -1000.f;
+      fx[i] = data ? v : v * w;
+      if (fx_noint) fx_noint[i] = data ? 0.0 : amp2_unsmeared(md, e, false) * w;
+    }
+    if (std::isnan(v)) err |= 1;
+  }
+  return err ? -12 : 0;
+}
+
+// Per-event unsmeared coherent |A|^2 without weights (GetAmp2s_NoSMR as used by
+// kernel_store_amp2s, kernel_calEva.cu:1365-1373).
+int oracle_amp2(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
+                const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                float FFR, float FFB, double* out, int nthreads) {
+  if (NX != 0) return -10;
+  Model md;
+  md.pl = paraList;
+  md.para_size = para_size;
+  md.vamp_size = vamp_size;
+  md.spline_size = spline_size;
+  md.NR = NR;
+  md.NZ = NZ;
+  md.FFR = FFR;
+  md.FFB = FFB;
+  configure(md);
+  int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(| : err)
+  for (long i = 0; i < n_events; ++i) {
+    Ev e{pp, pp1, pp2, n_size, i};
+    out[i] = amp2_unsmeared(md, e, true);
+    if (std::isnan(out[i])) err |= 1;
+  }
+  return err ? -12 : 0;
+}
+
+// NLL assembly of host_store_fx (kernel_calEva.cu:1296-1362) from per-event values, with
+// compensated sums.  Returns the MC normalisation sum; writes the NLL (including the
+// +1000 interference guard) to *nll.
+double oracle_assemble_nll(const double* fx, const double* fx_noint, const float* sw, long nda,
+                           long n_events, double sum_w_mc, double sum_w_data, double nll_shift,
+                           double* nll) {
+  auto kahan = [](double& s, double& c, double x) {
+    const double y = x - c, t = s + y;
+    c = (t - s) - y;
+    s = t;
+  };
+  double si = 0, ci = 0, sn = 0, cn = 0, sd = 0, cdd = 0;
+  for (long i = nda; i < n_events; ++i) {
+    kahan(si, ci, fx[i]);
+    kahan(sn, cn, fx_noint[i]);
+  }
+  for (long i = 0; i < nda; ++i) kahan(sd, cdd, fx[i] > 0 ? std::log(fx[i]) * (double)sw[i] : -1e12);
+  double v = nll_shift + sum_w_data * std::log(si / sum_w_mc) - sd;
+  if (std::fabs(sn / si - 1.0) > F(0.3f)) v += 1000.0;
+  *nll = v;
+  return si;
+}
+
+// Lineshape probes for unit tests.
+void oracle_bw_lstar(double m_r, double gamma_r, double mpp, int LR, double ffr, double* out) {
+  const cd v = bw_lstar(m_r, gamma_r, mpp, LR, ffr);
+  out[0] = v.real();
+  out[1] = v.imag();
+}
+void oracle_bw_pc(double m_r, double gamma_r, double mpp, int LR, double ffr, double* out) {
+  const cd v = bw_pc(m_r, gamma_r, mpp, LR, ffr);
+  out[0] = v.real();
+  out[1] = v.imag();
+}
+double oracle_barrier_lb_lstar(double J, double mpp, double mr, double ffb) {
+  return barrier_lb_lstar(J, mpp, mr, ffb);
+}
+double oracle_barrier_lb_pc(double J, double mpp, double mr, double ffb) { return barrier_lb_pc(J, mpp, mr, ffb); }
+
+// P-vector outputs of K-matrix group ik at mass mpp; out holds 2*(Npole+4) doubles.  Returns the
+// number of complex outputs or a negative error.
+int oracle_kmatrix(const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                   double FFB, double mpp, int ik, double* out) {
+  Model md;
+  md.pl = paraList;
+  md.para_size = para_size;
+  md.vamp_size = vamp_size;
+  md.spline_size = spline_size;
+  md.NR = NR;
+  md.NZ = NZ;
+  md.FFB = FFB;
+  configure(md);
+  const int J = (ik == 1 || ik == 3) ? 3 : 1;
+  const int P = (ik >= 2) ? 1 : -1;
+  cd M[NPMAX + NKMC];
+  const int n = kmatrix_group(md, mpp, J, P, ik, M);
+  for (int i = 0; i < n; ++i) {
+    out[2 * i] = M[i].real();
+    out[2 * i + 1] = M[i].imag();
+  }
+  return n;
+}
+
+}  // extern "C"

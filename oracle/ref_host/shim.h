@@ -1,0 +1,83 @@
+// TEST INFRASTRUCTURE ONLY -- pre-included header that lets the reference's CUDA sources
+// (src/kernel_calEva.cu, src/cu_DPFPropogator.cu) compile and run as plain host C++.
+//
+// * CUDA runtime calls become host memory operations (no GPU is touched by this build).
+// * Kernel launches, rewritten at build time from `K<<<g, b>>>(args)` to
+//   `ref_host::Launch(g, b, K)(args)`, run every (block, thread) on host cores, blocks in parallel.
+// * blockIdx/threadIdx/blockDim are per-host-thread variables.
+#pragma once
+#define NVTX_DISABLE 1
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <vector>
+
+extern thread_local dim3 blockIdx;
+extern thread_local dim3 threadIdx;
+extern thread_local dim3 blockDim;
+
+namespace ref_host {
+// Allocations are padded: the reference's normalisation kernel writes and reads a few hundred
+// elements past the end of its buffers in tail threads (kernel_calEva.cu:908-917).
+constexpr size_t kPad = 1 << 16;
+inline cudaError_t malloc_padded(void** p, size_t n) {
+  *p = std::calloc(n + kPad, 1);
+  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+inline cudaError_t copy(void* dst, const void* src, size_t n) {
+  if (n) std::memcpy(dst, src, n);
+  return cudaSuccess;
+}
+template <class T>
+inline cudaError_t copy_to_symbol(T& sym, const void* src, size_t n) {
+  if (n) std::memcpy((void*)&sym, src, n);
+  return cudaSuccess;
+}
+
+struct Launch {
+  long grid, block;
+  Launch(long g, long b) : grid(g), block(b) {}
+  template <class K>
+  struct Bound {
+    long grid, block;
+    K kernel;
+    template <class... A>
+    void operator()(A... args) const {
+#pragma omp parallel for schedule(dynamic, 4)
+      for (long b = 0; b < grid; ++b) {
+        blockDim = dim3((unsigned)block, 1, 1);
+        blockIdx = dim3((unsigned)b, 1, 1);
+        for (long t = 0; t < block; ++t) {
+          threadIdx = dim3((unsigned)t, 1, 1);
+          kernel(args...);
+        }
+      }
+    }
+  };
+};
+template <class K>
+inline Launch::Bound<K> launch(long g, long b, K k) {
+  return Launch::Bound<K>{g, b, k};
+}
+
+// Reads a (re, im) coupling pair and advances the cursor by two, in source order.
+inline float2 ordered_pair(const float* p, int& cursor) {
+  float2 v;
+  v.x = p[cursor];
+  v.y = p[cursor + 1];
+  cursor += 2;
+  return v;
+}
+}  // namespace ref_host
+
+#define cudaSetDevice(d) (cudaSuccess)
+#define cudaDeviceReset() (cudaSuccess)
+#define cudaMalloc(p, n) ref_host::malloc_padded((void**)(p), (size_t)(n))
+#define cudaFree(p) (std::free((void*)(p)), cudaSuccess)
+#define cudaMemcpy(d, s, n, k) ref_host::copy((void*)(d), (const void*)(s), (size_t)(n))
+#define cudaMemcpyAsync(d, s, n, k) ref_host::copy((void*)(d), (const void*)(s), (size_t)(n))
+#define cudaMemcpyToSymbol(sym, s, n) ref_host::copy_to_symbol((sym), (const void*)(s), (size_t)(n))
+#define cudaGetErrorString(e) ("host build")

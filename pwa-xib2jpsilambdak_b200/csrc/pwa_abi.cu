@@ -1,0 +1,315 @@
+// C ABI (include/pwa_b200.h): contexts, event upload and one-call likelihood evaluation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pwa_b200.h"
+#include "pwa_kernels.cuh"
+
+using namespace pwa;
+
+namespace pwa {
+cudaError_t configure_kernels();
+}
+
+namespace {
+thread_local std::string g_last_cuda = "no error";
+
+int cuda_fail(cudaError_t e) {
+  g_last_cuda = cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? PWA_E_NOMEM : PWA_E_CUDA;
+}
+#define PWA_CUDA(x)                      \
+  do {                                   \
+    cudaError_t _e = (x);                \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+
+// m(J/psi p) windows of the 20-offset smearing of the normalisation kernel
+// (kernel_calEva.cu:874), tested on the float mass as the reference does.
+inline bool in_window(float mz) { return (mz > 4.4 && mz < 4.48) || (mz > 4.27 && mz < 4.34); }
+}  // namespace
+
+struct pwa_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // events
+  const float *pp = nullptr, *pp1 = nullptr, *pp2 = nullptr, *sw = nullptr;
+  float *own_pp = nullptr, *own_pp1 = nullptr, *own_pp2 = nullptr, *own_sw = nullptr;
+  int64_t n = 0, n_size = 0, nda = 0, nda_smr = 0, nda_fine = 0;
+  int32_t* d_lists = nullptr;
+  std::vector<Segment> segs;
+  std::vector<int> seg_off;
+  int total_parts = 0;
+  // per evaluation
+  PointTable* d_table = nullptr;
+  PointTable* h_table = nullptr;
+  Partial* d_parts = nullptr;
+  EvalResult* d_res = nullptr;
+  EvalResult* h_res = nullptr;
+  double* d_fx = nullptr;
+  int64_t fx_cap = 0;
+  double last_ms = 0;
+  int last_launches = 0;
+};
+
+namespace {
+
+void free_events(pwa_ctx* c) {
+  cudaFree(c->own_pp);
+  cudaFree(c->own_pp1);
+  cudaFree(c->own_pp2);
+  cudaFree(c->own_sw);
+  cudaFree(c->d_lists);
+  cudaFree(c->d_parts);
+  c->own_pp = c->own_pp1 = c->own_pp2 = c->own_sw = nullptr;
+  c->d_lists = nullptr;
+  c->d_parts = nullptr;
+  c->pp = c->pp1 = c->pp2 = c->sw = nullptr;
+  c->segs.clear();
+  c->seg_off.clear();
+  c->n = 0;
+}
+
+// Splits the events into the reference's kernel ranges (fake_kernel_store_fx,
+// kernel_calEva.cu:920-961, begin = 0) and classifies the tail by the 20-offset window.
+int build_segments(pwa_ctx* c, const float* h_mz) {
+  const int64_t n = c->n;
+  const int64_t b1e = std::max<int64_t>(0, std::min(n, c->nda_smr));
+  const int64_t b2s = std::max<int64_t>(0, c->nda_smr);
+  const int64_t b2e = std::max<int64_t>(b2s, std::min(n, c->nda_smr + c->nda_fine));
+  const int64_t r0 = std::min(n, std::max<int64_t>(0, c->nda_smr + c->nda_fine));
+  std::vector<int32_t> lw, lu;
+  lw.reserve(n / 4);
+  lu.reserve(n - r0);
+  for (int64_t e = r0; e < n; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+  const size_t nl = lw.size() + lu.size();
+  if (nl) {
+    PWA_CUDA(cudaMalloc(&c->d_lists, nl * sizeof(int32_t)));
+    if (!lw.empty()) PWA_CUDA(cudaMemcpy(c->d_lists, lw.data(), lw.size() * 4, cudaMemcpyHostToDevice));
+    if (!lu.empty())
+      PWA_CUDA(cudaMemcpy(c->d_lists + lw.size(), lu.data(), lu.size() * 4, cudaMemcpyHostToDevice));
+  }
+  c->segs.clear();
+  // heaviest work first so the long tiles start early
+  if (b2e > b2s) c->segs.push_back({SMEAR_150, b2s, b2e, nullptr});
+  if (b1e > 0) c->segs.push_back({SMEAR_30, 0, b1e, nullptr});
+  if (!lw.empty()) c->segs.push_back({SMEAR_20, 0, (int64_t)lw.size(), c->d_lists});
+  if (!lu.empty()) c->segs.push_back({SMEAR_NONE, 0, (int64_t)lu.size(), c->d_lists + lw.size()});
+  c->seg_off.clear();
+  int tot = 0;
+  for (auto& s : c->segs) {
+    c->seg_off.push_back(tot);
+    tot += segment_blocks(s, c->sm_count);
+  }
+  c->total_parts = std::max(tot, 1);
+  PWA_CUDA(cudaMalloc(&c->d_parts, c->total_parts * sizeof(Partial)));
+  PWA_CUDA(cudaMemset(c->d_parts, 0, c->total_parts * sizeof(Partial)));
+  return PWA_OK;
+}
+
+int check_events(int64_t n, int64_t n_size, int64_t nda) {
+  if (n < 0 || nda < 0 || nda > n || n_size < n || n > INT32_MAX) return PWA_E_ARG;
+  return PWA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pwa_error_string(int code) {
+  switch (code) {
+    case PWA_OK: return "ok";
+    case PWA_E_CUDA: return "CUDA runtime error";
+    case PWA_E_ARG: return "invalid argument";
+    case PWA_E_LAYOUT: return "parameter block layout inconsistent with the resonance table";
+    case PWA_E_SIZE: return "model size exceeds the compiled maximum";
+    case PWA_E_UNSUPPORTED: return "lineshape type or decay chain not supported";
+    case PWA_E_PARAM: return "invalid resonance parameters";
+    case PWA_E_STATE: return "no events uploaded";
+    case PWA_E_NOMEM: return "device allocation failed";
+  }
+  return "unknown error";
+}
+
+const char* pwa_last_cuda_error(void) { return g_last_cuda.c_str(); }
+
+int pwa_ctx_create(int device, pwa_ctx** out) {
+  if (!out) return PWA_E_ARG;
+  *out = nullptr;
+  pwa_ctx* c = new pwa_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = configure_kernels();
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->e1);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_table, sizeof(PointTable));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->h_table, sizeof(PointTable));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_res, sizeof(EvalResult));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->h_res, sizeof(EvalResult));
+  if (e != cudaSuccess) {
+    pwa_ctx_destroy(c);
+    return cuda_fail(e);
+  }
+  *out = c;
+  return PWA_OK;
+}
+
+int pwa_ctx_destroy(pwa_ctx* c) {
+  if (!c) return PWA_OK;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  free_events(c);
+  cudaFree(c->d_table);
+  cudaFreeHost(c->h_table);
+  cudaFree(c->d_res);
+  cudaFreeHost(c->h_res);
+  cudaFree(c->d_fx);
+  if (c->e0) cudaEventDestroy(c->e0);
+  if (c->e1) cudaEventDestroy(c->e1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return PWA_OK;
+}
+
+int pwa_ctx_upload_events(pwa_ctx* c, const float* pp, const float* pp1, const float* pp2, const float* sw,
+                          int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr, int64_t nda_fine) {
+  if (!c || !pp || !pp1 || !pp2 || (nda > 0 && !sw)) return PWA_E_ARG;
+  int rc = check_events(n, n_size, nda);
+  if (rc) return rc;
+  PWA_CUDA(cudaSetDevice(c->device));
+  free_events(c);
+  const size_t ns = (size_t)n_size;
+  PWA_CUDA(cudaMalloc(&c->own_pp, 111 * ns * sizeof(float)));
+  PWA_CUDA(cudaMalloc(&c->own_pp1, 96 * ns * sizeof(float)));
+  PWA_CUDA(cudaMalloc(&c->own_pp2, 96 * ns * sizeof(float)));
+  PWA_CUDA(cudaMalloc(&c->own_sw, ns * sizeof(float)));
+  PWA_CUDA(cudaMemcpy(c->own_pp, pp, 111 * ns * sizeof(float), cudaMemcpyHostToDevice));
+  PWA_CUDA(cudaMemcpy(c->own_pp1, pp1, 96 * ns * sizeof(float), cudaMemcpyHostToDevice));
+  PWA_CUDA(cudaMemcpy(c->own_pp2, pp2, 96 * ns * sizeof(float), cudaMemcpyHostToDevice));
+  if (sw)
+    PWA_CUDA(cudaMemcpy(c->own_sw, sw, ns * sizeof(float), cudaMemcpyHostToDevice));
+  else
+    PWA_CUDA(cudaMemset(c->own_sw, 0, ns * sizeof(float)));
+  c->pp = c->own_pp;
+  c->pp1 = c->own_pp1;
+  c->pp2 = c->own_pp2;
+  c->sw = c->own_sw;
+  c->n = n;
+  c->n_size = n_size;
+  c->nda = nda;
+  c->nda_smr = nda_smr;
+  c->nda_fine = nda_fine;
+  return build_segments(c, pp + n_size);
+}
+
+int pwa_ctx_set_device_events(pwa_ctx* c, const float* d_pp, const float* d_pp1, const float* d_pp2,
+                              const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
+                              int64_t nda_fine) {
+  if (!c || !d_pp || !d_pp1 || !d_pp2 || (nda > 0 && !d_sw)) return PWA_E_ARG;
+  int rc = check_events(n, n_size, nda);
+  if (rc) return rc;
+  PWA_CUDA(cudaSetDevice(c->device));
+  free_events(c);
+  c->pp = d_pp;
+  c->pp1 = d_pp1;
+  c->pp2 = d_pp2;
+  c->sw = d_sw;
+  c->n = n;
+  c->n_size = n_size;
+  c->nda = nda;
+  c->nda_smr = nda_smr;
+  c->nda_fine = nda_fine;
+  std::vector<float> mz((size_t)std::max<int64_t>(n, 1));
+  if (n) PWA_CUDA(cudaMemcpy(mz.data(), d_pp + n_size, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return build_segments(c, mz.data());
+}
+
+int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                     int NX, float FFR, float FFB, double sum_w_mc, double sum_w_data, double nll_shift,
+                     pwa_result* out, double* h_fx) {
+  if (!c || !pl || !out) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  if (spline_size != 0) return PWA_E_UNSUPPORTED;
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  if (rc) return rc;
+  PWA_CUDA(cudaSetDevice(c->device));
+  if (h_fx && c->fx_cap < c->n) {
+    cudaFree(c->d_fx);
+    c->d_fx = nullptr;
+    PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
+    c->fx_cap = c->n;
+  }
+  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
+  PWA_CUDA(cudaEventRecord(c->e0, c->st));
+  int launches = 0;
+  for (size_t i = 0; i < c->segs.size(); ++i) {
+    PWA_CUDA(launch_segment(ev, c->segs[i], c->d_table, c->d_parts + c->seg_off[i], h_fx ? c->d_fx : nullptr,
+                            c->sm_count, c->st));
+    ++launches;
+  }
+  PWA_CUDA(launch_finalize(c->d_parts, c->total_parts, sum_w_mc, sum_w_data, nll_shift, c->d_res, c->st));
+  ++launches;
+  PWA_CUDA(cudaEventRecord(c->e1, c->st));
+  PWA_CUDA(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, c->st));
+  if (h_fx && c->n) PWA_CUDA(cudaMemcpyAsync(h_fx, c->d_fx, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  PWA_CUDA(cudaStreamSynchronize(c->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->e0, c->e1);
+  c->last_ms = ms;
+  c->last_launches = launches;
+  out->nll = c->h_res->nll;
+  out->sumint = c->h_res->sumint;
+  out->sum_noint = c->h_res->sum_noint;
+  out->data_term = c->h_res->data_term;
+  out->n_nonpos = (int64_t)c->h_res->n_nonpos;
+  return PWA_OK;
+}
+
+int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                 float FFR, float FFB, double* h_amp2) {
+  if (!c || !pl || !h_amp2) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  if (spline_size != 0) return PWA_E_UNSUPPORTED;
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  if (rc) return rc;
+  PWA_CUDA(cudaSetDevice(c->device));
+  if (c->fx_cap < c->n) {
+    cudaFree(c->d_fx);
+    c->d_fx = nullptr;
+    PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
+    c->fx_cap = c->n;
+  }
+  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
+  PWA_CUDA(launch_amp2(ev, c->d_table, c->d_fx, c->sm_count, c->st));
+  if (c->n) PWA_CUDA(cudaMemcpyAsync(h_amp2, c->d_fx, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  PWA_CUDA(cudaStreamSynchronize(c->st));
+  return PWA_OK;
+}
+
+int pwa_host_lineshapes(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                        float FFR, float FFB, double mkp, double mz, double* lstar, double* pc) {
+  if (!pl || !lstar || !pc) return PWA_E_ARG;
+  PointTable* T = new PointTable();
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, T);
+  if (!rc) host_lineshapes(*T, mkp, mz, reinterpret_cast<cplx*>(lstar), reinterpret_cast<cplx*>(pc));
+  delete T;
+  return rc;
+}
+
+double pwa_ctx_last_kernel_ms(pwa_ctx* c) { return c ? c->last_ms : 0.0; }
+int pwa_ctx_last_launches(pwa_ctx* c) { return c ? c->last_launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+// Host-visible declarations of the likelihood kernels (pwa_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pwa_point.cuh"
+
+namespace pwa {
+
+// Per-block partial sums written by the event kernels and reduced by finalize.
+struct Partial {
+  double data;      // sum of sw * ln(fx) over data events (fx <= 0 contributes -1e12)
+  double mc;        // sum of w * fx over MC events
+  double mc_noint;  // sum of w * fx without Pc/Lambda* interference over MC events
+  double n_nonpos;  // events with fx <= 0 or non-finite fx
+};
+
+// Evaluation result copied back to the host.
+struct EvalResult {
+  double nll;        // NLL_SHIFT + sumW_data * ln(I / sumW_mc) - sum sw ln fx (+1000 guard)
+  double sumint;     // sum over MC of w * fx
+  double sum_noint;  // same without interference
+  double data_term;  // sum over data of sw * ln fx
+  double n_nonpos;
+  double status;
+};
+
+// Event ranges of one evaluation.  Smeared classes are given as index lists or contiguous ranges.
+struct EventSet {
+  const float* pp;
+  const float* pp1;
+  const float* pp2;
+  const float* sw;  // data sWeights, index = event index (may be null when there is no data)
+  int64_t n_size;   // plane stride
+  int64_t n;        // events
+  int64_t nda;      // events [0, nda) are data (NLL term), the rest MC (normalisation)
+};
+
+enum Smear : int { SMEAR_NONE = 0, SMEAR_20 = 1, SMEAR_30 = 2, SMEAR_150 = 3 };
+
+struct Segment {
+  int kind;             // Smear
+  int64_t begin, end;   // contiguous event range when list == nullptr
+  const int32_t* list;  // event indices, [begin, end) positions in the list otherwise
+};
+
+// Number of partial slots a segment uses for a given launch width.
+int segment_blocks(const Segment& s, int sm_count);
+
+// Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.
+int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                      float ffr, float ffb, PointTable* out);
+
+// Launches one segment; partials written at out[0 .. segment_blocks).  fx_out (optional) receives
+// per-event fx (weighted by w for MC, like the reference's d_fx).
+cudaError_t launch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
+                           double* fx_out, int sm_count, cudaStream_t st);
+
+// Reduces nparts partials and assembles the NLL.
+cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, double sum_w_data,
+                            double nll_shift, EvalResult* res, cudaStream_t st);
+
+// Host evaluation of the decoded lineshapes (see pwa_kernels.cu).
+void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cplx* pc);
+
+// Per-event unsmeared |A|^2 without weights (host_store_amp2s semantics) for n events.
+cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int sm_count, cudaStream_t st);
+
+}  // namespace pwa

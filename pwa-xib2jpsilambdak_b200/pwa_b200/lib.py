@@ -1,0 +1,141 @@
+"""ctypes bindings of libpwa_b200.so (include/pwa_b200.h).
+
+The library is the only compute path: there is no CPU fallback, and loading fails loudly if the
+shared object is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libpwa_b200.so"
+
+EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
+            "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches",
+            "pwa_host_lineshapes", "pwa_error_string", "pwa_last_cuda_error"]
+
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+
+
+class PwaResult(C.Structure):
+    _fields_ = [("nll", C.c_double), ("sumint", C.c_double), ("sum_noint", C.c_double),
+                ("data_term", C.c_double), ("n_nonpos", C.c_int64)]
+
+
+class PwaError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise PwaError(f"{LIB_PATH} is missing: build it with pwa-xib2jpsilambdak_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        L.pwa_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        L.pwa_ctx_destroy.argtypes = [C.c_void_p]
+        L.pwa_ctx_upload_events.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp] + [C.c_int64] * 5
+        L.pwa_ctx_set_device_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + \
+            [C.c_int64] * 5
+        L.pwa_ctx_eval_nll.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_float, C.c_float, C.c_double, C.c_double, C.c_double,
+                                       C.POINTER(PwaResult), _dp]
+        L.pwa_ctx_amp2.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_float, C.c_float, _dp]
+        L.pwa_ctx_last_kernel_ms.restype = C.c_double
+        L.pwa_ctx_last_kernel_ms.argtypes = [C.c_void_p]
+        L.pwa_ctx_last_launches.argtypes = [C.c_void_p]
+        L.pwa_host_lineshapes.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                          C.c_float, C.c_double, C.c_double, _dp, _dp]
+        L.pwa_error_string.restype = C.c_char_p
+        L.pwa_last_cuda_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        L = load()
+        raise PwaError(f"{what}: {L.pwa_error_string(rc).decode()} ({L.pwa_last_cuda_error().decode()})")
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp)
+
+
+class Context:
+    """One device context holding an uploaded event sample."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        check(self.L.pwa_ctx_create(device, C.byref(h)), "pwa_ctx_create")
+        self.h = h
+        self.sample = None
+
+    def close(self):
+        if self.h:
+            self.L.pwa_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, sample, nda_smr: int | None = None, nda_fine: int | None = None):
+        """Upload a Sample (reference layout).  Band arguments default to what
+        RooDalitzAmplitude::IntegralMethod2 passes (first count minus one)."""
+        a, b = sample.reference_band_args()
+        a = a if nda_smr is None else nda_smr
+        b = b if nda_fine is None else nda_fine
+        pp = np.ascontiguousarray(sample.pp, np.float32)
+        pp1 = np.ascontiguousarray(sample.pp1, np.float32)
+        pp2 = np.ascontiguousarray(sample.pp2, np.float32)
+        sw = np.ascontiguousarray(sample.sw, np.float32)
+        check(self.L.pwa_ctx_upload_events(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n, sample.n_size,
+                                           sample.nda, a, b), "pwa_ctx_upload_events")
+        self.sample = sample
+
+    def eval_nll(self, block, nll_shift: float = 1e7, want_fx: bool = False):
+        s = self.sample
+        pl = np.ascontiguousarray(block.data, np.float32)
+        r = PwaResult()
+        fx = np.zeros(s.n, np.float64) if want_fx else None
+        check(self.L.pwa_ctx_eval_nll(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR,
+                                      block.NZ, block.NX, block.ffr, block.ffb, s.sum_w_mc, s.sum_w_data, nll_shift,
+                                      C.byref(r), fx.ctypes.data_as(_dp) if want_fx else None), "pwa_ctx_eval_nll")
+        return (r, fx) if want_fx else r
+
+    def amp2(self, block) -> np.ndarray:
+        s = self.sample
+        pl = np.ascontiguousarray(block.data, np.float32)
+        out = np.zeros(s.n, np.float64)
+        check(self.L.pwa_ctx_amp2(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR,
+                                  block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp)), "pwa_ctx_amp2")
+        return out
+
+    def last_kernel_ms(self) -> float:
+        return self.L.pwa_ctx_last_kernel_ms(self.h)
+
+    def last_launches(self) -> int:
+        return self.L.pwa_ctx_last_launches(self.h)
+
+
+def host_lineshapes(block, mkp: float, mz: float):
+    """Decoded Lambda* and Pc lineshapes (times production barriers) evaluated on the host."""
+    L = load()
+    pl = np.ascontiguousarray(block.data, np.float32)
+    ls = np.zeros(2 * max(block.NR, 1))
+    pc = np.zeros(2 * max(block.NZ, 1))
+    check(L.pwa_host_lineshapes(_f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR, block.NZ,
+                                block.NX, block.ffr, block.ffb, mkp, mz, ls.ctypes.data_as(_dp),
+                                pc.ctypes.data_as(_dp)), "pwa_host_lineshapes")
+    return ls[0::2][:block.NR] + 1j * ls[1::2][:block.NR], pc[0::2][:block.NZ] + 1j * pc[1::2][:block.NZ]

@@ -1,0 +1,406 @@
+"""Amplitude model: resonance lists, parameter values and the float parameter block.
+
+The parameter block ("h_paraList") is the hot path's per-call input.  Its layout and contents
+restate the reference host code that builds it every FCN call:
+
+* resonance table, 6 floats per resonance [m0, width-or-channel, 2J, L, type, parity]
+  (RooDalitzAmplitude::setup_paraList, src/RooDalitzAmplitude.cxx:3068-3139),
+* helicity couplings as (Re, Im) float pairs (ConfigureCouplings :2669-2986, PartWaveCoff :5533-5599,
+  PartWaveCoffZ :5601-5710),
+* K-matrix blocks, per J^P group 16 pole couplings g then the 4x4 scattering matrix f
+  (cu_init_data :3141-3210).
+
+Float intermediates of the reference (float sqrt of the kinematic factor, float Clebsch-Gordan
+coefficients) are reproduced so the block is bit-identical to the reference's for the same
+parameter values.  Parameter files use the reference's text format (see `read_func`).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import re
+from fractions import Fraction
+from functools import lru_cache
+from typing import Callable
+
+import numpy as np
+
+BREITWIGNER, MODELINDEPENDENT, KMATRIX, REVISEDKMATRIX, NONRESONANT = 1, 3, 240, 360, 361
+NSET, NPMAX, NKMC = 6, 4, 4
+KM_BLOCK = (NPMAX + NKMC) * NKMC  # floats per J^P group
+KM_SIZE = 4 * KM_BLOCK
+
+HEL1_TWO = (1, 1, -1, -1, 3, -3)
+HEL2 = (1, 0, 0, -1, 1, -1)
+
+# Clebsch-Gordan values <L 0; S 1/2 | 1/2 1/2> for 2S = 1..11, 2L = 2S-1, 2S+1, as tabulated by the
+# reference (RooDalitzAmplitude.cxx:96-107); the table's last-digit values are kept so couplings are
+# bit-identical (tests/test_model.py checks them against the Racah formula).
+C2 = ((1.0000000000000000e00, -5.7735026918962584e-01), (-5.7735026918962573e-01, 4.4721359549995765e-01),
+      (4.4721359549995754e-01, -3.7796447300922748e-01), (-3.7796447300922759e-01, 3.3333333333333659e-01),
+      (3.3333333333332898e-01, -3.0151134457775197e-01), (-3.0151134457772666e-01, 2.7735009811269257e-01))
+
+f32 = np.float32
+
+
+@lru_cache(maxsize=None)
+def clebsch(j1: int, m1: int, j2: int, m2: int, J: int, M: int) -> float:
+    """<j1/2 m1/2; j2/2 m2/2 | J/2 M/2> (all arguments doubled), Condon-Shortley phase, by the
+    Racah formula in exact rational arithmetic."""
+    if m1 + m2 != M or abs(m1) > j1 or abs(m2) > j2 or abs(M) > J:
+        return 0.0
+    if J < abs(j1 - j2) or J > j1 + j2 or (j1 + j2 + J) % 2 or (j1 + m1) % 2 or (j2 + m2) % 2:
+        return 0.0
+    f = math.factorial
+    a = (j1 + j2 - J) // 2
+    b = (j1 - m1) // 2
+    c = (j2 + m2) // 2
+    d = (J - j2 + m1) // 2
+    e = (J - j1 - m2) // 2
+    pref = Fraction((J + 1) * f((J + j1 - j2) // 2) * f((J - j1 + j2) // 2) * f(a), f((j1 + j2 + J) // 2 + 1))
+    pref *= Fraction(f((J + M) // 2) * f((J - M) // 2) * f((j1 - m1) // 2) * f((j1 + m1) // 2)
+                     * f((j2 - m2) // 2) * f((j2 + m2) // 2))
+    s = Fraction(0)
+    for k in range(0, a + 1):
+        if b - k < 0 or c - k < 0 or d + k < 0 or e + k < 0:
+            continue
+        s += Fraction((-1) ** k, f(k) * f(a - k) * f(b - k) * f(c - k) * f(d + k) * f(e + k))
+    if s == 0:
+        return 0.0
+    return float(math.copysign(math.sqrt(pref * s * s), s))
+
+
+# ------------------------------------------------------------------ model description
+@dataclasses.dataclass
+class Resonance:
+    """One entry of a resonance list.  chain: 'L' (Lambda* -> pK), 'Z' (Pc -> J/psi p).
+    couplings: names of the LS coupling parameters as (Re, Im) pairs (12 for 'L', 8 for 'Z').
+    extra: 'L': (scRe, scIm) names; 'Z' K-matrix pole: g1..g4 names; 'Z' K-matrix NR: (fsc,).
+    mass / width: parameter names or constants (for a K-matrix pole the width slot holds the
+    channel index used for the near-threshold mass shift)."""
+    chain: str
+    name: str
+    spin2: int
+    parity: int
+    type: int
+    mass: str | float
+    width: str | float
+    couplings: tuple
+    extra: tuple = ()
+
+
+@dataclasses.dataclass
+class Model:
+    lstar: list
+    pc: list
+    ffr: float = 3.0
+    ffb: float = 3.0
+    derived: dict = dataclasses.field(default_factory=dict)  # name -> callable(values) -> float
+
+    @property
+    def NR(self):
+        return len(self.lstar)
+
+    @property
+    def NZ(self):
+        return len(self.pc)
+
+    @property
+    def NX(self):
+        return 0
+
+    @property
+    def resonances(self):
+        return list(self.lstar) + list(self.pc)
+
+    def value(self, vals: dict, ref) -> float:
+        if isinstance(ref, (int, float)):
+            return float(ref)
+        if ref in self.derived:
+            return float(self.derived[ref](vals))
+        return float(vals[ref])
+
+    def parameter_names(self) -> list:
+        names = []
+        for r in self.resonances:
+            for ref in (*r.couplings, *r.extra, r.mass, r.width):
+                if isinstance(ref, str) and ref not in names and ref not in self.derived:
+                    names.append(ref)
+        return names
+
+
+def orbital_l(r: Resonance) -> int:
+    """Decay orbital angular momentum stored in the table (setup_paraList :3079-3112)."""
+    S = r.spin2 / 2.0
+    if r.chain == "L":
+        LR = int(S - 0.5)
+    else:
+        LR = max(int(S - 1.5), 0)
+    if ((-1) ** (LR + 1)) * r.parity < 0:
+        LR += 1
+    return LR
+
+
+def km_group(r: Resonance) -> int:
+    return (1 if r.spin2 == 3 else 0) + (2 if r.parity > 0 else 0)
+
+
+# ------------------------------------------------------------------ LS -> helicity couplings
+def _sqrt_f32(x: float) -> np.float32:
+    return np.sqrt(f32(x))
+
+
+def part_wave_lstar(lsc: list, J: int, lam2: int, lam3: int) -> complex:
+    """Lambda_b -> Lambda* J/psi helicity coupling from LS couplings (PartWaveCoff, all quantum
+    numbers doubled)."""
+    c = 0j
+    ib = 0
+    m1 = lam2 - lam3
+    for S in range(abs(J - 2), J + 3, 2):
+        for L in (S - 1, S + 1):
+            M = lsc[ib]
+            if abs(M) ** 2 < 1e-10:
+                ib += 1
+                continue
+            a = _sqrt_f32((L + 1.0) / 2.0)
+            ccg = f32(clebsch(J, lam2, 2, -lam3, S, m1))
+            pre = float(f32(a * ccg))
+            tmp = pre * C2[(S - 1) // 2][(L - S + 1) // 2] * M
+            if m1 < 0 and L > S:
+                tmp = -tmp
+            c += tmp
+            ib += 1
+    return c
+
+
+def part_wave_pc(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: int) -> complex:
+    """Lambda_b -> Pc K and Pc -> J/psi p helicity coupling from LS couplings (PartWaveCoffZ)."""
+    HB = 0j
+    SB = J
+    for LB in (SB - 1, SB + 1):
+        tmp = complex(C2[(SB - 1) // 2][(LB - SB + 1) // 2] * math.sqrt((LB + 1.0) / 2.0))
+        if LB > SB:
+            M = lsc[0]
+            if abs(M) ** 2 < 1e-10:
+                continue
+            tmp = tmp * M
+            if lamZ < 0:
+                tmp = -tmp
+        HB += tmp
+    ib = 1
+    c = 0j
+    m1 = lamPsi - lamp
+    for S in (1, 3):
+        for L in range(abs(J - S), J + S + 1, 2):
+            if ((-1) ** (L // 2 + 1)) * parity < 0:
+                continue
+            if S < abs(m1):
+                ib += 1
+                continue
+            ccg1 = f32(clebsch(2, lamPsi, 1, -lamp, S, m1))
+            M = lsc[ib]
+            if abs(M) ** 2 < 1e-10:
+                ib += 1
+                continue
+            a = _sqrt_f32((L + 1.0) / (J + 1.0))
+            if J == 1:
+                cg = C2[(S - 1) // 2][(L - S + 1) // 2]
+                if m1 < 0 and L > S:
+                    cg = -cg
+                ccg = f32(cg)
+            else:
+                ccg = f32(clebsch(L, 0, S, m1, J, m1))
+            pre = float(f32(f32(a * ccg) * ccg1))
+            c += pre * M
+            ib += 1
+    return c * HB
+
+
+def _pow_m1(e) -> float:
+    return 1.0 if int(round(e)) % 2 == 0 else -1.0
+
+
+@dataclasses.dataclass
+class ParamBlock:
+    data: np.ndarray  # float32 h_paraList
+    para_size: int
+    vamp_size: int
+    spline_size: int
+    NR: int
+    NZ: int
+    NX: int
+    ffr: float
+    ffb: float
+
+    @property
+    def kmcount(self):
+        return self.para_size + self.vamp_size + self.spline_size
+
+
+def build_param_block(model: Model, vals: dict, include: tuple | None = None) -> ParamBlock:
+    """The float parameter block for one parameter point (ConfigureCouplings + cu_init_data).
+    include: optional (Lambda* indices, Pc indices) whose couplings are kept (SetupCoupling);
+    the others are zeroed, as for per-resonance weights."""
+    res = model.resonances
+    table = np.zeros(NSET * len(res), f32)
+    vamp: list = []
+    galpha = [[] for _ in range(4)]
+    fscat = [[] for _ in range(4)]
+    for ir, r in enumerate(res):
+        q = table[ir * NSET:(ir + 1) * NSET]
+        q[0] = f32(model.value(vals, r.mass))
+        q[1] = f32(model.value(vals, r.width))
+        q[2] = r.spin2
+        q[3] = orbital_l(r)
+        q[4] = r.type
+        q[5] = r.parity
+        lsc = [complex(model.value(vals, r.couplings[2 * i]), model.value(vals, r.couplings[2 * i + 1]))
+               for i in range(len(r.couplings) // 2)]
+        keep = True
+        if include is not None:
+            keep = (ir in include[0]) if r.chain == "L" else ((ir - model.NR) in include[1])
+        if r.chain == "L":
+            S = f32(r.spin2) / f32(2)
+            sc = complex(model.value(vals, r.extra[0]), model.value(vals, r.extra[1]))
+            for k in range(2):
+                pp = _pow_m1(int(S - 1.5)) * r.parity if k == 0 else 1.0
+                for m in range(6):
+                    if r.spin2 == 1 and m >= 4:
+                        continue
+                    h2 = HEL2[m]
+                    a = part_wave_lstar(lsc, r.spin2, HEL1_TWO[m], h2 * 2) * pp
+                    a = a * _pow_m1(1 - h2)
+                    a = a * sc
+                    vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+        else:
+            S = r.spin2 / 2.0
+            for k in range(2):
+                for hpsi in (-1, 0, 1):
+                    for ihz in range(2):
+                        hz = -0.5 if ihz == 0 else 0.5
+                        for ihp in range(2):
+                            hp = -0.5 if ihp == 0 else 0.5
+                            if abs(hpsi - hp) > S:
+                                continue
+                            a = part_wave_pc(lsc, r.parity, r.spin2, int(hz * 2), hpsi * 2, int(hp * 2))
+                            a = a * _pow_m1(1 - ihp)
+                            vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+            if r.type == KMATRIX:
+                ik = km_group(r)
+                if q[0] > 0:
+                    galpha[ik] += [f32(model.value(vals, g)) for g in r.extra[:4]]
+                else:
+                    fscat[ik].append(f32(model.value(vals, r.extra[0])))
+            elif r.type not in (BREITWIGNER, NONRESONANT):
+                raise NotImplementedError(f"Pc lineshape type {r.type}")
+        if r.chain == "L" and r.type not in (BREITWIGNER, NONRESONANT):
+            raise NotImplementedError(f"Lambda* lineshape type {r.type}")
+    km = []
+    for ik in range(4):
+        g = galpha[ik][: NPMAX * NKMC]
+        if len(galpha[ik]) > NPMAX * NKMC:
+            raise ValueError("more than 4 K-matrix poles in one J^P group")
+        f = (fscat[ik] + [f32(0)] * (NKMC * NKMC))[: NKMC * NKMC]
+        for i in range(1, NKMC):
+            f[NKMC * i] = f[i]
+        km += g + [f32(0)] * (NPMAX * NKMC - len(g)) + f
+    data = np.concatenate([table, np.array(vamp, f32), np.array(km, f32)]).astype(f32)
+    return ParamBlock(data, len(table), len(vamp), 0, model.NR, model.NZ, 0, model.ffr, model.ffb)
+
+
+# ------------------------------------------------------------------ parameter files
+_FUNC_RE = re.compile(
+    r"^\s*(?P<name>[A-Za-z_][\w\.]*)\s*=\s*(?P<val>[-+\w\.]+)(?:\s*\+/-\s*(?P<err>[-+\w\.]+))?"
+    r"(?P<const>\s+C)?(?:\s+L\((?P<lo>[-+\w\.]+)\s*-\s*(?P<hi>[-+\w\.]+)\))?\s*$")
+
+
+def _num(s: str) -> float:
+    s = s.strip()
+    if s.upper() in ("INF", "+INF"):
+        return math.inf
+    if s.upper() == "-INF":
+        return -math.inf
+    return float(s)
+
+
+@dataclasses.dataclass
+class Param:
+    name: str
+    value: float
+    error: float | None = None
+    constant: bool = False
+    lo: float = -math.inf
+    hi: float = math.inf
+
+
+def read_func(text: str) -> dict:
+    """Parse the reference's parameter-file format (RooArgSet::readFromFile, e.g.
+    Fit_Jpsippi/func/yujie_test.func):  name = value [+/- error] [C] [L(lo - hi)]."""
+    out = {}
+    for line in text.splitlines():
+        line = line.split("//")[0].rstrip()
+        if not line.strip():
+            continue
+        m = _FUNC_RE.match(line)
+        if not m:
+            raise ValueError(f"cannot parse parameter line: {line!r}")
+        out[m["name"]] = Param(m["name"], _num(m["val"]), _num(m["err"]) if m["err"] else None,
+                               bool(m["const"]), _num(m["lo"]) if m["lo"] else -math.inf,
+                               _num(m["hi"]) if m["hi"] else math.inf)
+    return out
+
+
+def _fmt(x: float) -> str:
+    if math.isinf(x):
+        return "+INF" if x > 0 else "-INF"
+    return f"{x:.6g}"
+
+
+def write_func(params: dict) -> str:
+    lines = []
+    for name in sorted(params):
+        p = params[name]
+        s = f"{name} = {p.value:.8g}"
+        if p.error is not None:
+            s += f" +/- {p.error:.5g}"
+        if p.constant:
+            s += " C"
+        s += f" L({_fmt(p.lo)} - {_fmt(p.hi)})"
+        lines.append(s)
+    return "\n".join(lines) + "\n"
+
+
+@dataclasses.dataclass
+class Constraint:
+    """Flat-top two-sided Gaussian penalty (RooFGaussian::evaluate, src/RooFGaussian.cxx:60-75)."""
+    name: str
+    mean1: float
+    mean2: float
+    sigma1: float
+    sigma2: float
+    lo: float
+    hi: float
+
+    def penalty(self, x: float) -> float:
+        if x < self.mean1:
+            return 0.5 * ((x - self.mean1) / self.sigma1) ** 2
+        if x > self.mean2:
+            return 0.5 * ((x - self.mean2) / self.sigma2) ** 2
+        return 0.0
+
+
+def read_constraints(text: str) -> list:
+    """Constraint file: name mean1 mean2 err1 err2 lo hi per line (Fitter::ConstrMW, src/fit.cpp:33-79)."""
+    out = []
+    for line in text.splitlines():
+        f = line.split()
+        if len(f) < 7:
+            continue
+        out.append(Constraint(f[0], *map(float, f[1:7])))
+    return out
+
+
+def fcn(nll: float, nll_shift: float, alpha: float, constraints: list, vals: dict) -> float:
+    """Minuit FCN of the reference: (NLL - NLL_SHIFT) * alpha + sum of constraints
+    (src/fit.cpp:312-317), alpha = sum w / sum w^2 of the data weights (:201-220)."""
+    return (nll - nll_shift) * alpha + sum(c.penalty(vals[c.name]) for c in constraints if c.name in vals)

@@ -1,0 +1,65 @@
+"""GPU likelihood vs the FP64 oracle on identical seeded inputs (calls through the C ABI)."""
+import numpy as np
+import pytest
+
+from conftest import make_test_sample
+
+pytestmark = pytest.mark.gpu
+
+# FP64 on both sides: the tolerance covers summation-order differences only.
+NLL_TOL = 1e-6
+FX_RTOL = 1e-9
+
+CASES = [("small_kmatrix", 1500, 15000), ("small_bw", 1500, 15000), ("lstar_only", 1000, 10000),
+         ("kmatrix", 1200, 12000), ("full_bw", 800, 8000)]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from pwa_b200 import lib
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name,nd,nm", CASES)
+def test_nll_and_fx_match_oracle(ctx, oracle_mod, name, nd, nm):
+    mdl, vals, blk, smp = make_test_sample(name, nd, nm)
+    ctx.upload(smp)
+    r, fx = ctx.eval_nll(blk, want_fx=True)
+    v, s, ofx, ofxn = oracle_mod.nll(smp, blk)
+    rel = np.abs(fx - ofx) / np.maximum(np.abs(ofx), 1e-300)
+    assert np.max(rel) < FX_RTOL, (name, np.max(rel), int(np.argmax(rel)))
+    assert abs(r.nll - v) < NLL_TOL, (name, r.nll, v)
+    assert abs(r.sumint / s - 1) < 1e-12
+    assert r.n_nonpos == 0
+
+
+def test_amp2_matches_oracle(ctx, oracle_mod):
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    ctx.upload(smp)
+    a = ctx.amp2(blk)
+    o = oracle_mod.amp2(smp, blk)
+    assert np.max(np.abs(a - o) / o) < FX_RTOL
+
+
+def test_band_edges_and_ragged_sizes(ctx, oracle_mod):
+    """Band arguments at the edges (no band-1 events, -1 shift, bands covering everything) and
+    sizes not multiple of the tile/warp widths."""
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 700, 5013, seed=5)
+    for a, b in [(-1, 0), (0, 0), (smp.nda_smr1 - 1, smp.nda_fine), (smp.nda_smr1, smp.nda_fine),
+                 (smp.nda, 0), (-1, smp.nda_fine + 3), (37, 1)]:
+        ctx.upload(smp, a, b)
+        r, fx = ctx.eval_nll(blk, want_fx=True)
+        ofx, ofxn = oracle_mod.eval_fx(smp, blk, a, b)
+        v, s = oracle_mod.assemble_nll(smp, ofx, ofxn)
+        assert np.max(np.abs(fx - ofx) / np.abs(ofx)) < FX_RTOL, (a, b)
+        assert abs(r.nll - v) < NLL_TOL, (a, b)
+
+
+def test_repeated_calls_identical(ctx):
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    ctx.upload(smp)
+    a = ctx.eval_nll(blk).nll
+    b = ctx.eval_nll(blk).nll
+    assert a == b
