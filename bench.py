@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark: NLL evaluations per second of the coupled-channel Pc K-matrix model (6 Lambda*,
+12 Pc K-matrix entries) on 500k data + 5M efficiency-weighted MC events.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+One step = one evaluation of the unbinned NLL over the whole sample (data -log L plus the MC
+normalisation sum) for one parameter point, inputs resident in HBM.  Under torchrun each rank holds
+its own full-size event shard (weak scaling) and the three per-rank sums are all-reduced over NCCL
+every step.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "pwa-xib2jpsilambdak_b200"))
+
+METRIC = "NLL evals/s, 5M-event K-matrix model"
+WORKLOAD = {"name": "kmatrix", "n_data": 500_000, "n_mc": 5_000_000, "w_range": (0.2, 1.0)}
+CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------ helpers
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def required_bytes_per_event(model) -> tuple:
+    """Bytes of the reference SoA the model's amplitude reads per event (planes of d-functions for
+    spins the model does not use are not needed), and the full reference row (all planes)."""
+    ls = sorted({r.spin2 for r in model.lstar})
+    pcs = sorted({r.spin2 for r in model.pc})
+    ncm = max([4 if s == 1 else 6 for s in ls], default=0)
+    planes = 3 + 8 * ncm + sum(2 * (4 if s == 1 else 6) for s in ls)
+    if pcs:
+        planes += 96 + sum(2 * (8 if s == 1 else 12) for s in pcs)
+    full = 111 + (192 if model.NZ else 0)
+    return 4 * planes, 4 * full
+
+
+# ------------------------------------------------------------------------------ CPU side
+def cpu_reference_seconds(sample, block, reps: int = 2) -> float:
+    """Seconds per host_store_fx of the reference's own code built for host cores on `sample`."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    ref = O.RefHost(sample, block)
+    ref.store_fx(block)
+    t = time.perf_counter()
+    for _ in range(reps):
+        ref.store_fx(block)
+    return (time.perf_counter() - t) / reps
+
+
+def cpu_oracle_seconds(sample, block) -> float:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    t = time.perf_counter()
+    O.nll(sample, block)
+    return time.perf_counter() - t
+
+
+def cpu_sample_from_device(dsample, n_data: int, n_mc: int, seed: int = 5):
+    rng = np.random.default_rng(seed)
+    di = np.sort(rng.choice(dsample.nda, size=min(n_data, dsample.nda), replace=False))
+    mi = np.sort(rng.choice(dsample.nmc, size=min(n_mc, dsample.nmc), replace=False))
+    return dsample.to_host(di, mi)
+
+
+def reference_arm(args):
+    """--impl reference: the reference's own likelihood code (FP32, OpenMP over all host cores) on a
+    bounded sample of the workload, reported in evals/s of the full workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from pwa_b200 import configs, dataset as D, model as M
+    mdl, vals = configs.kmatrix()
+    block = M.build_param_block(mdl, vals)
+    L = O.ref_lib(block.NR, block.NZ, block.NX, build_if_missing=False)
+    if L is None:
+        print(json.dumps({"impl": "reference", "unavailable": "host build of the reference not found in oracle/_ref"}))
+        return 0
+    nd, nm = CPU_SAMPLE
+
+    def amp2(ang):
+        s = D.build_sample({k: v[:0] for k, v in ang.items()}, ang, np.ones(len(ang["mLk"])))
+        return O.RefHost(s, block).amp2s(block)
+
+    sample = D.make_sample(nd, nm, WORKLOAD["w_range"], 4242, amp2)
+    ref = O.RefHost(sample, block)
+    for _ in range(max(args.warmup, 1)):
+        ref.store_fx(block)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.store_fx(block)
+    dt = (time.perf_counter() - t0) / args.steps
+    scale = (WORKLOAD["n_data"] + WORKLOAD["n_mc"]) / (nd + nm)
+    value = 1.0 / (dt * scale)
+    cores = os.cpu_count()
+    out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * scale * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": "kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
+                                  "500k data + 5M MC", "parallelism": "host cores (OpenMP)"},
+           "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
+                            "sample": f"{nd} data + {nm} MC events per step, time scaled by {scale:.1f} to the "
+                                      f"full workload"},
+           "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# ------------------------------------------------------------------------------ GPU arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import torch.distributed as dist
+    from pwa_b200 import configs, gpu_sample, lib, model as M
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    mdl, vals = configs.kmatrix()
+    block = M.build_param_block(mdl, vals)
+    frac = 10 if args.small else 1
+    nd, nm = WORKLOAD["n_data"] // frac, WORKLOAD["n_mc"] // frac
+    t_gen = time.perf_counter()
+    sample = gpu_sample.generate(block, nd, nm, WORKLOAD["w_range"], seed=1000 + rank, device=local)
+    t_gen = time.perf_counter() - t_gen
+    ctx = lib.Context(local)
+    ctx.bind_device(sample)
+    ctx.set_timing(True)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    sums = torch.zeros(3, dtype=torch.float64, device=dev)
+
+    def step():
+        r = ctx.eval_nll(block)
+        if world > 1:
+            sums.copy_(torch.tensor([r.data_term, r.sumint, r.sum_noint], dtype=torch.float64))
+            dist.all_reduce(sums)
+        return r
+
+    for _ in range(max(args.warmup, 3)):
+        r = step()
+    # timed region: device time with CUDA events on the launching stream
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    seg_time = {}
+    kernel_ms = 0.0
+    launches = 0
+    for _ in range(args.steps):
+        r = step()
+        kernel_ms += ctx.last_kernel_ms()
+        launches += ctx.last_launches()
+        for kind, n, ms in ctx.segments():
+            t, _ = seg_time.get(kind, (0.0, n))
+            seg_time[kind] = (t + ms, n)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dev_ms = e0.elapsed_time(e1)
+    # end to end through the public API (host parameter block in, result out), wall clock
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    clocks = clk.stop()
+    if world > 1:
+        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, e2e_ms = t.tolist()
+        dist.barrier()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    value = world * args.steps / (dev_ms / 1e3)
+    e2e = world * args.steps / (e2e_ms / 1e3)
+    hbm, bf16, peak_kind = measured_peaks()
+    req_b, full_b = required_bytes_per_event(mdl)
+    names = {0: "k_unsmeared", 1: "k_smeared<20>", 2: "k_smeared<30>", 3: "k_smeared<150>"}
+    total_seg = sum(t for t, _ in seg_time.values())
+    shares = {names[k]: round(t / total_seg, 4) for k, (t, n) in seg_time.items()}
+    dom = max(seg_time, key=lambda k: seg_time[k][0])
+    dom_ms = seg_time[dom][0] / args.steps
+    dom_bytes = seg_time[dom][1] * req_b + (sample.nda * 4 if dom in (2, 3) else 0)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
+                                  f"{nd} data + {nm} MC events per GPU", "global_events": world * (nd + nm),
+                      "parallelism": f"dp{world} event shards, NCCL all-reduce of 3 sums per step",
+                      "l2": "inputs larger than L2 (events x 828 B >> 126 MB)", "precision": "plain FP64 path"},
+           "gpu_launches": launches,
+           "kernel_shares": shares,
+           "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                        "frac": achieved / hbm, "traffic": None,
+                        "note": f"algorithmic bytes = {req_b} B per event (planes the model reads) of the "
+                                f"{full_b} B reference row; peak {peak_kind}"},
+           "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(lib.load().pwa_point_table_bytes()),
+                   "d2h_bytes_per_step": 48},
+           "clocks": clocks, "setup_s": round(t_gen, 2)}
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            smp = cpu_sample_from_device(sample, *CPU_SAMPLE)
+            t_ref = cpu_reference_seconds(smp, block)
+            scale = (nd + nm) / smp.n
+            out["cpu_baseline"] = {"value": 1.0 / (t_ref * scale), "unit": "evals/s", "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": f"{smp.nda} data + {smp.nmc} MC events drawn from the bench sample; "
+                                             f"time x{scale:.0f} to the full workload"}
+            # parity on the same sample: this GPU path and the reference FP32 code vs the FP64 oracle
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import oracle as O
+            v_or, _, _, _ = O.nll(smp, block)
+            c2 = lib.Context(local)
+            c2.upload(smp)
+            v_gpu = c2.eval_nll(block).nll
+            c2.close()
+            v_ref, _ = O.RefHost(smp, block).store_fx(block)
+            out["parity"] = {"sample_events": smp.n, "dnll_gpu_vs_oracle": v_gpu - v_or,
+                             "dnll_reference_fp32_vs_oracle": v_ref - v_or}
+        except Exception as ex:  # the baseline is reported, never required for the GPU number
+            out["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": f"failed: {ex}"}
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

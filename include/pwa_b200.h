@@ -86,6 +86,18 @@ int pwa_ctx_amp2(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_
 /* Device time of the last pwa_ctx_eval_nll kernels in milliseconds (CUDA events). */
 double pwa_ctx_last_kernel_ms(pwa_ctx* ctx);
 
+/* The context's CUDA stream (cudaStream_t), for callers that bracket calls with their own events. */
+void* pwa_ctx_stream(pwa_ctx* ctx);
+
+/* Per-kernel timing: when on, pwa_ctx_eval_nll records a CUDA event after each event-class kernel.
+ * Classes (segments): 0 unsmeared, 1 20-offset smearing, 2 30-offset, 3 150-offset. */
+int pwa_ctx_set_timing(pwa_ctx* ctx, int on);
+int pwa_ctx_segment_count(pwa_ctx* ctx);
+int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double* last_ms);
+
+/* Bytes copied host to device per evaluation (the decoded parameter table). */
+int64_t pwa_point_table_bytes(void);
+
 /* Number of kernels launched by the last pwa_ctx_eval_nll. */
 int pwa_ctx_last_launches(pwa_ctx* ctx);
 
@@ -96,6 +108,23 @@ int pwa_ctx_last_launches(pwa_ctx* ctx);
  * K-matrix lineshapes. */
 int pwa_host_lineshapes(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
                         int NX, float FFR, float FFB, double mkp, double mz, double* lstar, double* pc);
+
+/* Synthetic events on the device (flat phase space, the reference ntuple maker's helicity angles,
+ * the filldlz basis), written into columns [col0, col0 + n) of device planes with stride n_size.
+ * Event t uses the counter-based random stream (seed, first_id + t).  data != 0 writes the data
+ * weight sentinel -1001, else a weight uniform in [w_lo, w_hi].  stream: cudaStream_t or NULL. */
+int pwa_generate_events(float* d_pp, float* d_pp1, float* d_pp2, int64_t n_size, int64_t col0, int64_t n,
+                        uint64_t seed, uint64_t first_id, float w_lo, float w_hi, int data, void* stream);
+
+/* Basis from given angles (device arrays [16][n]: mLk, mjpsiL, cosTheta_Lb, cosTheta_L, cosTheta_Jpsi,
+ * phiK, phiMu, Z_cosTheta_Lb, Z_cosTheta_Z, Z_cosTheta_Jpsi, Z_phiZ, Z_phiJpsi, Z_phiMu,
+ * cosTheta_Lambda, alpha_Mu, weight) into columns [0, n). */
+int pwa_basis_from_angles(const double* d_angles, int64_t n, float* d_pp, float* d_pp1, float* d_pp2,
+                          int64_t n_size, void* stream);
+
+/* Helicity angles from four-vectors in the Lambda_b rest frame (device [16][n]: p, K, mu+, mu-, each
+ * px py pz E) into device [15][n] (the first 15 rows of the layout above). */
+int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles, void* stream);
 
 const char* pwa_error_string(int code);
 const char* pwa_last_cuda_error(void);

@@ -59,6 +59,10 @@ struct pwa_ctx {
   int64_t fx_cap = 0;
   double last_ms = 0;
   int last_launches = 0;
+  // optional per-segment timing
+  int timing = 0;
+  std::vector<cudaEvent_t> seg_ev;
+  std::vector<double> seg_ms;
 };
 
 namespace {
@@ -175,6 +179,7 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   cudaFree(c->d_res);
   cudaFreeHost(c->h_res);
   cudaFree(c->d_fx);
+  for (auto e : c->seg_ev) cudaEventDestroy(e);
   if (c->e0) cudaEventDestroy(c->e0);
   if (c->e1) cudaEventDestroy(c->e1);
   if (c->st) cudaStreamDestroy(c->st);
@@ -254,9 +259,17 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
   PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   int launches = 0;
+  if (c->timing) {
+    while (c->seg_ev.size() < c->segs.size()) {
+      cudaEvent_t e;
+      PWA_CUDA(cudaEventCreate(&e));
+      c->seg_ev.push_back(e);
+    }
+  }
   for (size_t i = 0; i < c->segs.size(); ++i) {
     PWA_CUDA(launch_segment(ev, c->segs[i], c->d_table, c->d_parts + c->seg_off[i], h_fx ? c->d_fx : nullptr,
                             c->sm_count, c->st));
+    if (c->timing) PWA_CUDA(cudaEventRecord(c->seg_ev[i], c->st));
     ++launches;
   }
   PWA_CUDA(launch_finalize(c->d_parts, c->total_parts, sum_w_mc, sum_w_data, nll_shift, c->d_res, c->st));
@@ -268,6 +281,16 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
   float ms = 0;
   cudaEventElapsedTime(&ms, c->e0, c->e1);
   c->last_ms = ms;
+  if (c->timing) {
+    c->seg_ms.assign(c->segs.size(), 0.0);
+    cudaEvent_t prev = c->e0;
+    for (size_t i = 0; i < c->segs.size(); ++i) {
+      float m = 0;
+      cudaEventElapsedTime(&m, prev, c->seg_ev[i]);
+      c->seg_ms[i] = m;
+      prev = c->seg_ev[i];
+    }
+  }
   c->last_launches = launches;
   out->nll = c->h_res->nll;
   out->sumint = c->h_res->sumint;
@@ -310,6 +333,25 @@ int pwa_host_lineshapes(const float* pl, int para_size, int vamp_size, int splin
 }
 
 double pwa_ctx_last_kernel_ms(pwa_ctx* c) { return c ? c->last_ms : 0.0; }
+void* pwa_ctx_stream(pwa_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int pwa_ctx_set_timing(pwa_ctx* c, int on) {
+  if (!c) return PWA_E_ARG;
+  c->timing = on ? 1 : 0;
+  return PWA_OK;
+}
+
+int pwa_ctx_segment_count(pwa_ctx* c) { return c ? (int)c->segs.size() : 0; }
+
+int pwa_ctx_segment_info(pwa_ctx* c, int i, int* kind, int64_t* events, double* last_ms) {
+  if (!c || i < 0 || i >= (int)c->segs.size()) return PWA_E_ARG;
+  if (kind) *kind = c->segs[i].kind;
+  if (events) *events = c->segs[i].end - c->segs[i].begin;
+  if (last_ms) *last_ms = (i < (int)c->seg_ms.size()) ? c->seg_ms[i] : 0.0;
+  return PWA_OK;
+}
+
+int64_t pwa_point_table_bytes(void) { return (int64_t)sizeof(PointTable); }
 int pwa_ctx_last_launches(pwa_ctx* c) { return c ? c->last_launches : 0; }
 
 }  // extern "C"

@@ -74,7 +74,7 @@ def dfun(beta, j, m, n):
     k0 = max(0, mpn)
     kq = np.full(b.shape, k0 + jpm)
     kq = kq + np.where(beta[gen] > pi, mpn, 0)
-    q = np.where(kq % 2 == 1, -1.0, 1.0)
+    q = np.where(np.fmod(kq, 2) == 1, -1.0, 1.0)  # C remainder: a negative kq gives q = +1
     cx = 2 * k0 - mpn
     sx = jpm + jpn - 2 * k0
     r = np.zeros_like(b)

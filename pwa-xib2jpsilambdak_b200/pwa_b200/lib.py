@@ -13,8 +13,10 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "libpwa_b200.so"
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
-            "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches",
-            "pwa_host_lineshapes", "pwa_error_string", "pwa_last_cuda_error"]
+            "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
+            "pwa_ctx_set_timing", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_point_table_bytes",
+            "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
+            "pwa_error_string", "pwa_last_cuda_error"]
 
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
@@ -51,8 +53,20 @@ def load() -> C.CDLL:
         L.pwa_ctx_last_kernel_ms.restype = C.c_double
         L.pwa_ctx_last_kernel_ms.argtypes = [C.c_void_p]
         L.pwa_ctx_last_launches.argtypes = [C.c_void_p]
+        L.pwa_ctx_set_timing.argtypes = [C.c_void_p, C.c_int]
+        L.pwa_ctx_segment_count.argtypes = [C.c_void_p]
+        L.pwa_ctx_segment_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                           C.POINTER(C.c_double)]
+        L.pwa_point_table_bytes.restype = C.c_int64
+        L.pwa_ctx_stream.restype = C.c_void_p
+        L.pwa_ctx_stream.argtypes = [C.c_void_p]
         L.pwa_host_lineshapes.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                           C.c_float, C.c_double, C.c_double, _dp, _dp]
+        L.pwa_generate_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
+                                          C.c_uint64, C.c_uint64, C.c_float, C.c_float, C.c_int, C.c_void_p]
+        L.pwa_basis_from_angles.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                            C.c_void_p]
+        L.pwa_angles_from_vectors.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.pwa_error_string.restype = C.c_char_p
         L.pwa_last_cuda_error.restype = C.c_char_p
         _lib = L
@@ -78,6 +92,7 @@ class Context:
         check(self.L.pwa_ctx_create(device, C.byref(h)), "pwa_ctx_create")
         self.h = h
         self.sample = None
+        self.n = 0
 
     def close(self):
         if self.h:
@@ -103,6 +118,25 @@ class Context:
         check(self.L.pwa_ctx_upload_events(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n, sample.n_size,
                                            sample.nda, a, b), "pwa_ctx_upload_events")
         self.sample = sample
+        self.n = sample.n
+
+    def bind_device(self, dsample, nda_smr: int | None = None, nda_fine: int | None = None):
+        """Use a DeviceSample's torch-owned planes (borrowed; the sample must outlive the binding)."""
+        a, b = dsample.reference_band_args()
+        a = a if nda_smr is None else nda_smr
+        b = b if nda_fine is None else nda_fine
+        check(self.L.pwa_ctx_set_device_events(self.h, dsample.pp.data_ptr(), dsample.pp1.data_ptr(),
+                                               dsample.pp2.data_ptr(), dsample.sw.data_ptr(), dsample.n,
+                                               dsample.n_size, dsample.nda, a, b), "pwa_ctx_set_device_events")
+        self.sample = dsample
+        self.n = dsample.n
+
+    def bind_planes(self, pp, pp1, pp2, sw, n: int, n_size: int, nda: int = 0, nda_smr: int = -1, nda_fine: int = 0):
+        """Use device planes given as torch tensors (borrowed)."""
+        check(self.L.pwa_ctx_set_device_events(self.h, pp.data_ptr(), pp1.data_ptr(), pp2.data_ptr(), sw.data_ptr(),
+                                               n, n_size, nda, nda_smr, nda_fine), "pwa_ctx_set_device_events")
+        self.sample = None
+        self.n = n
 
     def eval_nll(self, block, nll_shift: float = 1e7, want_fx: bool = False):
         s = self.sample
@@ -115,12 +149,26 @@ class Context:
         return (r, fx) if want_fx else r
 
     def amp2(self, block) -> np.ndarray:
-        s = self.sample
         pl = np.ascontiguousarray(block.data, np.float32)
-        out = np.zeros(s.n, np.float64)
+        out = np.zeros(self.n, np.float64)
         check(self.L.pwa_ctx_amp2(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR,
                                   block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp)), "pwa_ctx_amp2")
         return out
+
+    def set_timing(self, on: bool = True):
+        check(self.L.pwa_ctx_set_timing(self.h, int(on)), "pwa_ctx_set_timing")
+
+    def segments(self) -> list:
+        """[(kind, events, last_ms)] of the event-class kernels of the last evaluation."""
+        out = []
+        for i in range(self.L.pwa_ctx_segment_count(self.h)):
+            k, n, ms = C.c_int(), C.c_int64(), C.c_double()
+            check(self.L.pwa_ctx_segment_info(self.h, i, C.byref(k), C.byref(n), C.byref(ms)), "segment_info")
+            out.append((k.value, n.value, ms.value))
+        return out
+
+    def stream(self) -> int:
+        return self.L.pwa_ctx_stream(self.h) or 0
 
     def last_kernel_ms(self) -> float:
         return self.L.pwa_ctx_last_kernel_ms(self.h)

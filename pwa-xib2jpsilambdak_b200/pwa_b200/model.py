@@ -70,6 +70,98 @@ def clebsch(j1: int, m1: int, j2: int, m2: int, J: int, M: int) -> float:
     return float(math.copysign(math.sqrt(pref * s * s), s))
 
 
+def _orthogonal_vector(n: int, vectors: list) -> list:
+    """Generalised cross product of n-1 vectors of dimension n, accumulated over permutations in the
+    order of EvtGen's EvtOrthogVector (src/EvtOrthogVector.cpp:31-127)."""
+    orth = [0.0] * n
+    holder = [0] * n
+
+    def sign_of_holder() -> int:
+        t = list(holder)
+        swaps = 0
+        for i in range(n - 1):
+            for j in range(i + 1, n):
+                if t[i] > t[j]:
+                    t[i], t[j] = t[j], t[i]
+                    swaps += 1
+        return -1 if swaps % 2 else 1
+
+    def product() -> float:
+        a = 1.0
+        for i in range(1, n):
+            a *= vectors[i - 1][holder[i]]
+        return a
+
+    def rec(dim: int, invect: list):
+        if dim == 2:
+            holder[0], holder[1] = invect[0], invect[1]
+            sign = sign_of_holder()
+            orth[holder[0]] += product() * sign
+            holder[0], holder[1] = invect[1], invect[0]
+            orth[holder[0]] -= product() * sign
+            return
+        temp = invect + invect
+        for i in range(dim):
+            holder[dim - 1] = temp[dim - 1 + i]
+            rec(dim - 1, temp[i:i + dim - 1])
+
+    rec(n, list(range(n)))
+    return orth
+
+
+@lru_cache(maxsize=None)
+def _cg_table(j1: int, j2: int) -> dict:
+    """Clebsch-Gordan coefficients for fixed j1, j2 (doubled) built as EvtGen's EvtCGCoefSingle does
+    (src/EvtCGCoefSingle.cpp:36-117): highest weight per J by orthogonalisation, then the lowering
+    recursion with float square roots.  The float roots leave ~1e-8 relative deviations from the exact
+    values; the reference's helicity couplings contain them, so they are reproduced."""
+    Jmax, Jmin = j1 + j2, abs(j1 - j2)
+    lenmax = min(j1, j2) + 1
+
+    def length(M):
+        return min(((j1 + j2) - abs(M)) // 2 + 1, lenmax)
+
+    def mmin(M):
+        return max(M - j2, -j1)
+
+    tab = {}
+
+    def cg(J, M, m1):
+        return tab[(J, M)][(m1 - mmin(M)) // 2]
+
+    for J in range(Jmax, Jmin - 1, -2):
+        for M in range(J, -J - 1, -2):
+            tab[(J, M)] = [0.0] * length(M)
+        if J == Jmax:
+            tab[(J, J)][0] = 1.0
+        else:
+            n = (Jmax - J) // 2 + 1
+            vectors = [[tab[(Jmax - 2 * i, J)][k] for k in range(n)] for i in range(n - 1)]
+            orth = _orthogonal_vector(n, vectors)
+            sign = -1 if orth[n - 1] < 0 else 1
+            tab[(J, J)] = [sign * orth[k] for k in range(n)]
+        for M in range(J - 2, -J - 1, -2):
+            lo = mmin(M)
+            for m1 in range(lo, lo + 2 * length(M), 2):
+                m2 = M - m1
+                acc = 0.0
+                if m1 + 2 <= j1:
+                    acc += 0.5 * float(np.sqrt(f32(j1 * (j1 + 2) - (m1 + 2) * m1))) * cg(J, M + 2, m1 + 2)
+                if m2 + 2 <= j2:
+                    acc += 0.5 * float(np.sqrt(f32(j2 * (j2 + 2) - (m2 + 2) * m2))) * cg(J, M + 2, m1)
+                acc /= 0.5 * float(np.sqrt(f32(J * (J + 2) - (M + 2) * M)))
+                tab[(J, M)][(m1 - lo) // 2] = acc
+    return tab
+
+
+def cg_evtgen(j1: int, j2: int, J: int, M: int, m1: int, m2: int) -> float:
+    """EvtCGCoefSingle(j1, j2).coef(J, M, j1, j2, m1, m2), all arguments doubled."""
+    if m1 + m2 != M or abs(M) > J or J > j1 + j2 or J < abs(j1 - j2) or abs(m1) > j1 or abs(m2) > j2:
+        raise ValueError((j1, j2, J, M, m1, m2))
+    t = _cg_table(j1, j2)
+    return t[(J, M)][(m1 - max(M - j2, -j1)) // 2]
+
+
 # ------------------------------------------------------------------ model description
 @dataclasses.dataclass
 class Resonance:
@@ -163,7 +255,7 @@ def part_wave_lstar(lsc: list, J: int, lam2: int, lam3: int) -> complex:
                 ib += 1
                 continue
             a = _sqrt_f32((L + 1.0) / 2.0)
-            ccg = f32(clebsch(J, lam2, 2, -lam3, S, m1))
+            ccg = f32(cg_evtgen(J, 2, S, m1, lam2, -lam3))
             pre = float(f32(a * ccg))
             tmp = pre * C2[(S - 1) // 2][(L - S + 1) // 2] * M
             if m1 < 0 and L > S:
@@ -197,7 +289,7 @@ def part_wave_pc(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: i
             if S < abs(m1):
                 ib += 1
                 continue
-            ccg1 = f32(clebsch(2, lamPsi, 1, -lamp, S, m1))
+            ccg1 = f32(cg_evtgen(2, 1, S, m1, lamPsi, -lamp))
             M = lsc[ib]
             if abs(M) ** 2 < 1e-10:
                 ib += 1
@@ -209,7 +301,7 @@ def part_wave_pc(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: i
                     cg = -cg
                 ccg = f32(cg)
             else:
-                ccg = f32(clebsch(L, 0, S, m1, J, m1))
+                ccg = f32(cg_evtgen(L, S, J, m1, 0, m1))
             pre = float(f32(f32(a * ccg) * ccg1))
             c += pre * M
             ib += 1
