@@ -126,6 +126,31 @@ int pwa_basis_from_angles(const double* d_angles, int64_t n, float* d_pp, float*
  * px py pz E) into device [15][n] (the first 15 rows of the layout above). */
 int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles, void* stream);
 
+/* Allocation-free likelihood evaluation.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory while they evaluate the likelihood -- for
+ * example a fit running in a process whose GPU memory is already handed to another framework's
+ * caching allocator, where a further cudaMalloc fails or fragments that pool, or a job with a fixed
+ * device-memory budget on a shared node.  Inputs (the event planes, same layout and band arguments
+ * as pwa_ctx_set_device_events, and the host parameter block) and the output are the caller's; all
+ * scratch of the evaluation lives in a fixed device array of PWA_NOALLOC_SCRATCH_BYTES inside the
+ * library, present on every GPU that loads the library until the process exits.  The call makes no
+ * cudaMalloc, cudaFree or other allocating call.
+ *
+ * Limits: at most PWA_NOALLOC_MAX_EVENTS events (larger samples return PWA_E_SIZE).  All calls share
+ * the array, which keeps the last call's contents; calls that overlap on the GPU race on it (calls
+ * from threads of one process are serialised inside the library).  The first call on a device
+ * resolves the array's device address for that device; make that first call before any stream
+ * capture.  Work is queued on `stream` (cudaStream_t, NULL for the default stream) and the call
+ * returns when the result is on the host. */
+#define PWA_NOALLOC_MAX_EVENTS (1 << 20)
+#define PWA_NOALLOC_SCRATCH_BYTES 4350464
+int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* d_pp1, const float* d_pp2, const float* d_sw,
+                         int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr, int64_t nda_fine,
+                         const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                         int NX, float FFR, float FFB, double sum_w_mc, double sum_w_data, double nll_shift,
+                         void* stream, pwa_result* out);
+
 const char* pwa_error_string(int code);
 const char* pwa_last_cuda_error(void);
 
