@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
+    ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
     return ap.parse_args()
 
 
@@ -218,6 +219,7 @@ def main():
     ctx = lib.Context(local)
     ctx.bind_device(sample)
     ctx.set_timing(True)
+    ctx.set_lineshape_tables(not args.exact)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     sums = torch.zeros(3, dtype=torch.float64, device=dev)
 
@@ -271,7 +273,7 @@ def main():
     e2e = world * args.steps / (e2e_ms / 1e3)
     hbm, bf16, peak_kind = measured_peaks()
     req_b, full_b = required_bytes_per_event(mdl)
-    names = {0: "k_unsmeared", 1: "k_smeared<20>", 2: "k_smeared<30>", 3: "k_smeared<150>"}
+    names = {0: "k_unsmeared", 1: "k_smeared<20>", 2: "k_smeared<30>", 3: "k_smeared<150>", -1: "k_build_tables"}
     total_seg = sum(t for t, _ in seg_time.values())
     shares = {names[k]: round(t / total_seg, 4) for k, (t, n) in seg_time.items()}
     dom = max(seg_time, key=lambda k: seg_time[k][0])
@@ -284,7 +286,9 @@ def main():
            "config": {"workload": f"kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
                                   f"{nd} data + {nm} MC events per GPU", "global_events": world * (nd + nm),
                       "parallelism": f"dp{world} event shards, NCCL all-reduce of 3 sums per step",
-                      "l2": "inputs larger than L2 (events x 828 B >> 126 MB)", "precision": "plain FP64 path"},
+                      "l2": "inputs larger than L2 (events x 828 B >> 126 MB)", "precision": "plain FP64 path",
+                      "lineshapes": "exact K-matrix solves" if args.exact else "FP64 K-matrix tables, exact near "
+                                                                               "thresholds"},
            "gpu_launches": launches,
            "kernel_shares": shares,
            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -95,6 +95,11 @@ int pwa_ctx_set_timing(pwa_ctx* ctx, int on);
 int pwa_ctx_segment_count(pwa_ctx* ctx);
 int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double* last_ms);
 
+/* K-matrix lineshape tables (default on): each evaluation first tabulates the exact FP64 K-matrix
+ * outputs on a 10 keV m(J/psi p) grid and interpolates them (6-point Lagrange), evaluating exactly
+ * near thresholds, branch switches and pole clamps.  Off: every lookup solves the K-matrix. */
+int pwa_ctx_set_lineshape_tables(pwa_ctx* ctx, int on);
+
 /* Bytes copied host to device per evaluation (the decoded parameter table). */
 int64_t pwa_point_table_bytes(void);
 
@@ -144,7 +149,7 @@ int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles
  * capture.  Work is queued on `stream` (cudaStream_t, NULL for the default stream) and the call
  * returns when the result is on the host. */
 #define PWA_NOALLOC_MAX_EVENTS (1 << 20)
-#define PWA_NOALLOC_SCRATCH_BYTES 4350464
+#define PWA_NOALLOC_SCRATCH_BYTES 4718592 /* 4.5 MiB */
 int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* d_pp1, const float* d_pp2, const float* d_sw,
                          int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr, int64_t nda_fine,
                          const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,

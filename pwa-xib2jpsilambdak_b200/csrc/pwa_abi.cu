@@ -59,6 +59,10 @@ struct pwa_ctx {
   int64_t fx_cap = 0;
   double last_ms = 0;
   int last_launches = 0;
+  // K-matrix lineshape tables (on by default)
+  int use_tables = 1;
+  cplx* d_tab = nullptr;
+  unsigned char* d_tab_flags = nullptr;
   // optional per-segment timing
   int timing = 0;
   std::vector<cudaEvent_t> seg_ev;
@@ -179,6 +183,8 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   cudaFree(c->d_res);
   cudaFreeHost(c->h_res);
   cudaFree(c->d_fx);
+  cudaFree(c->d_tab);
+  cudaFree(c->d_tab_flags);
   for (auto e : c->seg_ev) cudaEventDestroy(e);
   if (c->e0) cudaEventDestroy(c->e0);
   if (c->e1) cudaEventDestroy(c->e1);
@@ -256,9 +262,18 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
     c->fx_cap = c->n;
   }
   EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  if (c->use_tables) {
+    if (!c->d_tab) PWA_CUDA(cudaMalloc(&c->d_tab, (size_t)4 * TAB_NODES * TAB_SLOTS * sizeof(cplx)));
+    if (!c->d_tab_flags) PWA_CUDA(cudaMalloc(&c->d_tab_flags, (size_t)4 * TAB_NODES));
+    attach_tables(c->h_table, c->d_tab, c->d_tab_flags);
+  }
   PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   int launches = 0;
+  if (c->h_table->tab.enabled) {
+    PWA_CUDA(launch_build_tables(c->d_table, TAB_NODES, c->sm_count, c->st));
+    launches += 2;
+  }
   if (c->timing) {
     while (c->seg_ev.size() < c->segs.size()) {
       cudaEvent_t e;
@@ -338,6 +353,12 @@ void* pwa_ctx_stream(pwa_ctx* c) { return c ? (void*)c->st : nullptr; }
 int pwa_ctx_set_timing(pwa_ctx* c, int on) {
   if (!c) return PWA_E_ARG;
   c->timing = on ? 1 : 0;
+  return PWA_OK;
+}
+
+int pwa_ctx_set_lineshape_tables(pwa_ctx* c, int on) {
+  if (!c) return PWA_E_ARG;
+  c->use_tables = on ? 1 : 0;
   return PWA_OK;
 }
 

@@ -16,6 +16,8 @@
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "pwa_kernels.cuh"
 
@@ -23,6 +25,13 @@ namespace pwa {
 
 // Resolution offsets in units of the mass resolution (reference data, Resonances.h:31-54).
 #include "smear_tables.inc"
+
+#ifndef PWA_SMEAR_MIN_BLOCKS
+#define PWA_SMEAR_MIN_BLOCKS 2
+#endif
+#ifndef PWA_UNSMEARED_MIN_BLOCKS
+#define PWA_UNSMEARED_MIN_BLOCKS 4
+#endif
 
 constexpr int TILE = 32;          // events per smeared tile
 constexpr int SMEAR_THREADS = 256;
@@ -33,55 +42,103 @@ constexpr int MAX_GROUP_ENTRIES = 8;
 __device__ __forceinline__ double ldf(const float* p, int64_t i) { return (double)__ldg(p + i); }
 
 // ------------------------------------------------------------------------------- lineshapes
-__host__ __device__ inline cplx lstar_lineshape(const LstarEntry& L, double mkp, double ffr, double ffb) {
-  // Breit-Wigner (BW_AMP, cu_DPFPropogator.cu:248-314) with hoisted constants.
+// Quantities of one event mass that every lineshape at that mass shares: two-body momenta and
+// 1/sqrt of the Blatt-Weisskopf polynomials for each barrier order L in use.  Each resonance then
+// costs one division (its Breit-Wigner denominator) and no square root.
+struct LstarKin {
+  double mkp, inv_mkp, s, pR, pSP, pBm;
+  double rsR[6], rsB[6];
+};
+struct PcKin {
+  double mz, inv_mz, s, pR, pBm;
+  double rsR[6], rsB[6];
+};
+
+__host__ __device__ inline void fill_rs(double* rs, int mask, double r, double p) {
+  const double z = sq(r * p);
+#pragma unroll
+  for (int L = 1; L <= 5; ++L) rs[L] = (mask >> L & 1) ? 1.0 / sqrt(bw_poly(L, z)) : 1.0;
+  rs[0] = 1.0;
+}
+
+__host__ __device__ inline LstarKin lstar_kin(const PointTable& T, double mkp) {
+  LstarKin k;
+  k.mkp = mkp;
+  k.inv_mkp = 1.0 / mkp;
+  k.s = mkp * mkp;
+  k.pR = two_body_p(mkp, M_P, M_K);
+  k.pSP = T.needs_sigma_pi ? two_body_p(mkp, PWA_F(1.18937f), PWA_F(0.13957018f)) : 0.0;
+  const double pB = two_body_p(M_LB, M_JPSI, mkp);
+  k.pBm = pB / M_LB;
+  fill_rs(k.rsR, T.lmask_lstar_R, T.ffr, k.pR);
+  fill_rs(k.rsB, T.lmask_lstar_B, T.ffb, pB);
+  return k;
+}
+
+__host__ __device__ inline PcKin pc_kin(const PointTable& T, double mz) {
+  PcKin k;
+  k.mz = mz;
+  k.inv_mz = 1.0 / mz;
+  k.s = mz * mz;
+  k.pR = two_body_p(mz, M_P, M_JPSI);
+  const double pB = two_body_p(M_LB, M_K, mz);
+  k.pBm = pB / M_LB;
+  fill_rs(k.rsR, T.lmask_pc_R, T.ffr, k.pR);
+  fill_rs(k.rsB, T.lmask_pc_B, T.ffb, pB);
+  return k;
+}
+
+// Lambda* Breit-Wigner times the Lambda_b -> Lambda* J/psi barrier (BW_AMP, cu_DPFPropogator.cu:248-314;
+// BTerm :155-181) with the parameter-only constants of the point table.
+__host__ __device__ inline cplx lstar_lineshape(const LstarEntry& L, const LstarKin& k) {
   cplx bw = mk(1, 0);
   if (L.type == LT_BW) {
-    const double pR = two_body_p(mkp, M_P, M_K);
     if (L.branch == 2) {
-      bw = mk(ipow(pR / L.pR0, L.LR), 0);
+      bw = mk(ipow(k.pR * L.inv_pR0, L.LR), 0);
     } else if (L.branch == 4) {
       bw = mk(0, 0);
     } else {
-      double FR = 1.0, gamma = L.g_r, pR0 = L.pR0;
+      double FR = 1.0, gamma = L.g_r, ratio;
       if (L.branch == 0) {
-        FR = barrier_ratio_pre(ffr, L.LR, pR, L.polyR0);
-        gamma = L.g_r * ipow(pR / pR0, 2 * L.LR + 1) * (L.m_r / mkp) * FR * FR;
+        FR = L.sqrt_polyR0 * k.rsR[L.LR];
+        ratio = k.pR * L.inv_pR0;
+        gamma = L.g_r * ipow(ratio, 2 * L.LR + 1) * (L.m_r * k.inv_mkp) * FR * FR;
       } else if (L.branch == 1) {
-        const double pSP = two_body_p(mkp, PWA_F(1.18937f), PWA_F(0.13957018f));
-        pR0 = L.pR0_sp;
-        gamma = L.g_r * ipow(pR / pR0, 2 * L.LR + 1) * (L.m_r / mkp);
-        gamma += PWA_F(0.0505f) * ipow(pSP / pR0, 2 * L.LR + 1) * (L.m_r / mkp);
+        ratio = k.pR * L.inv_pR0_sp;
+        gamma = L.g_r * ipow(ratio, 2 * L.LR + 1) * (L.m_r * k.inv_mkp);
+        gamma += PWA_F(0.0505f) * ipow(k.pSP * L.inv_pR0_sp, 2 * L.LR + 1) * (L.m_r * k.inv_mkp);
       } else {  // branch 3: m_r in [1.43, pK threshold]
-        FR = barrier_ratio_pre(ffr, L.LR, pR, L.polyR0);
+        FR = L.sqrt_polyR0 * k.rsR[L.LR];
+        ratio = k.pR * L.inv_pR0;
       }
-      const double factor = FR * ipow(pR / pR0, L.LR) * L.norm;
-      bw = factor * breit_wigner(L.m_r, gamma, mkp * mkp);
+      const double factor = FR * ipow(ratio, L.LR) * L.norm;
+      const double de2 = L.m_r * L.m_r - k.s, gm = gamma * L.m_r;
+      const double f = factor / (de2 * de2 + gm * gm);
+      bw = mk(de2 * f, gm * f);
     }
   }
-  // Lambda_b -> Lambda* J/psi barrier (BTerm, cu_DPFPropogator.cu:155-181).
-  const double pB = two_body_p(M_LB, M_JPSI, mkp);
-  const double bt = barrier_ratio_pre(ffb, L.LB, pB, L.polyB0) * ipow(pB / M_LB, L.LB) * L.lb_scale;
+  const double bt = (L.LB ? L.sqrt_polyB0 * k.rsB[L.LB] : 1.0) * ipow(k.pBm, L.LB) * L.lb_scale;
   return bw * bt;
 }
 
-__host__ __device__ inline double pc_barrier(const PcEntry& Z, double mz, double ffb) {
-  // BTermZ (cu_DPFPropogator.cu:183-203).
-  const double pB = two_body_p(M_LB, M_K, mz);
-  const double F = Z.pB0_event ? 1.0 : barrier_ratio_pre(ffb, Z.LB, pB, Z.polyB0);
-  return F * ipow(pB / M_LB, Z.LB);
+// Lambda_b -> Pc K barrier (BTermZ, cu_DPFPropogator.cu:183-203).
+__host__ __device__ inline double pc_barrier(const PcEntry& Z, const PcKin& k) {
+  const double F = (Z.pB0_event || Z.LB == 0) ? 1.0 : Z.sqrt_polyB0 * k.rsB[Z.LB];
+  return F * ipow(k.pBm, Z.LB);
 }
 
-__host__ __device__ inline cplx pc_bw(const PcEntry& Z, double mz, double ffr) {
-  // BW_AMPZ (cu_DPFPropogator.cu:316-336).
-  const double pR = two_body_p(mz, M_P, M_JPSI);
+// Pc Breit-Wigner (BW_AMPZ, cu_DPFPropogator.cu:316-336).
+__host__ __device__ inline cplx pc_bw(const PcEntry& Z, const PcKin& k) {
   double FR = 1.0, gamma = Z.g_r, ratio = 1.0;
   if (Z.bw_above) {
-    FR = barrier_ratio_pre(ffr, Z.LR, pR, Z.polyR0);
-    ratio = pR / Z.pR0;
-    gamma = Z.g_r * ipow(ratio, 2 * Z.LR + 1) * (Z.m_r / mz) * FR * FR;
+    FR = Z.sqrt_polyR0 * k.rsR[Z.LR];
+    ratio = k.pR * Z.inv_pR0;
+    gamma = Z.g_r * ipow(ratio, 2 * Z.LR + 1) * (Z.m_r * k.inv_mz) * FR * FR;
   }
-  return (FR * ipow(ratio, Z.LR) * Z.norm) * breit_wigner(Z.m_r, gamma, mz * mz);
+  const double factor = FR * ipow(ratio, Z.LR) * Z.norm;
+  const double de2 = Z.m_r * Z.m_r - k.s, gm = gamma * Z.m_r;
+  const double f = factor / (de2 * de2 + gm * gm);
+  return mk(de2 * f, gm * f);
 }
 
 // One J^P group of the coupled-channel K-matrix at mass mz (Default_KMatrix,
@@ -151,21 +208,60 @@ __host__ __device__ inline void km_solve(const KmGroup& G, double mz, double ffb
   for (int i = 0; i < NKMC; ++i) out[G.npole + i] = T[i] * (ms[0] * na);
 }
 
-// Lineshape (with production barrier) of every entry of Pc group g at mass mz.
-__device__ __forceinline__ void pc_group_lineshapes(const PointTable& T, int g, double mz, cplx* raw) {
+// K-matrix outputs of group ik at mz from the per-point table (6-point Lagrange on the uniform grid);
+// false when mz is in a guard interval or too close to the grid ends.
+__device__ __forceinline__ bool table_lookup(const LineTables& tab, int ik, int nout, double mz, cplx* out) {
+  if (!tab.enabled) return false;
+  const double x = (mz - tab.m_lo) * tab.inv_h;
+  const double fj = floor(x);
+  if (!(fj >= 2.0 && fj + 3.0 < (double)tab.n_nodes)) return false;
+  const int j = (int)fj;
+  if (tab.bad[ik][j]) return false;
+  const double t = x - fj;
+  // Lagrange weights for nodes j-2 .. j+3 (denominators -120, 24, -12, 12, -24, 120)
+  const double d0 = t + 2.0, d1 = t + 1.0, d2 = t, d3 = t - 1.0, d4 = t - 2.0, d5 = t - 3.0;
+  const double p01 = d0 * d1, p012 = p01 * d2, p0123 = p012 * d3, p01234 = p0123 * d4;
+  const double s5 = d5, s45 = d4 * s5, s345 = d3 * s45, s2345 = d2 * s345, s12345 = d1 * s2345;
+  const double w[6] = {s12345 * (-1.0 / 120.0), d0 * s2345 * (1.0 / 24.0), p01 * s345 * (-1.0 / 12.0),
+                       p012 * s45 * (1.0 / 12.0), p0123 * s5 * (-1.0 / 24.0), p01234 * (1.0 / 120.0)};
+  const cplx* base = tab.data[ik] + (size_t)(j - 2) * TAB_SLOTS;
+  for (int o = 0; o < nout; ++o) {
+    cplx acc = mk(0, 0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const cplx v = base[k * TAB_SLOTS + o];
+      acc.re = fma(w[k], v.re, acc.re);
+      acc.im = fma(w[k], v.im, acc.im);
+    }
+    out[o] = acc;
+  }
+  return true;
+}
+
+// Exact solve for lookups the table cannot serve; kept out of line so that the rarely taken path
+// does not set the register budget of the event kernels.
+__device__ __noinline__ void km_solve_fallback(const KmGroup& G, double mz, double ffb, cplx* out) {
+  km_solve(G, mz, ffb, out);
+}
+
+// Lineshape (with production barrier) of every entry of Pc group g at the mass of `k`.
+__device__ __forceinline__ void pc_group_lineshapes(const PointTable& T, int g, const PcKin& k, cplx* raw) {
   const PcGroup& gr = T.grp[g];
   cplx kmo[NPMAX + NKMC];
-  if (gr.km >= 0) km_solve(T.G[gr.km], mz, T.ffb, kmo);
+  if (gr.km >= 0) {
+    const KmGroup& G = T.G[gr.km];
+    if (!table_lookup(T.tab, gr.km, G.npole + NKMC, k.mz, kmo)) km_solve_fallback(G, k.mz, T.ffb, kmo);
+  }
   for (int q = 0; q < gr.count; ++q) {
     const PcEntry& Z = T.Z[T.order[gr.first + q]];
     cplx v;
     if (Z.type == LT_KM)
       v = kmo[Z.slot];
     else if (Z.type == LT_BW)
-      v = pc_bw(Z, mz, T.ffr);
+      v = pc_bw(Z, k);
     else
       v = mk(1, 0);
-    raw[q] = v * pc_barrier(Z, mz, T.ffb);
+    raw[q] = v * pc_barrier(Z, k);
   }
 }
 
@@ -190,9 +286,10 @@ struct Ev {
 
 // Lambda* helicity amplitudes H[4*dmu + 2*lb + p] (GetAmpLz, kernel_calEva.cu:85-190).
 __device__ __forceinline__ void lstar_amplitudes(const PointTable& T, const Ev& ev, double mkp, cplx (&H)[8]) {
+  const LstarKin kin = lstar_kin(T, mkp);
   for (int r = 0; r < T.NR; ++r) {
     const LstarEntry& L = T.L[r];
-    const cplx q = lstar_lineshape(L, mkp, T.ffr, T.ffb);
+    const cplx q = lstar_lineshape(L, kin);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       for (int m = 0; m < L.ncm; ++m) {
@@ -210,10 +307,11 @@ __device__ __forceinline__ void lstar_amplitudes(const PointTable& T, const Ev& 
 
 // Pc helicity amplitudes at the event's own mass (unsmeared; GetAmp2s :347-503).
 __device__ __forceinline__ void pc_amplitudes(const PointTable& T, const Ev& ev, double mz, cplx (&H)[8]) {
+  const PcKin kin = pc_kin(T, mz);
   for (int g = 0; g < T.ngroups; ++g) {
     const PcGroup& gr = T.grp[g];
     cplx raw[MAX_GROUP_ENTRIES];
-    pc_group_lineshapes(T, g, mz, raw);
+    pc_group_lineshapes(T, g, kin, raw);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       cplx E[12];
@@ -295,7 +393,7 @@ struct Acc {
 };
 
 // ------------------------------------------------------------------------------- unsmeared
-__global__ void __launch_bounds__(UNSMEARED_THREADS)
+__global__ void __launch_bounds__(UNSMEARED_THREADS, PWA_UNSMEARED_MIN_BLOCKS)
     k_unsmeared(EventSet ev, int64_t nda, int64_t begin, int64_t end, const int32_t* list,
                 const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int amp2_only) {
   __shared__ __align__(16) PointTable T;
@@ -352,7 +450,7 @@ template <>
 __device__ __forceinline__ const float* smear_table<150>() { return kSmear150; }
 
 template <int NB>
-__global__ void __launch_bounds__(SMEAR_THREADS)
+__global__ void __launch_bounds__(SMEAR_THREADS, PWA_SMEAR_MIN_BLOCKS)
     k_smeared(EventSet ev, int64_t nda, int64_t begin, int64_t end, const int32_t* list,
               const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -379,7 +477,7 @@ __global__ void __launch_bounds__(SMEAR_THREADS)
     for (int t = tid; t < T.NR * TILE; t += SMEAR_THREADS) {
       const int r = t / TILE, el = t % TILE;
       const int64_t e = S.ev[el];
-      S.Q[r][el] = (e >= 0) ? lstar_lineshape(T.L[r], ldf(ev.pp, e), T.ffr, T.ffb) : mk(0, 0);
+      S.Q[r][el] = (e >= 0) ? lstar_lineshape(T.L[r], lstar_kin(T, ldf(ev.pp, e))) : mk(0, 0);
     }
     __syncthreads();
     // phase 1b/1c: helicity amplitudes; thread -> (event el, helicity h)
@@ -441,12 +539,13 @@ __global__ void __launch_bounds__(SMEAR_THREADS)
         // b == -1 is the unsmeared evaluation for the MC non-interference sum
         for (int b = (need_noint && b0 == 0) ? -1 : b0; b < NB; b += (b < 0) ? (1 + b0) : LANES_PER_EVENT) {
           const double m = (b < 0) ? mz : mz + (double)qoff[b] * mres;
+          const PcKin kin = pc_kin(T, m);
           cplx s8[8];
 #pragma unroll
           for (int h = 0; h < 8; ++h) s8[h] = mk(0, 0);
           for (int g = 0; g < T.ngroups; ++g) {
             cplx raw[MAX_GROUP_ENTRIES];
-            pc_group_lineshapes(T, g, m, raw);
+            pc_group_lineshapes(T, g, kin, raw);
             const PcGroup& gr = T.grp[g];
             for (int q = 0; q < gr.count; ++q) {
               const int qq = gr.first + q;
@@ -515,6 +614,85 @@ __global__ void __launch_bounds__(SMEAR_THREADS)
     __syncthreads();
   }
   block_reduce_store<SMEAR_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
+}
+
+// ------------------------------------------------------------------------------- tables
+// Exact K-matrix outputs at every grid node of every active J^P group.
+__global__ void k_build_tables(const PointTable* __restrict__ T, int n_nodes) {
+  const int64_t total = 4 * (int64_t)n_nodes;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int ik = (int)(t / n_nodes), j = (int)(t % n_nodes);
+    cplx* dst = const_cast<cplx*>(T->tab.data[ik]);
+    if (!dst) continue;
+    const double m = T->tab.m_lo + j * T->tab.h;
+    cplx out[TAB_SLOTS];
+#pragma unroll
+    for (int o = 0; o < TAB_SLOTS; ++o) out[o] = mk(0, 0);
+    km_solve(T->G[ik], m, T->ffb, out);
+#pragma unroll
+    for (int o = 0; o < TAB_SLOTS; ++o) dst[(size_t)j * TAB_SLOTS + o] = out[o];
+  }
+}
+
+// Verifies every interval [j, j+1] of every table: the 6-point interpolant at three interior points
+// against exact solves; flags the interval when the largest output error exceeds TAB_CHECK_TOL times
+// the largest output magnitude.
+__global__ void k_check_tables(const PointTable* __restrict__ T, int n_nodes) {
+  const int64_t total = 4 * (int64_t)n_nodes;
+  const LineTables& tab = T->tab;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int ik = (int)(t / n_nodes), j = (int)(t % n_nodes);
+    if (!tab.data[ik]) continue;
+    unsigned char* bad = const_cast<unsigned char*>(tab.bad[ik]);
+    if (j < 2 || j + 3 >= n_nodes) {
+      bad[j] = 1;
+      continue;
+    }
+    const int nout = T->G[ik].npole + NKMC;
+    const cplx* base = tab.data[ik] + (size_t)(j - 2) * TAB_SLOTS;
+    bool ok = true;
+    // the stencil [m_{j-2}, m_{j+3}] must not reach into a guard interval
+    const double s_lo = tab.m_lo + (j - 2) * tab.h, s_hi = tab.m_lo + (j + 3) * tab.h;
+    for (int q = 0; q < tab.nguard; ++q)
+      if (s_hi >= tab.guard_lo[q] && s_lo <= tab.guard_hi[q]) ok = false;
+    const double ts[3] = {0.2, 0.5, 0.8};
+    for (int q = 0; q < 3 && ok; ++q) {
+      const double tt = ts[q];
+      const double d0 = tt + 2.0, d1 = tt + 1.0, d2 = tt, d3 = tt - 1.0, d4 = tt - 2.0, d5 = tt - 3.0;
+      const double w[6] = {d1 * d2 * d3 * d4 * d5 * (-1.0 / 120.0), d0 * d2 * d3 * d4 * d5 * (1.0 / 24.0),
+                           d0 * d1 * d3 * d4 * d5 * (-1.0 / 12.0), d0 * d1 * d2 * d4 * d5 * (1.0 / 12.0),
+                           d0 * d1 * d2 * d3 * d5 * (-1.0 / 24.0), d0 * d1 * d2 * d3 * d4 * (1.0 / 120.0)};
+      cplx ex[TAB_SLOTS];
+      km_solve(T->G[ik], tab.m_lo + (j + tt) * tab.h, T->ffb, ex);
+      double emax = 0, vmax = 0;
+      for (int o = 0; o < nout; ++o) {
+        cplx acc = mk(0, 0);
+        for (int k = 0; k < 6; ++k) acc += base[k * TAB_SLOTS + o] * w[k];
+        emax = fmax(emax, sqrt(norm2(acc - ex[o])));
+        vmax = fmax(vmax, sqrt(norm2(ex[o])));
+      }
+      ok = isfinite(emax) && emax <= TAB_CHECK_TOL * vmax;
+    }
+    bad[j] = ok ? 0 : 1;
+  }
+}
+
+cudaError_t launch_build_tables(const PointTable* d_table, int n_nodes, int sm_count, cudaStream_t st) {
+  k_build_tables<<<sm_count * 8, 128, 0, st>>>(d_table, n_nodes);
+  k_check_tables<<<sm_count * 8, 128, 0, st>>>(d_table, n_nodes);
+  return cudaGetLastError();
+}
+
+void attach_tables(PointTable* T, cplx* d_mem, unsigned char* d_flags) {
+  bool any = false;
+  for (int ik = 0; ik < 4; ++ik) {
+    bool used = false;
+    for (int g = 0; g < T->ngroups; ++g) used |= (T->grp[g].km == ik);
+    T->tab.data[ik] = used ? d_mem + (size_t)ik * TAB_NODES * TAB_SLOTS : nullptr;
+    T->tab.bad[ik] = used ? d_flags + (size_t)ik * TAB_NODES : nullptr;
+    any |= used;
+  }
+  T->tab.enabled = any ? 1 : 0;
 }
 
 // ------------------------------------------------------------------------------- finalize
@@ -635,6 +813,44 @@ cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* o
 }
 
 // ------------------------------------------------------------------------------- point table
+// Masses in the table range where the reference's complex square root (csqrt_branch) changes branch
+// for one of the complex-mass channels (D* Sigma_c, D* Sigma_c*, D Sigma_c, D Sigma_c*): the lineshape
+// jumps there, so interpolation must not straddle them.  Scan plus bisection, computed once.
+static const std::vector<double>& complex_branch_masses() {
+  static std::vector<double> out;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const cplx ch[4][2] = {{mk(KM_DST, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_DST, 0), mk(KM_SCST, KM_SCST_HW)},
+                           {mk(KM_D, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_D, 0), mk(KM_SCST, KM_SCST_HW)}};
+    for (auto& c : ch) {
+      auto state = [&](double m) {
+        const double s = m * m;
+        const cplx a = c[0] + c[1], b = c[0] - c[1];
+        const cplx p = (a * a - mk(s, 0)) * (b * b - mk(s, 0));
+        if (fabs(p.re) < PWA_F(0.000001f) && fabs(p.im) < PWA_F(0.000001f)) return 2;
+        return (signbit(p.im) && fabs(p.im / p.re) > PWA_F(0.001f)) ? 1 : 0;
+      };
+      const double lo = TAB_M_LO - 1e-3, hi = TAB_M_HI + 1e-3, dm = 1e-6;
+      double prev_m = lo;
+      int prev = state(lo);
+      for (double m = lo + dm; m <= hi; m += dm) {
+        const int st = state(m);
+        if (st != prev) {
+          double a = prev_m, b = m;
+          for (int it = 0; it < 60; ++it) {
+            const double c2 = 0.5 * (a + b);
+            (state(c2) == prev ? a : b) = c2;
+          }
+          out.push_back(0.5 * (a + b));
+          prev = st;
+        }
+        prev_m = m;
+      }
+    }
+  });
+  return out;
+}
+
 // Decodes the float parameter block (layout of cu_init_data, RooDalitzAmplitude.cxx:3141-3210;
 // coupling offsets of cuda_configure_ampcount, kernel_calEva.cu:1014-1098; K-matrix output slots
 // of cuda_configure_Pc_KMatrix, :978-1010) and hoists every parameter-only constant.
@@ -692,6 +908,12 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     }
     L.polyR0 = bw_poly(L.LR, sq(T->ffr * L.pR0));
     L.norm = bw_norm(m_r, L.g_r);
+    L.inv_pR0 = (L.pR0 != 0) ? 1.0 / L.pR0 : 0.0;
+    L.sqrt_polyR0 = std::sqrt(L.polyR0);
+    L.inv_pR0_sp = (L.pR0_sp != 0) ? 1.0 / L.pR0_sp : 0.0;
+    if (L.type == LT_BW && (L.branch == 0 || L.branch == 3) && L.LR >= 1 && L.LR <= 5) T->lmask_lstar_R |= 1 << L.LR;
+    if (L.type == LT_BW && L.branch == 1) T->needs_sigma_pi = 1;
+    if (L.LR > 5) return 5;
     // Lambda_b barrier constants (BTerm)
     const double J = 0.5 * S2;
     L.LB = (J <= 1) ? 0 : (int)(J - 1.5);
@@ -703,6 +925,9 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     L.pB0 = pB0;
     L.polyB0 = bw_poly(L.LB, sq(T->ffb * pB0));
     L.lb_scale = ipow(M_LB / pB0, L.LB);
+    L.sqrt_polyB0 = std::sqrt(L.polyB0);
+    if (L.LB >= 1 && L.LB <= 5) T->lmask_lstar_B |= 1 << L.LB;
+    if (L.LB > 5) return 5;
     for (int k = 0; k < 2; ++k)
       for (int m = 0; m < 6; ++m) {
         if (S2 == 1 && m >= 4) continue;
@@ -740,6 +965,10 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
       Z.pR0 = Z.bw_above ? two_body_p(Z.m_r, M_P, M_JPSI) : 0.0;
       Z.polyR0 = bw_poly(Z.LR, sq(T->ffr * Z.pR0));
       Z.norm = bw_norm(Z.m_r, Z.g_r);
+      Z.inv_pR0 = (Z.pR0 != 0) ? 1.0 / Z.pR0 : 0.0;
+      Z.sqrt_polyR0 = std::sqrt(Z.polyR0);
+      if (Z.bw_above && Z.LR >= 1 && Z.LR <= 5) T->lmask_pc_R |= 1 << Z.LR;
+      if (Z.LR > 5) return 5;
     }
     const double J = 0.5 * S2;
     Z.LB = (int)(J - 0.5);
@@ -749,6 +978,9 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     Z.pB0_event = (pB0 < 0);
     Z.pB0 = pB0;
     Z.polyB0 = bw_poly(Z.LB, sq(T->ffb * pB0));
+    Z.sqrt_polyB0 = std::sqrt(Z.polyB0);
+    if (!Z.pB0_event && Z.LB >= 1 && Z.LB <= 5) T->lmask_pc_B |= 1 << Z.LB;
+    if (Z.LB > 5) return 5;
     const double S = 0.5 * S2;
     for (int k = 0; k < 2; ++k) {
       int m = 0;
@@ -836,6 +1068,44 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     }
   }
   T->ngroups = ng;
+  // table grid and guard intervals (tables stay disabled until the caller attaches table memory)
+  LineTables& tb = T->tab;
+  tb.enabled = 0;
+  tb.n_nodes = TAB_NODES;
+  tb.m_lo = TAB_M_LO;
+  tb.h = TAB_H;
+  tb.inv_h = 1.0 / TAB_H;
+  tb.nguard = 0;
+  auto guard = [&](double m, double half) {
+    if (tb.nguard < MAX_GUARDS && m > TAB_M_LO - 1e-3 && m < TAB_M_HI + 1e-3) {
+      tb.guard_lo[tb.nguard] = m - half;
+      tb.guard_hi[tb.nguard] = m + half;
+      ++tb.nguard;
+    }
+  };
+  const double cusp = 3e-4, step = 3.5 * TAB_H;
+  guard(M_P + M_JPSI, cusp);  // J/psi p threshold
+  guard(M_LB - M_K, cusp);    // upper kinematic edge (production barrier momentum)
+  bool neg_parity = false, pos_parity = false;
+  for (int ik = 0; ik < 4; ++ik) {
+    bool used = false;
+    for (int g = 0; g < ng; ++g) used |= (T->grp[g].km == ik);
+    if (!used) continue;
+    (T->G[ik].P == 1 ? pos_parity : neg_parity) = true;
+    for (int p = 0; p < T->G[ik].npole; ++p) {  // pole clamp |m0^2 - s| < 1e-3
+      const double a = T->G[ik].m0sq[p] - KM_DENORM_MIN, b = T->G[ik].m0sq[p] + KM_DENORM_MIN;
+      if (a > 0) guard(std::sqrt(a), step);
+      guard(std::sqrt(b), step);
+    }
+  }
+  if (pos_parity) {  // real-mass channel thresholds of the positive-parity groups
+    guard(KM_DST + KM_SC, cusp);
+    guard(KM_D + KM_SC, cusp);
+    guard(KM_D + KM_SCST, cusp);
+  }
+  if (neg_parity)
+    for (double m : complex_branch_masses()) guard(m, step);
+  if (tb.nguard >= MAX_GUARDS) return 4;
   return 0;
 }
 
@@ -843,7 +1113,9 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
 // lineshape x production barrier at mkp, and every Pc entry's lineshape x barrier at mz, entries in
 // parameter-block order.
 void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cplx* pc) {
-  for (int r = 0; r < T.NR; ++r) lstar[r] = lstar_lineshape(T.L[r], mkp, T.ffr, T.ffb);
+  const LstarKin lk = lstar_kin(T, mkp);
+  const PcKin pk = pc_kin(T, mz);
+  for (int r = 0; r < T.NR; ++r) lstar[r] = lstar_lineshape(T.L[r], lk);
   for (int g = 0; g < T.ngroups; ++g) {
     const PcGroup& gr = T.grp[g];
     cplx kmo[NPMAX + NKMC];
@@ -851,8 +1123,8 @@ void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cp
     for (int q = 0; q < gr.count; ++q) {
       const int i = T.order[gr.first + q];
       const PcEntry& Z = T.Z[i];
-      cplx v = (Z.type == LT_KM) ? kmo[Z.slot] : (Z.type == LT_BW) ? pc_bw(Z, mz, T.ffr) : mk(1, 0);
-      pc[i] = v * pc_barrier(Z, mz, T.ffb);
+      cplx v = (Z.type == LT_KM) ? kmo[Z.slot] : (Z.type == LT_BW) ? pc_bw(Z, pk) : mk(1, 0);
+      pc[i] = v * pc_barrier(Z, pk);
     }
   }
 }

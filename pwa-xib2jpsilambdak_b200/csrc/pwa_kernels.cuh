@@ -57,6 +57,14 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
 cudaError_t launch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
                            double* fx_out, int sm_count, cudaStream_t st);
 
+// Fills the per-point K-matrix tables T->tab.data[ik] (null for groups without table memory) from
+// the device copy of the point table and verifies every interval (two launches).
+cudaError_t launch_build_tables(const PointTable* d_table, int n_nodes, int sm_count, cudaStream_t st);
+
+// Attaches table memory (4 * TAB_NODES * TAB_SLOTS complex values and 4 * TAB_NODES interval flags)
+// to a host point table: enables interpolation for the K-matrix groups the model uses.
+void attach_tables(PointTable* T, cplx* d_mem, unsigned char* d_flags);
+
 // Reduces nparts partials and assembles the NLL.
 cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, double sum_w_data,
                             double nll_shift, EvalResult* res, cudaStream_t st);

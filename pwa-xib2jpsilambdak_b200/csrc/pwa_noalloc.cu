@@ -8,7 +8,7 @@
 // per-block partial sums, tail index lists, result slot) lives in one file-scope device array of
 // fixed size, so this entry point calls no cudaMalloc, cudaFree or other allocating routine.
 //
-// The array is PWA_NOALLOC_SCRATCH_BYTES (about 4.3 MB) on every GPU that loads the library and is
+// The array is PWA_NOALLOC_SCRATCH_BYTES (4.5 MiB) on every GPU that loads the library and is
 // held until the process exits.  Samples are limited to PWA_NOALLOC_MAX_EVENTS events.  All calls
 // share the array and it keeps the last call's contents: a call rewrites everything it reads
 // before reading it.  Calls that overlap on the GPU race on the array; calls from threads of one
@@ -47,8 +47,9 @@ constexpr size_t kOffParts = align256(kOffResult + sizeof(EvalResult));
 constexpr size_t kOffCounts = align256(kOffParts + kMaxParts * sizeof(Partial));
 constexpr size_t kOffOffsets = align256(kOffCounts + (kMaxChunks + 1) * sizeof(int));
 constexpr size_t kOffLists = align256(kOffOffsets + (kMaxChunks + 1) * sizeof(int));
-constexpr size_t kScratchBytes = align256(kOffLists + kMaxEvents * sizeof(int32_t));
-static_assert(kScratchBytes == PWA_NOALLOC_SCRATCH_BYTES, "update PWA_NOALLOC_SCRATCH_BYTES in pwa_b200.h");
+constexpr size_t kScratchBytes = PWA_NOALLOC_SCRATCH_BYTES;
+static_assert(align256(kOffLists + kMaxEvents * sizeof(int32_t)) <= kScratchBytes,
+              "scratch layout exceeds PWA_NOALLOC_SCRATCH_BYTES");
 
 // The scratch.  In host code this name is a host-side stand-in, not a device address: kernels get the
 // address looked up with cudaGetSymbolAddress below.

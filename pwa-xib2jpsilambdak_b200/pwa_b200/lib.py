@@ -10,11 +10,14 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "libpwa_b200.so"
+import os
+
+# The in-tree build; PWA_B200_LIB may name another build of the same library (A/B comparisons).
+LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
             "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
-            "pwa_ctx_set_timing", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_point_table_bytes",
+            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
 
@@ -54,6 +57,7 @@ def load() -> C.CDLL:
         L.pwa_ctx_last_kernel_ms.argtypes = [C.c_void_p]
         L.pwa_ctx_last_launches.argtypes = [C.c_void_p]
         L.pwa_ctx_set_timing.argtypes = [C.c_void_p, C.c_int]
+        L.pwa_ctx_set_lineshape_tables.argtypes = [C.c_void_p, C.c_int]
         L.pwa_ctx_segment_count.argtypes = [C.c_void_p]
         L.pwa_ctx_segment_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64),
                                            C.POINTER(C.c_double)]
@@ -154,6 +158,9 @@ class Context:
         check(self.L.pwa_ctx_amp2(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR,
                                   block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp)), "pwa_ctx_amp2")
         return out
+
+    def set_lineshape_tables(self, on: bool = True):
+        check(self.L.pwa_ctx_set_lineshape_tables(self.h, int(on)), "pwa_ctx_set_lineshape_tables")
 
     def set_timing(self, on: bool = True):
         check(self.L.pwa_ctx_set_timing(self.h, int(on)), "pwa_ctx_set_timing")

@@ -63,3 +63,17 @@ def test_repeated_calls_identical(ctx):
     a = ctx.eval_nll(blk).nll
     b = ctx.eval_nll(blk).nll
     assert a == b
+
+
+def test_lineshape_tables_match_exact_solves(ctx, oracle_mod):
+    """K-matrix tables (interpolated) against solving the K-matrix for every lookup, and the oracle."""
+    mdl, vals, blk, smp = make_test_sample("kmatrix", 3000, 40000, seed=17)
+    ctx.upload(smp)
+    ctx.set_lineshape_tables(False)
+    r0, fx0 = ctx.eval_nll(blk, want_fx=True)
+    ctx.set_lineshape_tables(True)
+    r1, fx1 = ctx.eval_nll(blk, want_fx=True)
+    assert np.max(np.abs(fx1 - fx0) / np.abs(fx0)) < 1e-10
+    assert abs(r1.nll - r0.nll) < 1e-7
+    v, s, ofx, _ = oracle_mod.nll(smp, blk)
+    assert abs(r1.nll - v) < NLL_TOL
