@@ -291,6 +291,9 @@ def main():
                                                                                "thresholds"},
            "gpu_launches": launches,
            "kernel_shares": shares,
+           "segments": {names[k]: {"events": int(n), "ms_per_step": round(t / args.steps, 4),
+                                   "ns_per_event": round(t / args.steps / max(n, 1) * 1e6, 3)}
+                        for k, (t, n) in seg_time.items()},
            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": None,
                         "note": f"algorithmic bytes = {req_b} B per event (planes the model reads) of the "

@@ -48,6 +48,10 @@ struct pwa_ctx {
   int32_t* d_lists = nullptr;
   std::vector<Segment> segs;
   std::vector<int> seg_off;
+  std::vector<int64_t> seg_defer_off;  // segment's region of d_defer
+  // events the table-only pass defers to the exact pass: n slots, one counter per segment (+ amp2)
+  int32_t* d_defer = nullptr;
+  int* d_defer_cnt = nullptr;
   int total_parts = 0;
   // per evaluation
   PointTable* d_table = nullptr;
@@ -61,8 +65,7 @@ struct pwa_ctx {
   int last_launches = 0;
   // K-matrix lineshape tables (on by default)
   int use_tables = 1;
-  cplx* d_tab = nullptr;
-  unsigned char* d_tab_flags = nullptr;
+  void* d_tab = nullptr;  // TAB_BYTES of two-level lineshape tables
   // optional per-segment timing
   int timing = 0;
   std::vector<cudaEvent_t> seg_ev;
@@ -78,12 +81,17 @@ void free_events(pwa_ctx* c) {
   cudaFree(c->own_sw);
   cudaFree(c->d_lists);
   cudaFree(c->d_parts);
+  cudaFree(c->d_defer);
+  cudaFree(c->d_defer_cnt);
   c->own_pp = c->own_pp1 = c->own_pp2 = c->own_sw = nullptr;
   c->d_lists = nullptr;
   c->d_parts = nullptr;
+  c->d_defer = nullptr;
+  c->d_defer_cnt = nullptr;
   c->pp = c->pp1 = c->pp2 = c->sw = nullptr;
   c->segs.clear();
   c->seg_off.clear();
+  c->seg_defer_off.clear();
   c->n = 0;
 }
 
@@ -113,14 +121,20 @@ int build_segments(pwa_ctx* c, const float* h_mz) {
   if (!lw.empty()) c->segs.push_back({SMEAR_20, 0, (int64_t)lw.size(), c->d_lists});
   if (!lu.empty()) c->segs.push_back({SMEAR_NONE, 0, (int64_t)lu.size(), c->d_lists + lw.size()});
   c->seg_off.clear();
+  c->seg_defer_off.clear();
   int tot = 0;
+  int64_t doff = 0;
   for (auto& s : c->segs) {
     c->seg_off.push_back(tot);
-    tot += segment_blocks(s, c->sm_count);
+    tot += segment_parts(s, c->sm_count, true);
+    c->seg_defer_off.push_back(doff);
+    doff += s.end - s.begin;
   }
   c->total_parts = std::max(tot, 1);
   PWA_CUDA(cudaMalloc(&c->d_parts, c->total_parts * sizeof(Partial)));
   PWA_CUDA(cudaMemset(c->d_parts, 0, c->total_parts * sizeof(Partial)));
+  PWA_CUDA(cudaMalloc(&c->d_defer, std::max<int64_t>(n, 1) * sizeof(int32_t)));
+  PWA_CUDA(cudaMalloc(&c->d_defer_cnt, 8 * sizeof(int)));
   return PWA_OK;
 }
 
@@ -184,7 +198,6 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   cudaFreeHost(c->h_res);
   cudaFree(c->d_fx);
   cudaFree(c->d_tab);
-  cudaFree(c->d_tab_flags);
   for (auto e : c->seg_ev) cudaEventDestroy(e);
   if (c->e0) cudaEventDestroy(c->e0);
   if (c->e1) cudaEventDestroy(c->e1);
@@ -246,6 +259,21 @@ int pwa_ctx_set_device_events(pwa_ctx* c, const float* d_pp, const float* d_pp1,
   return build_segments(c, mz.data());
 }
 
+// Copies the decoded point table to the device and, with tables on, builds the lineshape tables
+// for it on the context's stream.
+static int upload_point(pwa_ctx* c, int* launches) {
+  if (c->use_tables) {
+    if (!c->d_tab) PWA_CUDA(cudaMalloc(&c->d_tab, TAB_BYTES));
+    attach_tables(c->h_table, c->d_tab);
+  }
+  PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
+  if (c->h_table->tab.enabled) {
+    PWA_CUDA(launch_build_tables(c->d_table, TAB_NODES, c->sm_count, c->st));
+    *launches += 4;
+  }
+  return PWA_OK;
+}
+
 int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ,
                      int NX, float FFR, float FFB, double sum_w_mc, double sum_w_data, double nll_shift,
                      pwa_result* out, double* h_fx) {
@@ -262,18 +290,9 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
     c->fx_cap = c->n;
   }
   EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
-  if (c->use_tables) {
-    if (!c->d_tab) PWA_CUDA(cudaMalloc(&c->d_tab, (size_t)4 * TAB_NODES * TAB_SLOTS * sizeof(cplx)));
-    if (!c->d_tab_flags) PWA_CUDA(cudaMalloc(&c->d_tab_flags, (size_t)4 * TAB_NODES));
-    attach_tables(c->h_table, c->d_tab, c->d_tab_flags);
-  }
-  PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   int launches = 0;
-  if (c->h_table->tab.enabled) {
-    PWA_CUDA(launch_build_tables(c->d_table, TAB_NODES, c->sm_count, c->st));
-    launches += 2;
-  }
+  if ((rc = upload_point(c, &launches))) return rc;
   if (c->timing) {
     while (c->seg_ev.size() < c->segs.size()) {
       cudaEvent_t e;
@@ -281,11 +300,17 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
       c->seg_ev.push_back(e);
     }
   }
+  const bool defer = c->h_table->tab.enabled != 0;
+  // slots of passes that do not run this time must read as zero
+  PWA_CUDA(cudaMemsetAsync(c->d_parts, 0, c->total_parts * sizeof(Partial), c->st));
+  PWA_CUDA(cudaMemsetAsync(c->d_defer_cnt, 0, 8 * sizeof(int), c->st));
   for (size_t i = 0; i < c->segs.size(); ++i) {
-    PWA_CUDA(launch_segment(ev, c->segs[i], c->d_table, c->d_parts + c->seg_off[i], h_fx ? c->d_fx : nullptr,
+    int32_t* dq = defer ? c->d_defer + c->seg_defer_off[i] : nullptr;
+    int* dc = defer ? c->d_defer_cnt + i : nullptr;
+    PWA_CUDA(launch_segment(ev, c->segs[i], c->d_table, c->d_parts + c->seg_off[i], h_fx ? c->d_fx : nullptr, dq, dc,
                             c->sm_count, c->st));
     if (c->timing) PWA_CUDA(cudaEventRecord(c->seg_ev[i], c->st));
-    ++launches;
+    launches += defer ? 2 : 1;
   }
   PWA_CUDA(launch_finalize(c->d_parts, c->total_parts, sum_w_mc, sum_w_data, nll_shift, c->d_res, c->st));
   ++launches;
@@ -330,8 +355,12 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
     c->fx_cap = c->n;
   }
   EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
-  PWA_CUDA(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
-  PWA_CUDA(launch_amp2(ev, c->d_table, c->d_fx, c->sm_count, c->st));
+  int launches = 0;
+  if ((rc = upload_point(c, &launches))) return rc;
+  const bool defer = c->h_table->tab.enabled != 0;
+  if (defer) PWA_CUDA(cudaMemsetAsync(c->d_defer_cnt + 7, 0, sizeof(int), c->st));
+  PWA_CUDA(launch_amp2(ev, c->d_table, c->d_fx, defer ? c->d_defer : nullptr, defer ? c->d_defer_cnt + 7 : nullptr,
+                       c->sm_count, c->st));
   if (c->n) PWA_CUDA(cudaMemcpyAsync(h_amp2, c->d_fx, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   PWA_CUDA(cudaStreamSynchronize(c->st));
   return PWA_OK;

@@ -1,21 +1,21 @@
 // Likelihood kernels for sm_100a, FP64 arithmetic on the reference's float SoA basis.
 //
 // Work split (reference: src/kernel_calEva.cu:819-976):
-//   * unsmeared events: one thread per event (persistent grid-stride loop); lineshapes at the
-//     event's m(J/psi p), Lambda* and Pc helicity sums, |A|^2 with and without interference.
-//   * smeared events (30 / 150 / 20 resolution offsets): a block takes a tile of 32 events.  Phase 1
-//     builds the Lambda* amplitudes and the per-entry Pc angular amplitudes HZ_i[h] (couplings
-//     included, lineshape excluded) in shared memory; phase 2 spreads the (event, offset) pairs over
-//     8 lanes per event, each evaluating all Pc lineshapes (K-matrix solves) at its offsets and
-//     accumulating S = sum_i BW_i HZ_i; phase 3 combines
-//       |A|^2 = sum_h |H_L|^2 + 2 w Re(conj(H_L) sum_b S_b) + w^2 u sum_b |S_b|^2,
-//     which is the reference's BW1/BW2 form (kernel_calEva.cu:676-810) with its float weight
-//     w = float(1/NBINS) and rescale u = float(1/w).
+//   * per parameter point, every Pc entry's lineshape is tabulated on a 10 keV grid of m(J/psi p)
+//     (k_build_tables) and each grid interval is verified against exact evaluations
+//     (k_check_tables); the event kernels interpolate, and evaluate exactly where the table cannot
+//     serve a mass (thresholds, flagged intervals).
+//   * unsmeared events (k_unsmeared): two lanes per event, one per proton helicity.
+//   * smeared events (k_smeared<NB>, 20 / 30 / 150 resolution offsets): eight lanes per event, one per
+//     helicity, holding the Pc angular amplitudes of every entry in registers; the lineshapes at
+//     the offsets are computed eight at a time into per-warp shared memory and contracted by all
+//     eight lanes.  Warp-synchronous, no block barriers in the event loop.
 //   * every block writes FP64 partial sums (data sw ln fx, MC w fx, MC w fx without
 //     interference); one finalize block reduces them with compensated summation.
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -26,17 +26,6 @@ namespace pwa {
 // Resolution offsets in units of the mass resolution (reference data, Resonances.h:31-54).
 #include "smear_tables.inc"
 
-#ifndef PWA_SMEAR_MIN_BLOCKS
-#define PWA_SMEAR_MIN_BLOCKS 2
-#endif
-#ifndef PWA_UNSMEARED_MIN_BLOCKS
-#define PWA_UNSMEARED_MIN_BLOCKS 4
-#endif
-
-constexpr int TILE = 32;          // events per smeared tile
-constexpr int SMEAR_THREADS = 256;
-constexpr int LANES_PER_EVENT = SMEAR_THREADS / TILE;  // 8
-constexpr int UNSMEARED_THREADS = 128;
 constexpr int MAX_GROUP_ENTRIES = 8;
 
 __device__ __forceinline__ double ldf(const float* p, int64_t i) { return (double)__ldg(p + i); }
@@ -208,60 +197,99 @@ __host__ __device__ inline void km_solve(const KmGroup& G, double mz, double ffb
   for (int i = 0; i < NKMC; ++i) out[G.npole + i] = T[i] * (ms[0] * na);
 }
 
-// K-matrix outputs of group ik at mz from the per-point table (6-point Lagrange on the uniform grid);
-// false when mz is in a guard interval or too close to the grid ends.
-__device__ __forceinline__ bool table_lookup(const LineTables& tab, int ik, int nout, double mz, cplx* out) {
+// ------------------------------------------------------------------------------- Pc entry tables
+// Exact lineshapes (with production barrier) of the entries of Pc group g at the mass of k, written
+// to raw[0 .. count) (order positions gr.first ...).
+__host__ __device__ inline void pc_group_exact(const PointTable& T, int g, const PcKin& k, cplx* raw) {
+  const PcGroup& gr = T.grp[g];
+  cplx kmo[NPMAX + NKMC];
+  if (gr.km >= 0) km_solve(T.G[gr.km], k.mz, T.ffb, kmo);
+  for (int q = 0; q < gr.count; ++q) {
+    const PcEntry& Z = T.Z[T.order[gr.first + q]];
+    const cplx v = (Z.type == LT_KM) ? kmo[Z.slot] : (Z.type == LT_BW) ? pc_bw(Z, k) : mk(1, 0);
+    raw[q] = v * pc_barrier(Z, k);
+  }
+}
+
+// Every Pc entry's lineshape at mass m, exactly, at raw[order position].  Kept out of line so that
+// the rarely taken exact path does not set the register budget of the event kernels.
+__device__ __noinline__ void pc_entries_exact(const PointTable& T, double m, cplx* raw) {
+  const PcKin kin = pc_kin(T, m);
+  for (int g = 0; g < T.ngroups; ++g) pc_group_exact(T, g, kin, raw + T.grp[g].first);
+}
+
+// 6-point Lagrange weights for nodes j-2 .. j+3 at x = j + t (denominators -120, 24, -12, 12, -24, 120).
+__host__ __device__ __forceinline__ void lagrange6(double t, double* w) {
+  const double d0 = t + 2.0, d1 = t + 1.0, d2 = t, d3 = t - 1.0, d4 = t - 2.0, d5 = t - 3.0;
+  const double p01 = d0 * d1, p012 = p01 * d2, p0123 = p012 * d3, p01234 = p0123 * d4;
+  const double s45 = d4 * d5, s345 = d3 * s45, s2345 = d2 * s345, s12345 = d1 * s2345;
+  w[0] = s12345 * (-1.0 / 120.0);
+  w[1] = d0 * s2345 * (1.0 / 24.0);
+  w[2] = p01 * s345 * (-1.0 / 12.0);
+  w[3] = p012 * s45 * (1.0 / 12.0);
+  w[4] = p0123 * d5 * (-1.0 / 24.0);
+  w[5] = p01234 * (1.0 / 120.0);
+}
+
+struct TabAt {
+  const double2* base;  // first stencil node, order position 0
+  double w[6];
+};
+
+// Locates mass m on the per-point entry table: the level-1 grid, or the refined block of a flagged
+// interval; false when neither can serve m (the caller then evaluates exactly).
+__device__ __forceinline__ bool tab_at(const LineTables& tab, double m, TabAt& a) {
   if (!tab.enabled) return false;
-  const double x = (mz - tab.m_lo) * tab.inv_h;
+  const double x = (m - tab.m_lo) * tab.inv_h;
   const double fj = floor(x);
   if (!(fj >= 2.0 && fj + 3.0 < (double)tab.n_nodes)) return false;
   const int j = (int)fj;
-  if (tab.bad[ik][j]) return false;
-  const double t = x - fj;
-  // Lagrange weights for nodes j-2 .. j+3 (denominators -120, 24, -12, 12, -24, 120)
-  const double d0 = t + 2.0, d1 = t + 1.0, d2 = t, d3 = t - 1.0, d4 = t - 2.0, d5 = t - 3.0;
-  const double p01 = d0 * d1, p012 = p01 * d2, p0123 = p012 * d3, p01234 = p0123 * d4;
-  const double s5 = d5, s45 = d4 * s5, s345 = d3 * s45, s2345 = d2 * s345, s12345 = d1 * s2345;
-  const double w[6] = {s12345 * (-1.0 / 120.0), d0 * s2345 * (1.0 / 24.0), p01 * s345 * (-1.0 / 12.0),
-                       p012 * s45 * (1.0 / 12.0), p0123 * s5 * (-1.0 / 24.0), p01234 * (1.0 / 120.0)};
-  const cplx* base = tab.data[ik] + (size_t)(j - 2) * TAB_SLOTS;
-  for (int o = 0; o < nout; ++o) {
-    cplx acc = mk(0, 0);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const cplx v = base[k * TAB_SLOTS + o];
-      acc.re = fma(w[k], v.re, acc.re);
-      acc.im = fma(w[k], v.im, acc.im);
-    }
-    out[o] = acc;
+  const int c = __ldg(tab.cell + j);
+  if (c == 0) {
+    lagrange6(x - fj, a.w);
+    a.base = reinterpret_cast<const double2*>(tab.data) + (size_t)(j - 2) * tab.stride;
+    return true;
   }
+  if (c < 0) return false;
+  const double x2 = (x - fj) * (double)TAB_SUB;
+  const double fi = fmin(floor(x2), (double)(TAB_SUB - 1));
+  const int i = (int)fi;
+  if (__ldg(tab.sub_bad + (size_t)(c - 1) * TAB_SUB + i)) return false;
+  lagrange6(x2 - fi, a.w);
+  a.base = reinterpret_cast<const double2*>(tab.sub) + ((size_t)(c - 1) * TAB_SUB_NODES + i) * tab.stride;
   return true;
 }
 
-// Exact solve for lookups the table cannot serve; kept out of line so that the rarely taken path
-// does not set the register budget of the event kernels.
-__device__ __noinline__ void km_solve_fallback(const KmGroup& G, double mz, double ffb, cplx* out) {
-  km_solve(G, mz, ffb, out);
+__device__ __forceinline__ cplx tab_get(const TabAt& a, int stride, int pos) {
+  cplx acc = mk(0, 0);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double2 v = __ldg(a.base + k * stride + pos);
+    acc.re = fma(a.w[k], v.x, acc.re);
+    acc.im = fma(a.w[k], v.y, acc.im);
+  }
+  return acc;
 }
 
-// Lineshape (with production barrier) of every entry of Pc group g at the mass of `k`.
-__device__ __forceinline__ void pc_group_lineshapes(const PointTable& T, int g, const PcKin& k, cplx* raw) {
-  const PcGroup& gr = T.grp[g];
-  cplx kmo[NPMAX + NKMC];
-  if (gr.km >= 0) {
-    const KmGroup& G = T.G[gr.km];
-    if (!table_lookup(T.tab, gr.km, G.npole + NKMC, k.mz, kmo)) km_solve_fallback(G, k.mz, T.ffb, kmo);
-  }
-  for (int q = 0; q < gr.count; ++q) {
-    const PcEntry& Z = T.Z[T.order[gr.first + q]];
-    cplx v;
-    if (Z.type == LT_KM)
-      v = kmo[Z.slot];
-    else if (Z.type == LT_BW)
-      v = pc_bw(Z, k);
-    else
-      v = mk(1, 0);
-    raw[q] = v * pc_barrier(Z, k);
+// All Pc entry lineshapes at mass m into out[order position] from the table; false (and zeros) when
+// the table cannot serve m.
+__device__ __forceinline__ bool lookup_table(const PointTable& T, double m, cplx* out) {
+  TabAt ta;
+  const bool ok = tab_at(T.tab, m, ta);
+#pragma unroll 2
+  for (int q = 0; q < T.NZ; ++q) out[q] = ok ? tab_get(ta, T.tab.stride, q) : mk(0, 0);
+  return ok;
+}
+
+// All Pc entry lineshapes at mass m into out[order position]: interpolated, or exact where the table
+// cannot serve the mass.
+__device__ __forceinline__ void lookup_entries(const PointTable& T, double m, cplx* out) {
+  TabAt ta;
+  if (tab_at(T.tab, m, ta)) {
+#pragma unroll 2
+    for (int q = 0; q < T.NZ; ++q) out[q] = tab_get(ta, T.tab.stride, q);
+  } else {
+    pc_entries_exact(T, m, out);
   }
 }
 
@@ -284,55 +312,10 @@ struct Ev {
   __device__ __forceinline__ double DZ(int s, int k, int m) const { return ldf(pp2, e + (s * 24 + k * 12 + m) * ns); }
 };
 
-// Lambda* helicity amplitudes H[4*dmu + 2*lb + p] (GetAmpLz, kernel_calEva.cu:85-190).
-__device__ __forceinline__ void lstar_amplitudes(const PointTable& T, const Ev& ev, double mkp, cplx (&H)[8]) {
-  const LstarKin kin = lstar_kin(T, mkp);
-  for (int r = 0; r < T.NR; ++r) {
-    const LstarEntry& L = T.L[r];
-    const cplx q = lstar_lineshape(L, kin);
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      for (int m = 0; m < L.ncm; ++m) {
-        const cplx c = L.c[k * 6 + m];
-        if (c.re == 0.0 && c.im == 0.0) continue;
-        const cplx D = (q * c) * ev.DL(L.sidx, k, m);
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) cmac(H[4 * i + 2 * j + k], ev.A(i, j, m), D);
-      }
-    }
-  }
-}
+__device__ __forceinline__ bool nonzero(cplx c) { return c.re != 0.0 || c.im != 0.0; }
 
-// Pc helicity amplitudes at the event's own mass (unsmeared; GetAmp2s :347-503).
-__device__ __forceinline__ void pc_amplitudes(const PointTable& T, const Ev& ev, double mz, cplx (&H)[8]) {
-  const PcKin kin = pc_kin(T, mz);
-  for (int g = 0; g < T.ngroups; ++g) {
-    const PcGroup& gr = T.grp[g];
-    cplx raw[MAX_GROUP_ENTRIES];
-    pc_group_lineshapes(T, g, kin, raw);
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      cplx E[12];
-#pragma unroll
-      for (int m = 0; m < 12; ++m) E[m] = mk(0, 0);
-      for (int q = 0; q < gr.count; ++q) {
-        const PcEntry& Z = T.Z[T.order[gr.first + q]];
-#pragma unroll
-        for (int m = 0; m < 12; ++m) cmac(E[m], raw[q], Z.c[k * 12 + m]);
-      }
-#pragma unroll
-      for (int m = 0; m < 12; ++m) {
-        if (E[m].re == 0.0 && E[m].im == 0.0) continue;
-        const cplx D = E[m] * ev.DZ(gr.sidx, k, m);
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) cmac(H[4 * i + 2 * j + k], ev.AZ(i, j, m), D);
-      }
-    }
-  }
+__device__ __forceinline__ cplx shfl_xor(cplx v, int o) {
+  return mk(__shfl_xor_sync(0xffffffffu, v.re, o), __shfl_xor_sync(0xffffffffu, v.im, o));
 }
 
 // ------------------------------------------------------------------------------- reductions
@@ -371,6 +354,7 @@ __device__ void block_reduce_store(double a, double b, double c, double d, Parti
 
 template <int NT>
 __device__ __forceinline__ void load_table(const PointTable* g, PointTable* s) {
+  static_assert(sizeof(PointTable) % sizeof(int4) == 0, "PointTable must be a whole number of int4");
   const int4* src = reinterpret_cast<const int4*>(g);
   int4* dst = reinterpret_cast<int4*>(s);
   constexpr int n = sizeof(PointTable) / sizeof(int4);
@@ -392,53 +376,151 @@ struct Acc {
   }
 };
 
-// ------------------------------------------------------------------------------- unsmeared
-__global__ void __launch_bounds__(UNSMEARED_THREADS, PWA_UNSMEARED_MIN_BLOCKS)
-    k_unsmeared(EventSet ev, int64_t nda, int64_t begin, int64_t end, const int32_t* list,
-                const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int amp2_only) {
-  __shared__ __align__(16) PointTable T;
-  load_table<UNSMEARED_THREADS>(gtab, &T);
-  Acc acc;
-  const int64_t count = end - begin;
-  for (int64_t p = (int64_t)blockIdx.x * UNSMEARED_THREADS + threadIdx.x; p < count;
-       p += (int64_t)gridDim.x * UNSMEARED_THREADS) {
-    const int64_t e = list ? (int64_t)list[begin + p] : begin + p;
-    Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, e};
-    cplx HL[8], HZ[8];
-#pragma unroll
-    for (int h = 0; h < 8; ++h) HL[h] = HZ[h] = mk(0, 0);
-    const double mkp = E.mkp(), mz = E.mz();
-    lstar_amplitudes(T, E, mkp, HL);
-    pc_amplitudes(T, E, mz, HZ);
-    double v = 0, vn = 0;
-#pragma unroll
-    for (int h = 0; h < 8; ++h) {
-      v += norm2(HL[h] + HZ[h]);
-      vn += norm2(HL[h]) + norm2(HZ[h]);
-    }
-    if (amp2_only) {
-      fx_out[e] = v;
-      continue;
-    }
-    const float wf = E.w();
-    const bool is_data_w = wf <= -1000.f;
-    const double w = wf;
-    const double fxe = is_data_w ? v : v * w;
-    if (fx_out) fx_out[e] = fxe;
-    acc.add(e, nda, ev.sw, fxe, is_data_w ? 0.0 : vn * w, false);
-  }
-  if (!amp2_only) block_reduce_store<UNSMEARED_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
+// ------------------------------------------------------------------------------- event kernels
+constexpr int EV_THREADS = 256;
+constexpr int EV_WARPS = EV_THREADS / 32;
+constexpr int UNSMEARED_PER_WARP = 16;  // events per warp: lane = 16 * k + event
+constexpr int SMEARED_PER_WARP = 4;     // events per warp: lane = 8 * event + helicity
+
+__device__ __forceinline__ int64_t event_index(const int32_t* list, int64_t begin, int64_t p) {
+  return list ? (int64_t)list[begin + p] : begin + p;
 }
 
-// ------------------------------------------------------------------------------- smeared
-struct SmearShared {
-  PointTable T;
-  cplx Q[MAX_LSTAR][TILE];    // Lambda* lineshapes per event
-  double HZre[MAX_PC][8][TILE], HZim[MAX_PC][8][TILE];
-  double HLre[8][TILE], HLim[8][TILE];
-  double A1re[8][TILE], A1im[8][TILE], A2[8][TILE], VN[TILE];
-  int64_t ev[TILE];
+// Contiguous share [c0, c1) of a segment's count positions for this block, a whole number of rounds
+// long: consecutive rounds of a block take neighbouring events (masses), whose lineshape-table nodes
+// stay in L1.
+struct Chunk {
+  int64_t c0, c1;
 };
+__device__ __forceinline__ Chunk block_chunk(int64_t count, int per_round) {
+  int64_t chunk = (count + gridDim.x - 1) / gridDim.x;
+  chunk = (chunk + per_round - 1) / per_round * per_round;
+  const int64_t c0 = (int64_t)blockIdx.x * chunk;
+  return Chunk{c0, min(count, c0 + chunk)};
+}
+
+// Unsmeared events.  Lane l of a warp takes event l % 16 of the warp's 16 and proton helicity
+// k = l / 16, i.e. the four amplitudes H[dmu][lb][k] (GetAmpLz kernel_calEva.cu:85-190 and the Pc
+// part of GetAmp2s :347-503): per group the coupling sums E_m = sum_entries lineshape * c_{k,m} are
+// formed once and contracted with DZ * AZ; the Lambda* lineshapes are split between the two lanes of
+// an event and exchanged.  mode 1: unweighted coherent |A|^2 to fx_out, no sums
+// (host_store_amp2s).
+//
+// FIX = false: lineshapes come from the per-point table only; an event whose mass the table cannot
+// serve is not evaluated but appended to defer[] (count in *defer_count).  FIX = true evaluates such
+// masses exactly (out of line); it runs over the deferred list (events [0, *n_list) of list) or,
+// without tables, over the whole segment.  Keeping the exact path out of the main kernel keeps its
+// register allocation free of the call's save/restore.
+template <bool FIX>
+__global__ void __launch_bounds__(EV_THREADS, 2)
+    k_unsmeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
+                const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int mode, int32_t* defer,
+                int* defer_count) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  PointTable& T = *reinterpret_cast<PointTable*>(sm);
+  load_table<EV_THREADS>(gtab, &T);
+  const int lane = threadIdx.x & 31, k = lane >> 4, el = lane & 15;
+  if (n_list) end = begin + *n_list;
+  const Chunk ch = block_chunk(end - begin, EV_WARPS * UNSMEARED_PER_WARP);
+  Acc acc;
+  for (int64_t base = ch.c0 + (threadIdx.x / 32) * UNSMEARED_PER_WARP; base < ch.c1;
+       base += EV_WARPS * UNSMEARED_PER_WARP) {
+    const int64_t p = base + el;
+    const bool valid = p < ch.c1;
+    const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? p : 0)};
+    const double mkp = E.mkp(), mz = E.mz();
+    // Lambda*: F_m = sum_r lineshape_r c_{r,k,m} DL_{r,k,m}
+    cplx F[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) F[m] = mk(0, 0);
+    {
+      const LstarKin lk = lstar_kin(T, mkp);
+      for (int r0 = 0; r0 < T.NR; r0 += 2) {
+        const int rm = r0 + k;
+        const cplx mine = (rm < T.NR) ? lstar_lineshape(T.L[rm], lk) : mk(0, 0);
+        const cplx other = shfl_xor(mine, 16);
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const int r = r0 + d;
+          if (r >= T.NR) break;
+          const LstarEntry& L = T.L[r];
+          const cplx q = (d == k) ? mine : other;
+#pragma unroll
+          for (int m = 0; m < 6; ++m) {
+            const cplx c = L.c[k * 6 + m];
+            if (!nonzero(c)) continue;
+            cmac(F[m], q * c, mk(E.DL(L.sidx, k, m), 0.0));
+          }
+        }
+      }
+    }
+    cplx H[4], HZ[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) H[q] = HZ[q] = mk(0, 0);
+    const int lmask = T.lstar_mmask[k];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      if (!(lmask >> m & 1)) continue;
+#pragma unroll
+      for (int ij = 0; ij < 4; ++ij) cmac(H[ij], E.A(ij >> 1, ij & 1, m), F[m]);
+    }
+    // Pc
+    bool deferred = false;
+    if (T.NZ > 0) {
+      TabAt ta;
+      const bool tab_ok = tab_at(T.tab, mz, ta);
+      cplx rawx[FIX ? MAX_PC : 1];
+      if (FIX && !tab_ok) pc_entries_exact(T, mz, rawx);
+      deferred = !FIX && !tab_ok;
+      for (int g = 0; g < T.ngroups; ++g) {
+        const PcGroup& gr = T.grp[g];
+        cplx Eg[12];
+#pragma unroll
+        for (int m = 0; m < 12; ++m) Eg[m] = mk(0, 0);
+        for (int q = 0; q < gr.count; ++q) {
+          const int pos = gr.first + q;
+          const cplx raw = tab_ok ? tab_get(ta, T.tab.stride, pos) : (FIX ? rawx[pos] : mk(0, 0));
+          const PcEntry& Z = T.Z[T.order[pos]];
+#pragma unroll
+          for (int m = 0; m < 12; ++m) {
+            const cplx c = Z.c[k * 12 + m];
+            if (nonzero(c)) cmac(Eg[m], raw, c);
+          }
+        }
+        const int gmask = gr.mmask[k];
+#pragma unroll
+        for (int m = 0; m < 12; ++m) {
+          if (!(gmask >> m & 1)) continue;
+          const cplx D = Eg[m] * E.DZ(gr.sidx, k, m);
+#pragma unroll
+          for (int ij = 0; ij < 4; ++ij) cmac(HZ[ij], E.AZ(ij >> 1, ij & 1, m), D);
+        }
+      }
+    }
+    double v = 0, vn = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      v += norm2(H[q] + HZ[q]);
+      vn += norm2(H[q]) + norm2(HZ[q]);
+    }
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    vn += __shfl_xor_sync(0xffffffffu, vn, 16);
+    if (k == 0 && valid) {
+      if (deferred) {
+        defer[atomicAdd(defer_count, 1)] = (int32_t)E.e;
+      } else if (mode == 1) {
+        fx_out[E.e] = v;
+      } else {
+        const float wf = E.w();
+        const bool data_w = wf <= -1000.f;
+        const double fxe = data_w ? v : v * (double)wf;
+        if (fx_out) fx_out[E.e] = fxe;
+        acc.add(E.e, ev.nda, ev.sw, fxe, data_w ? 0.0 : vn * (double)wf, false);
+      }
+    }
+  }
+  if (mode != 1) block_reduce_store<EV_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
+}
 
 template <int NB>
 __device__ __forceinline__ const float* smear_table();
@@ -449,250 +531,277 @@ __device__ __forceinline__ const float* smear_table<30>() { return kSmear30; }
 template <>
 __device__ __forceinline__ const float* smear_table<150>() { return kSmear150; }
 
-template <int NB>
-__global__ void __launch_bounds__(SMEAR_THREADS, PWA_SMEAR_MIN_BLOCKS)
-    k_smeared(EventSet ev, int64_t nda, int64_t begin, int64_t end, const int32_t* list,
-              const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmearShared& S = *reinterpret_cast<SmearShared*>(smem_raw);
-  load_table<SMEAR_THREADS>(gtab, &S.T);
-  const PointTable& T = S.T;
+// Per-warp scratch of the smeared kernels: Lambda* lineshapes of the warp's 4 events and, per event,
+// the Pc entry lineshapes at 8 resolution offsets.  Row and event strides are 4 words modulo 32
+// banks, so the 8 lanes of an event write their rows without bank conflicts.
+constexpr int RAW_ROW = MAX_PC + 1;
+constexpr int RAW_EVENT = 8 * RAW_ROW + 1;
+struct SmearWarp {
+  cplx q[SMEARED_PER_WARP][MAX_LSTAR];
+  cplx raw[SMEARED_PER_WARP * RAW_EVENT];
+};
+
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+constexpr size_t UNSMEARED_SMEM = align16(sizeof(PointTable));
+constexpr size_t SMEARED_SMEM = align16(sizeof(PointTable)) + EV_WARPS * sizeof(SmearWarp);
+
+// Events smeared over NB resolution offsets (kernel_store_fx_SMR / _finebinning, kernel_calEva.cu:
+// 819-900; TemplateGetAmp2s :583-784).  Lanes 8e .. 8e+7 of a warp hold event e; lane h holds the
+// helicity (dmu, lb, k) = (h/4, h/2 % 2, h % 2), its Lambda* amplitude H_L and, in registers, the Pc
+// angular amplitude HZ_q of every entry q (couplings included, lineshape excluded).  The offsets go
+// in rounds of 8: each lane evaluates all Pc entry lineshapes at one offset into the warp's scratch,
+// then every lane contracts S_b = sum_q lineshape_q(m_b) HZ_q for all 8 offsets.  Finally
+//   |A|^2 = sum_h |H_L|^2 + 2 w Re(conj(H_L) sum_b S_b) + w^2 u sum_b |S_b|^2,
+// the reference's BW1/BW2 form (kernel_calEva.cu:676-810) with its float weight w = float(1/NB)
+// and rescale u = float(1/w).  band = 1 for the two data bands (fx unweighted, no non-interference
+// term), 0 for the tail-region window events.
+//
+// FIX as for k_unsmeared: the main launch defers every event with a resolution offset the table
+// cannot serve.
+template <int NB, bool FIX>
+__global__ void __launch_bounds__(EV_THREADS, 2)
+    k_smeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
+              const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band, int32_t* defer,
+              int* defer_count) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  PointTable& T = *reinterpret_cast<PointTable*>(sm);
+  load_table<EV_THREADS>(gtab, &T);
+  SmearWarp& W = reinterpret_cast<SmearWarp*>(sm + align16(sizeof(PointTable)))[threadIdx.x / 32];
+  const int lane = threadIdx.x & 31, ei = lane >> 3, h = lane & 7;
+  const int hi = h >> 2, hj = (h >> 1) & 1, hk = h & 1;
   const float* qoff = smear_table<NB>();
-  // float weight 1/NBINS and its float reciprocal, as the reference (kernel_calEva.cu:676,771)
   const float wf = (float)(1.0 / NB);
   const double wgt = wf;
   const double c2 = wgt * wgt * (double)(1.0f / wf);
-  const int tid = threadIdx.x;
-  const int64_t count = end - begin;
-  const int64_t ntiles = (count + TILE - 1) / TILE;
+  if (n_list) end = begin + *n_list;
+  const Chunk ch = block_chunk(end - begin, EV_WARPS * SMEARED_PER_WARP);
+  cplx* R = W.raw + ei * RAW_EVENT;
+  // band 0: lookup 0 is at the event's own mass (|A|^2 without interference for the MC check sum)
+  const int shift = band ? 0 : 1;
+  const int nlook = NB + shift;
   Acc acc;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    // event indices of this tile
-    if (tid < TILE) {
-      const int64_t p = tile * TILE + tid;
-      S.ev[tid] = (p < count) ? (list ? (int64_t)list[begin + p] : begin + p) : -1;
-    }
-    __syncthreads();
-    // phase 1a: Lambda* lineshapes per (resonance, event)
-    for (int t = tid; t < T.NR * TILE; t += SMEAR_THREADS) {
-      const int r = t / TILE, el = t % TILE;
-      const int64_t e = S.ev[el];
-      S.Q[r][el] = (e >= 0) ? lstar_lineshape(T.L[r], lstar_kin(T, ldf(ev.pp, e))) : mk(0, 0);
-    }
-    __syncthreads();
-    // phase 1b/1c: helicity amplitudes; thread -> (event el, helicity h)
+  for (int64_t base = ch.c0 + (threadIdx.x / 32) * SMEARED_PER_WARP; base < ch.c1;
+       base += EV_WARPS * SMEARED_PER_WARP) {
+    const int64_t p = base + ei;
+    const bool valid = p < ch.c1;
+    const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? p : 0)};
+    const double mkp = E.mkp(), mz = E.mz();
     {
-      const int el = tid % TILE, h = tid / TILE;
-      const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
-      const int64_t e = S.ev[el];
-      cplx hl = mk(0, 0);
-      if (e >= 0) {
-        Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, e};
-        for (int r = 0; r < T.NR; ++r) {
-          const LstarEntry& L = T.L[r];
-          const cplx q = S.Q[r][el];
-          for (int m = 0; m < L.ncm; ++m) {
-            const cplx c = L.c[k * 6 + m];
-            if (c.re == 0.0 && c.im == 0.0) continue;
-            cmac(hl, E.A(i, j, m), (q * c) * E.DL(L.sidx, k, m));
-          }
-        }
-        cplx az[12];
-#pragma unroll
-        for (int m = 0; m < 12; ++m) az[m] = E.AZ(i, j, m);
-        for (int q = 0; q < T.NZ; ++q) {
-          const int zi = T.order[q];
-          const PcEntry& Z = T.Z[zi];
-          cplx hz = mk(0, 0);
-#pragma unroll
-          for (int m = 0; m < 12; ++m) {
-            const cplx c = Z.c[k * 12 + m];
-            if (c.re == 0.0 && c.im == 0.0) continue;
-            cmac(hz, az[m], c * E.DZ(Z.sidx, k, m));
-          }
-          S.HZre[q][h][el] = hz.re;
-          S.HZim[q][h][el] = hz.im;
-        }
-      } else {
-        for (int q = 0; q < T.NZ; ++q) S.HZre[q][h][el] = S.HZim[q][h][el] = 0.0;
-      }
-      S.HLre[h][el] = hl.re;
-      S.HLim[h][el] = hl.im;
+      const LstarKin lk = lstar_kin(T, mkp);
+      for (int r = h; r < T.NR; r += 8) W.q[ei][r] = lstar_lineshape(T.L[r], lk);
     }
-    __syncthreads();
-    // phase 2: offsets; thread -> (event el, lane b0), bins b0, b0+8, ...
-    {
-      const int el = tid / LANES_PER_EVENT, b0 = tid % LANES_PER_EVENT;
-      const int64_t e = S.ev[el];
-      cplx a1[8];
-      double a2[8];
+    __syncwarp();
+    cplx hl = mk(0, 0);
+    for (int r = 0; r < T.NR; ++r) {
+      const LstarEntry& L = T.L[r];
+      cplx f = mk(0, 0);
 #pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        a1[h] = mk(0, 0);
-        a2[h] = 0;
+      for (int m = 0; m < 6; ++m) {
+        const cplx c = L.c[hk * 6 + m];
+        if (nonzero(c)) cmac(f, c, E.A(hi, hj, m) * E.DL(L.sidx, hk, m));
       }
-      double vn = 0;
-      if (e >= 0) {
-        const double mz = ldf(ev.pp, e + ev.n_size);
-        const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
-        const bool need_noint = (band == 0) && (e >= nda) && !(__ldg(ev.pp + e + 2 * ev.n_size) <= -1000.f);
-        // b == -1 is the unsmeared evaluation for the MC non-interference sum
-        for (int b = (need_noint && b0 == 0) ? -1 : b0; b < NB; b += (b < 0) ? (1 + b0) : LANES_PER_EVENT) {
-          const double m = (b < 0) ? mz : mz + (double)qoff[b] * mres;
-          const PcKin kin = pc_kin(T, m);
-          cplx s8[8];
+      cmac(hl, W.q[ei][r], f);
+    }
+    cplx hz[MAX_PC];
 #pragma unroll
-          for (int h = 0; h < 8; ++h) s8[h] = mk(0, 0);
-          for (int g = 0; g < T.ngroups; ++g) {
-            cplx raw[MAX_GROUP_ENTRIES];
-            pc_group_lineshapes(T, g, kin, raw);
-            const PcGroup& gr = T.grp[g];
-            for (int q = 0; q < gr.count; ++q) {
-              const int qq = gr.first + q;
+    for (int q = 0; q < MAX_PC; ++q) hz[q] = mk(0, 0);
+    const int pmask = T.pc_mmask[hk];
 #pragma unroll
-              for (int h = 0; h < 8; ++h) cmac(s8[h], raw[q], mk(S.HZre[qq][h][el], S.HZim[qq][h][el]));
-            }
-          }
-          if (b < 0) {
+    for (int m = 0; m < 12; ++m) {
+      if (!(pmask >> m & 1)) continue;
+      const cplx az = E.AZ(hi, hj, m);
 #pragma unroll
-            for (int h = 0; h < 8; ++h) vn += norm2(mk(S.HLre[h][el], S.HLim[h][el])) + norm2(s8[h]);
-          } else {
-#pragma unroll
-            for (int h = 0; h < 8; ++h) {
-              a1[h] += s8[h];
-              a2[h] += norm2(s8[h]);
-            }
-          }
-        }
-      }
-      // reduce over the 8 lanes of this event (they are adjacent lanes of one warp)
-#pragma unroll
-      for (int o = 1; o < LANES_PER_EVENT; o <<= 1) {
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          a1[h].re += __shfl_xor_sync(0xffffffffu, a1[h].re, o);
-          a1[h].im += __shfl_xor_sync(0xffffffffu, a1[h].im, o);
-          a2[h] += __shfl_xor_sync(0xffffffffu, a2[h], o);
-        }
-        vn += __shfl_xor_sync(0xffffffffu, vn, o);
-      }
-      if (b0 == 0) {
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          S.A1re[h][el] = a1[h].re;
-          S.A1im[h][el] = a1[h].im;
-          S.A2[h][el] = a2[h];
-        }
-        S.VN[el] = vn;
+      for (int q = 0; q < MAX_PC; ++q) {
+        if (q >= T.NZ) break;
+        const PcEntry& Z = T.Z[T.order[q]];
+        const cplx c = Z.c[hk * 12 + m];
+        if (nonzero(c)) cmac(hz[q], c, az * E.DZ(Z.sidx, hk, m));
       }
     }
-    __syncthreads();
-    // phase 3: combine per event
-    if (tid < TILE) {
-      const int el = tid;
-      const int64_t e = S.ev[el];
-      if (e >= 0) {
-        double v = 0;
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          const cplx hl = mk(S.HLre[h][el], S.HLim[h][el]);
-          const cplx a1 = mk(S.A1re[h][el], S.A1im[h][el]);
-          v += norm2(hl) + 2.0 * wgt * (hl.re * a1.re + hl.im * a1.im) + c2 * S.A2[h][el];
-        }
-        double fxe = v, vnw = 0;
-        if (!band) {
-          const float wfe = __ldg(ev.pp + e + 2 * ev.n_size);
-          if (!(wfe <= -1000.f)) {
-            fxe = v * (double)wfe;
-            vnw = S.VN[el] * (double)wfe;
-          }
-        }
-        if (fx_out) fx_out[e] = fxe;
-        acc.add(e, nda, ev.sw, fxe, vnw, band != 0);
+    const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
+    double vn = 0, a2 = 0;
+    cplx a1 = mk(0, 0);
+    bool fail = false;
+    for (int l0 = 0; l0 < nlook; l0 += 8) {
+      const int l = l0 + h;
+      if (l < nlook) {
+        const int b = l - shift;
+        const double m = b < 0 ? mz : mz + (double)qoff[b] * mres;
+        if (FIX)
+          lookup_entries(T, m, R + h * RAW_ROW);
+        else
+          fail |= !lookup_table(T, m, R + h * RAW_ROW);
       }
+      __syncwarp();
+      const int nl = min(8, nlook - l0);
+      for (int bb = 0; bb < nl; ++bb) {
+        const cplx* r = R + bb * RAW_ROW;
+        cplx s = mk(0, 0);
+#pragma unroll
+        for (int q = 0; q < MAX_PC; ++q) {
+          if (q >= T.NZ) break;
+          cmac(s, r[q], hz[q]);
+        }
+        if (l0 + bb < shift) {
+          vn = norm2(hl) + norm2(s);
+        } else {
+          a1 += s;
+          a2 += norm2(s);
+        }
+      }
+      __syncwarp();
     }
-    __syncthreads();
+    double v = norm2(hl) + 2.0 * wgt * (hl.re * a1.re + hl.im * a1.im) + c2 * a2;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, o);
+      vn += __shfl_xor_sync(0xffffffffu, vn, o);
+    }
+    const bool deferred = !FIX && ((__ballot_sync(0xffffffffu, fail) >> (ei * 8)) & 0xFFu);
+    if (h == 0 && valid && deferred) defer[atomicAdd(defer_count, 1)] = (int32_t)E.e;
+    if (h == 0 && valid && !deferred) {
+      double fxe = v, vnw = 0;
+      if (!band) {
+        const float wfe = E.w();
+        if (!(wfe <= -1000.f)) {
+          fxe = v * (double)wfe;
+          vnw = vn * (double)wfe;
+        }
+      }
+      if (fx_out) fx_out[E.e] = fxe;
+      acc.add(E.e, ev.nda, ev.sw, fxe, vnw, band != 0);
+    }
+    __syncwarp();
   }
-  block_reduce_store<SMEAR_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
+  block_reduce_store<EV_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
 }
 
 // ------------------------------------------------------------------------------- tables
-// Exact K-matrix outputs at every grid node of every active J^P group.
+// Exact lineshapes of every Pc entry at every level-1 grid node.
 __global__ void k_build_tables(const PointTable* __restrict__ T, int n_nodes) {
-  const int64_t total = 4 * (int64_t)n_nodes;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int ik = (int)(t / n_nodes), j = (int)(t % n_nodes);
-    cplx* dst = const_cast<cplx*>(T->tab.data[ik]);
-    if (!dst) continue;
-    const double m = T->tab.m_lo + j * T->tab.h;
-    cplx out[TAB_SLOTS];
-#pragma unroll
-    for (int o = 0; o < TAB_SLOTS; ++o) out[o] = mk(0, 0);
-    km_solve(T->G[ik], m, T->ffb, out);
-#pragma unroll
-    for (int o = 0; o < TAB_SLOTS; ++o) dst[(size_t)j * TAB_SLOTS + o] = out[o];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *T->tab.nblocks = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_nodes; j += gridDim.x * blockDim.x) {
+    cplx* dst = const_cast<cplx*>(T->tab.data) + (size_t)j * T->tab.stride;
+    const PcKin kin = pc_kin(*T, T->tab.m_lo + j * T->tab.h);
+    for (int g = 0; g < T->ngroups; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first);
   }
 }
 
-// Verifies every interval [j, j+1] of every table: the 6-point interpolant at three interior points
-// against exact solves; flags the interval when the largest output error exceeds TAB_CHECK_TOL times
-// the largest output magnitude.
+// Interpolation check of one interval: stencil nodes base[0 .. 5] (node stride `stride`) against
+// exact evaluations at three interior points t of the interval [m0, m0 + step]; per Pc group, the
+// largest entry error must stay within TAB_CHECK_TOL of the group's largest entry.
+__device__ bool interval_ok(const PointTable& T, const cplx* base, int stride, double m0, double step) {
+  const double ts[3] = {0.2, 0.5, 0.8};
+  for (int pt = 0; pt < 3; ++pt) {
+    double w[6];
+    lagrange6(ts[pt], w);
+    const PcKin kin = pc_kin(T, m0 + ts[pt] * step);
+    for (int g = 0; g < T.ngroups; ++g) {
+      const PcGroup& gr = T.grp[g];
+      cplx ex[MAX_PC];
+      pc_group_exact(T, g, kin, ex);
+      double emax = 0, vmax = 0;
+      for (int q = 0; q < gr.count; ++q) {
+        cplx acc = mk(0, 0);
+        for (int n = 0; n < 6; ++n) acc += base[n * stride + gr.first + q] * w[n];
+        emax = fmax(emax, sqrt(norm2(acc - ex[q])));
+        vmax = fmax(vmax, sqrt(norm2(ex[q])));
+      }
+      if (!(isfinite(emax) && emax <= TAB_CHECK_TOL * vmax)) return false;
+    }
+  }
+  return true;
+}
+
+// True when [lo, hi] touches a guard interval; level 2 (sub = true) only keeps the stencil off the
+// guard centres (the non-smooth points themselves) and leaves the rest to the interpolation check.
+__device__ bool touches_guard(const LineTables& tab, double lo, double hi, bool sub) {
+  for (int q = 0; q < tab.nguard; ++q) {
+    double glo = tab.guard_lo[q], ghi = tab.guard_hi[q];
+    if (sub) glo = ghi = 0.5 * (glo + ghi);
+    if (hi >= glo && lo <= ghi) return true;
+  }
+  return false;
+}
+
+// Level-1 check of every interval; a failing interval gets a refinement block while blocks last.
 __global__ void k_check_tables(const PointTable* __restrict__ T, int n_nodes) {
-  const int64_t total = 4 * (int64_t)n_nodes;
   const LineTables& tab = T->tab;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int ik = (int)(t / n_nodes), j = (int)(t % n_nodes);
-    if (!tab.data[ik]) continue;
-    unsigned char* bad = const_cast<unsigned char*>(tab.bad[ik]);
+  int* cell = const_cast<int*>(tab.cell);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_nodes; j += gridDim.x * blockDim.x) {
     if (j < 2 || j + 3 >= n_nodes) {
-      bad[j] = 1;
+      cell[j] = -1;
       continue;
     }
-    const int nout = T->G[ik].npole + NKMC;
-    const cplx* base = tab.data[ik] + (size_t)(j - 2) * TAB_SLOTS;
-    bool ok = true;
-    // the stencil [m_{j-2}, m_{j+3}] must not reach into a guard interval
-    const double s_lo = tab.m_lo + (j - 2) * tab.h, s_hi = tab.m_lo + (j + 3) * tab.h;
-    for (int q = 0; q < tab.nguard; ++q)
-      if (s_hi >= tab.guard_lo[q] && s_lo <= tab.guard_hi[q]) ok = false;
-    const double ts[3] = {0.2, 0.5, 0.8};
-    for (int q = 0; q < 3 && ok; ++q) {
-      const double tt = ts[q];
-      const double d0 = tt + 2.0, d1 = tt + 1.0, d2 = tt, d3 = tt - 1.0, d4 = tt - 2.0, d5 = tt - 3.0;
-      const double w[6] = {d1 * d2 * d3 * d4 * d5 * (-1.0 / 120.0), d0 * d2 * d3 * d4 * d5 * (1.0 / 24.0),
-                           d0 * d1 * d3 * d4 * d5 * (-1.0 / 12.0), d0 * d1 * d2 * d4 * d5 * (1.0 / 12.0),
-                           d0 * d1 * d2 * d3 * d5 * (-1.0 / 24.0), d0 * d1 * d2 * d3 * d4 * (1.0 / 120.0)};
-      cplx ex[TAB_SLOTS];
-      km_solve(T->G[ik], tab.m_lo + (j + tt) * tab.h, T->ffb, ex);
-      double emax = 0, vmax = 0;
-      for (int o = 0; o < nout; ++o) {
-        cplx acc = mk(0, 0);
-        for (int k = 0; k < 6; ++k) acc += base[k * TAB_SLOTS + o] * w[k];
-        emax = fmax(emax, sqrt(norm2(acc - ex[o])));
-        vmax = fmax(vmax, sqrt(norm2(ex[o])));
+    const double m0 = tab.m_lo + j * tab.h;
+    bool ok = !touches_guard(tab, m0 - 2 * tab.h, m0 + 3 * tab.h, false);
+    if (ok) ok = interval_ok(*T, tab.data + (size_t)(j - 2) * tab.stride, tab.stride, m0, tab.h);
+    int c = 0;
+    if (!ok) {
+      const int b = atomicAdd(tab.nblocks, 1);
+      c = -1;
+      if (b < TAB_MAX_BLOCKS) {
+        tab.block_interval[b] = j;
+        c = b + 1;
       }
-      ok = isfinite(emax) && emax <= TAB_CHECK_TOL * vmax;
     }
-    bad[j] = ok ? 0 : 1;
+    cell[j] = c;
+  }
+}
+
+// Exact lineshapes at the nodes of every refinement block: node s of block b sits at
+// m_j + (s - 2) h / TAB_SUB.
+__global__ void k_build_sub(const PointTable* __restrict__ T) {
+  const LineTables& tab = T->tab;
+  const int nb = min(*tab.nblocks, TAB_MAX_BLOCKS);
+  const double hs = tab.h / TAB_SUB;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * TAB_SUB_NODES; t += gridDim.x * blockDim.x) {
+    const int b = t / TAB_SUB_NODES, s = t % TAB_SUB_NODES;
+    const double m = tab.m_lo + tab.block_interval[b] * tab.h + (s - 2) * hs;
+    cplx* dst = const_cast<cplx*>(tab.sub) + ((size_t)b * TAB_SUB_NODES + s) * tab.stride;
+    const PcKin kin = pc_kin(*T, m);
+    for (int g = 0; g < T->ngroups; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first);
+  }
+}
+
+// Check of every sub-interval of every refinement block.
+__global__ void k_check_sub(const PointTable* __restrict__ T) {
+  const LineTables& tab = T->tab;
+  const int nb = min(*tab.nblocks, TAB_MAX_BLOCKS);
+  const double hs = tab.h / TAB_SUB;
+  unsigned char* bad = const_cast<unsigned char*>(tab.sub_bad);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * TAB_SUB; t += gridDim.x * blockDim.x) {
+    const int b = t / TAB_SUB, i = t % TAB_SUB;
+    const double m0 = tab.m_lo + tab.block_interval[b] * tab.h + i * hs;
+    bool ok = !touches_guard(tab, m0 - 2 * hs, m0 + 3 * hs, true);
+    if (ok) ok = interval_ok(*T, tab.sub + ((size_t)b * TAB_SUB_NODES + i) * tab.stride, tab.stride, m0, hs);
+    bad[t] = ok ? 0 : 1;
   }
 }
 
 cudaError_t launch_build_tables(const PointTable* d_table, int n_nodes, int sm_count, cudaStream_t st) {
   k_build_tables<<<sm_count * 8, 128, 0, st>>>(d_table, n_nodes);
   k_check_tables<<<sm_count * 8, 128, 0, st>>>(d_table, n_nodes);
+  k_build_sub<<<sm_count * 4, 128, 0, st>>>(d_table);
+  k_check_sub<<<sm_count * 4, 128, 0, st>>>(d_table);
   return cudaGetLastError();
 }
 
-void attach_tables(PointTable* T, cplx* d_mem, unsigned char* d_flags) {
-  bool any = false;
-  for (int ik = 0; ik < 4; ++ik) {
-    bool used = false;
-    for (int g = 0; g < T->ngroups; ++g) used |= (T->grp[g].km == ik);
-    T->tab.data[ik] = used ? d_mem + (size_t)ik * TAB_NODES * TAB_SLOTS : nullptr;
-    T->tab.bad[ik] = used ? d_flags + (size_t)ik * TAB_NODES : nullptr;
-    any |= used;
-  }
-  T->tab.enabled = any ? 1 : 0;
+void attach_tables(PointTable* T, void* d_mem) {
+  LineTables& tb = T->tab;
+  unsigned char* p = static_cast<unsigned char*>(d_mem);
+  tb.data = reinterpret_cast<const cplx*>(p);
+  p += TAB_BYTES_DATA;
+  tb.cell = reinterpret_cast<const int*>(p);
+  p += TAB_BYTES_CELL;
+  tb.sub = reinterpret_cast<const cplx*>(p);
+  p += TAB_BYTES_SUB;
+  tb.sub_bad = p;
+  p += TAB_BYTES_SUB_BAD;
+  tb.nblocks = reinterpret_cast<int*>(p);
+  tb.block_interval = tb.nblocks + 1;
+  tb.stride = T->NZ > 0 ? T->NZ : 1;
+  tb.enabled = (T->NZ > 0 && d_mem) ? 1 : 0;
 }
 
 // ------------------------------------------------------------------------------- finalize
@@ -744,58 +853,100 @@ __global__ void k_finalize(const Partial* parts, int n, double sum_w_mc, double 
 }
 
 // ------------------------------------------------------------------------------- host side
-static int blocks_for(int64_t work, int per_block, int cap) {
-  int64_t b = (work + per_block - 1) / per_block;
-  if (b < 1) b = 1;
-  if (b > cap) b = cap;
-  return (int)b;
+// Resident blocks per SM of the event kernels by segment kind (from the occupancy calculator, set by
+// configure_kernels); a segment launches at most sm_count times that many blocks.
+static int g_occ[4] = {1, 1, 1, 1};
+
+static int events_per_block(int kind) {
+  return kind == SMEAR_NONE ? EV_WARPS * UNSMEARED_PER_WARP : EV_WARPS * SMEARED_PER_WARP;
 }
 
 int segment_blocks(const Segment& s, int sm_count) {
-  const int64_t n = s.end - s.begin;
-  if (s.kind == SMEAR_NONE) return blocks_for(n, UNSMEARED_THREADS, sm_count * 8);
-  return blocks_for((n + TILE - 1) / TILE, 1, sm_count * 2);
+  const int per = events_per_block(s.kind);
+  int64_t b = (s.end - s.begin + per - 1) / per;
+  const int64_t cap = (int64_t)sm_count * g_occ[s.kind];
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
 }
 
-static size_t smear_smem() { return sizeof(SmearShared); }
+// Blocks of the pass over a segment's deferred events (their number is known only on the device).
+static int fix_blocks(const Segment& s, int sm_count) { return sm_count * g_occ[s.kind]; }
 
-// A K-matrix group must have a channel layout (J^P in {1/2-, 3/2-, 1/2+, 3/2+}) and at most
-// NPMAX + NKMC outputs.
-static int G_valid_check(const KmGroup& G) { return (G.npole <= NPMAX) ? 0 : 1; }
+int segment_parts(const Segment& s, int sm_count, bool deferred) {
+  return segment_blocks(s, sm_count) + (deferred ? fix_blocks(s, sm_count) : 0);
+}
 
-cudaError_t launch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
-                           double* fx_out, int sm_count, cudaStream_t st) {
-  if (seg.end <= seg.begin) return cudaSuccess;
-  const int nb = segment_blocks(seg, sm_count);
-  const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
-  switch (seg.kind) {
+template <bool FIX>
+static void launch_kind(const EventSet& ev, int kind, int64_t begin, int64_t end, const int32_t* list,
+                        const int* n_list, const PointTable* d_table, Partial* out, double* fx_out, int mode,
+                        int32_t* defer, int* defer_count, int nb, cudaStream_t st) {
+  switch (kind) {
     case SMEAR_NONE:
-      k_unsmeared<<<nb, UNSMEARED_THREADS, 0, st>>>(ev, ev.nda, seg.begin, seg.end, seg.list, d_table, out, fx_out, 0);
+      k_unsmeared<FIX><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out,
+                                                                mode, defer, defer_count);
       break;
     case SMEAR_20:
-      k_smeared<20><<<nb, SMEAR_THREADS, smear_smem(), st>>>(ev, ev.nda, seg.begin, seg.end, seg.list, d_table, out,
-                                                             fx_out, band);
+      k_smeared<20, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 0,
+                                                                defer, defer_count);
       break;
     case SMEAR_30:
-      k_smeared<30><<<nb, SMEAR_THREADS, smear_smem(), st>>>(ev, ev.nda, seg.begin, seg.end, seg.list, d_table, out,
-                                                             fx_out, band);
+      k_smeared<30, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 1,
+                                                                defer, defer_count);
       break;
     case SMEAR_150:
-      k_smeared<150><<<nb, SMEAR_THREADS, smear_smem(), st>>>(ev, ev.nda, seg.begin, seg.end, seg.list, d_table, out,
-                                                              fx_out, band);
+      k_smeared<150, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 1,
+                                                                 defer, defer_count);
       break;
-    default:
-      return cudaErrorInvalidValue;
+  }
+}
+
+// One segment: with a deferral buffer (tables on), the table-only pass over the segment and then the
+// exact-capable pass over the events it deferred; without, the exact-capable pass over the segment.
+static cudaError_t launch_passes(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
+                                 double* fx_out, int mode, int32_t* defer, int* defer_count, int sm_count,
+                                 cudaStream_t st) {
+  if (seg.end <= seg.begin) return cudaSuccess;
+  if (seg.kind < SMEAR_NONE || seg.kind > SMEAR_150) return cudaErrorInvalidValue;
+  const int nb = segment_blocks(seg, sm_count);
+  if (defer) {
+    launch_kind<false>(ev, seg.kind, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, defer,
+                       defer_count, nb, st);
+    launch_kind<true>(ev, seg.kind, 0, 0, defer, defer_count, d_table, out ? out + nb : nullptr, fx_out, mode,
+                      nullptr, nullptr, fix_blocks(seg, sm_count), st);
+  } else {
+    launch_kind<true>(ev, seg.kind, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, nullptr,
+                      nullptr, nb, st);
   }
   return cudaGetLastError();
 }
 
+cudaError_t launch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
+                           double* fx_out, int32_t* defer, int* defer_count, int sm_count, cudaStream_t st) {
+  return launch_passes(ev, seg, d_table, out, fx_out, 0, defer, defer_count, sm_count, st);
+}
+
+template <class K>
+static cudaError_t configure_one(K kernel, size_t smem, int* occ) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  int n = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, EV_THREADS, smem))) return e;
+  *occ = n > 0 ? n : 1;
+  return cudaSuccess;
+}
+
 cudaError_t configure_kernels() {
-  const int smem = (int)smear_smem();
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_smeared<20>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return e;
-  if ((e = cudaFuncSetAttribute(k_smeared<30>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return e;
-  if ((e = cudaFuncSetAttribute(k_smeared<150>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return e;
+  int unused = 0;
+  if ((e = configure_one(k_unsmeared<false>, UNSMEARED_SMEM, &g_occ[SMEAR_NONE]))) return e;
+  if ((e = configure_one(k_unsmeared<true>, UNSMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<20, false>, SMEARED_SMEM, &g_occ[SMEAR_20]))) return e;
+  if ((e = configure_one(k_smeared<30, false>, SMEARED_SMEM, &g_occ[SMEAR_30]))) return e;
+  if ((e = configure_one(k_smeared<150, false>, SMEARED_SMEM, &g_occ[SMEAR_150]))) return e;
+  if ((e = configure_one(k_smeared<20, true>, SMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<30, true>, SMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<150, true>, SMEARED_SMEM, &unused))) return e;
   return cudaSuccess;
 }
 
@@ -805,12 +956,14 @@ cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, d
   return cudaGetLastError();
 }
 
-cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int sm_count, cudaStream_t st) {
-  if (ev.n <= 0) return cudaSuccess;
-  const int nb = blocks_for(ev.n, UNSMEARED_THREADS, sm_count * 8);
-  k_unsmeared<<<nb, UNSMEARED_THREADS, 0, st>>>(ev, 0, 0, ev.n, nullptr, d_table, nullptr, out, 1);
-  return cudaGetLastError();
+cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int32_t* defer, int* defer_count,
+                        int sm_count, cudaStream_t st) {
+  const Segment seg{SMEAR_NONE, 0, ev.n, nullptr};
+  return launch_passes(ev, seg, d_table, nullptr, out, 1, defer, defer_count, sm_count, st);
 }
+
+// A K-matrix group must have at most NPMAX poles.
+static int G_valid_check(const KmGroup& G) { return (G.npole <= NPMAX) ? 0 : 1; }
 
 // ------------------------------------------------------------------------------- point table
 // Masses in the table range where the reference's complex square root (csqrt_branch) changes branch
@@ -1068,6 +1221,25 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     }
   }
   T->ngroups = ng;
+  // helicity slots m with a non-zero coupling, per proton helicity k: Lambda* entries, all Pc
+  // entries, each Pc group
+  for (int r = 0; r < NR; ++r)
+    for (int k = 0; k < 2; ++k)
+      for (int m = 0; m < 6; ++m) {
+        const cplx c = T->L[r].c[k * 6 + m];
+        if (c.re != 0.0 || c.im != 0.0) T->lstar_mmask[k] |= 1 << m;
+      }
+  for (int g = 0; g < ng; ++g) {
+    PcGroup& gr = T->grp[g];
+    for (int q = 0; q < gr.count; ++q)
+      for (int k = 0; k < 2; ++k)
+        for (int m = 0; m < 12; ++m) {
+          const cplx c = T->Z[T->order[gr.first + q]].c[k * 12 + m];
+          if (c.re != 0.0 || c.im != 0.0) gr.mmask[k] |= 1 << m;
+        }
+    T->pc_mmask[0] |= gr.mmask[0];
+    T->pc_mmask[1] |= gr.mmask[1];
+  }
   // table grid and guard intervals (tables stay disabled until the caller attaches table memory)
   LineTables& tb = T->tab;
   tb.enabled = 0;
@@ -1116,17 +1288,9 @@ void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cp
   const LstarKin lk = lstar_kin(T, mkp);
   const PcKin pk = pc_kin(T, mz);
   for (int r = 0; r < T.NR; ++r) lstar[r] = lstar_lineshape(T.L[r], lk);
-  for (int g = 0; g < T.ngroups; ++g) {
-    const PcGroup& gr = T.grp[g];
-    cplx kmo[NPMAX + NKMC];
-    if (gr.km >= 0) km_solve(T.G[gr.km], mz, T.ffb, kmo);
-    for (int q = 0; q < gr.count; ++q) {
-      const int i = T.order[gr.first + q];
-      const PcEntry& Z = T.Z[i];
-      cplx v = (Z.type == LT_KM) ? kmo[Z.slot] : (Z.type == LT_BW) ? pc_bw(Z, pk) : mk(1, 0);
-      pc[i] = v * pc_barrier(Z, pk);
-    }
-  }
+  cplx raw[MAX_PC];
+  for (int g = 0; g < T.ngroups; ++g) pc_group_exact(T, g, pk, raw + T.grp[g].first);
+  for (int q = 0; q < T.NZ; ++q) pc[T.order[q]] = raw[q];
 }
 
 }  // namespace pwa

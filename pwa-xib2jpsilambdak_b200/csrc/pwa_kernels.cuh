@@ -45,25 +45,30 @@ struct Segment {
   const int32_t* list;  // event indices, [begin, end) positions in the list otherwise
 };
 
-// Number of partial slots a segment uses for a given launch width.
+// Blocks of the pass over a segment (and partial slots of that pass).
 int segment_blocks(const Segment& s, int sm_count);
+
+// Partial slots a segment uses: its pass, plus the pass over deferred events when deferred is true.
+int segment_parts(const Segment& s, int sm_count, bool deferred);
 
 // Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                       float ffr, float ffb, PointTable* out);
 
-// Launches one segment; partials written at out[0 .. segment_blocks).  fx_out (optional) receives
-// per-event fx (weighted by w for MC, like the reference's d_fx).
+// Launches one segment; partials written at out[0 .. segment_parts).  fx_out (optional) receives
+// per-event fx (weighted by w for MC, like the reference's d_fx).  With the lineshape tables on, defer
+// (room for the segment's events) and defer_count (zeroed before the launch) receive the events the
+// tables cannot serve, which a second pass evaluates exactly; with tables off both are null.
 cudaError_t launch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_table, Partial* out,
-                           double* fx_out, int sm_count, cudaStream_t st);
+                           double* fx_out, int32_t* defer, int* defer_count, int sm_count, cudaStream_t st);
 
-// Fills the per-point K-matrix tables T->tab.data[ik] (null for groups without table memory) from
-// the device copy of the point table and verifies every interval (two launches).
+// Fills the per-point Pc entry tables from the device copy of the point table, verifies every
+// interval, refines and verifies the failing ones (four launches).
 cudaError_t launch_build_tables(const PointTable* d_table, int n_nodes, int sm_count, cudaStream_t st);
 
-// Attaches table memory (4 * TAB_NODES * TAB_SLOTS complex values and 4 * TAB_NODES interval flags)
-// to a host point table: enables interpolation for the K-matrix groups the model uses.
-void attach_tables(PointTable* T, cplx* d_mem, unsigned char* d_flags);
+// Attaches TAB_BYTES of device memory (256-byte aligned) for the two-level tables to a host point
+// table: enables interpolation of the Pc lineshapes.
+void attach_tables(PointTable* T, void* d_mem);
 
 // Reduces nparts partials and assembles the NLL.
 cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, double sum_w_data,
@@ -73,6 +78,7 @@ cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, d
 void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cplx* pc);
 
 // Per-event unsmeared |A|^2 without weights (host_store_amp2s semantics) for n events.
-cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int sm_count, cudaStream_t st);
+cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int32_t* defer, int* defer_count,
+                        int sm_count, cudaStream_t st);
 
 }  // namespace pwa

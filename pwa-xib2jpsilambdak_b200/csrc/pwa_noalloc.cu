@@ -185,7 +185,7 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
   if (tot > kMaxParts) return finish(PWA_E_SIZE);
   const EventSet ev{d_pp, d_pp1, d_pp2, d_sw, n_size, n, nda};
   for (int i = 0; i < nseg; ++i)
-    if (launch_segment(ev, segs[i], d_table, d_parts + offs[i], nullptr, sm_count, st) != cudaSuccess)
+    if (launch_segment(ev, segs[i], d_table, d_parts + offs[i], nullptr, nullptr, nullptr, sm_count, st) != cudaSuccess)
       return finish(PWA_E_CUDA);
   if (launch_finalize(d_parts, std::max(tot, 1), sum_w_mc, sum_w_data, nll_shift, d_res, st) != cudaSuccess)
     return finish(PWA_E_CUDA);

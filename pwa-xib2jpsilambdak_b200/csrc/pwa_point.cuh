@@ -57,38 +57,62 @@ struct PcGroup {
   int km;       // K-matrix group index (0..3) or -1
   int sidx;     // common spin index
   int first, count;  // range in PointTable::order
+  int mmask[2];      // helicity slots with a non-zero coupling in any entry, per proton helicity
 };
 
-// Per-point tables of the K-matrix P-vector outputs on a uniform m(J/psi p) grid, interpolated with
-// 6-point Lagrange polynomials.  Guard intervals surround every mass where the reference's lineshape
-// is not smooth (real-mass thresholds, the branch switches of its complex square root, the pole
-// clamp |m0^2 - s| < 1e-3, the upper kinematic edge).  In addition every grid interval is verified
-// after the table is built: its interpolant is compared with exact solves at interior points, and
-// intervals off by more than TAB_CHECK_TOL (parameter-dependent narrow states, e.g. a K-matrix pole
-// just below a real-mass threshold) are flagged.  Lookups in a guard interval, a flagged interval or
-// near the grid ends evaluate the K-matrix exactly.
+// Per-point tables of every Pc entry's lineshape (production barrier included; all of them depend on
+// m(J/psi p) only) on a uniform grid, interpolated with 6-point Lagrange polynomials.  Guard
+// intervals surround every mass where the reference's lineshapes are not smooth (real-mass
+// thresholds, the branch switches of its complex square root, the K-matrix pole clamp
+// |m0^2 - s| < 1e-3, the upper kinematic edge).  In addition every grid interval is verified after
+// the table is built: its interpolant is compared with exact evaluations at interior points, group by
+// group, and intervals off by more than TAB_CHECK_TOL relative to the group's largest entry
+// (parameter-dependent narrow states, e.g. a K-matrix pole just below a real-mass threshold) are
+// flagged and refined.  Lookups that neither level can serve, and those near the grid ends, evaluate
+// the lineshapes exactly.
 constexpr int MAX_GUARDS = 48;
+// Intervals that fail the check are refined: each gets a block of TAB_SUB sub-intervals (step
+// h / TAB_SUB) with TAB_SUB + 5 nodes (the 6-point stencils of all sub-intervals), verified the same
+// way.  Up to TAB_MAX_BLOCKS intervals are refined per point; the others and sub-intervals that fail
+// again are evaluated exactly.
+constexpr int TAB_SUB = 16;
+constexpr int TAB_SUB_NODES = TAB_SUB + 5;
+constexpr int TAB_MAX_BLOCKS = 4096;
 struct LineTables {
   int enabled;
-  int n_nodes;
+  int n_nodes, stride;  // stride: complex values per node (= NZ, entries in group order)
   double m_lo, h, inv_h;
   int nguard;
   double guard_lo[MAX_GUARDS], guard_hi[MAX_GUARDS];
-  const cplx* data[4];          // per K-matrix J^P group: [node][output], NPMAX + NKMC outputs per node
-  const unsigned char* bad[4];  // per group and interval: 1 when the interpolant failed the check
+  const cplx* data;   // [node][order position]
+  const int* cell;    // per interval [j, j+1]: 0 interpolate, -1 exact, b + 1 refined in block b
+  const cplx* sub;    // [block][TAB_SUB_NODES][order position]
+  const unsigned char* sub_bad;  // [block][TAB_SUB]: 1 when lookups must evaluate exactly
+  int* nblocks;       // refined-block counter (reset by the build kernel)
+  int* block_interval;  // [block] -> interval j
 };
 constexpr double TAB_CHECK_TOL = 1e-11;
 constexpr double TAB_M_LO = 4.030, TAB_M_HI = 5.130, TAB_H = 1e-5;  // GeV
 constexpr int TAB_NODES = 110001;
-constexpr int TAB_SLOTS = NPMAX + NKMC;
+// Device memory a context attaches for the tables (bytes, 256-aligned parts).
+constexpr size_t tab_align(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t TAB_BYTES_DATA = tab_align((size_t)TAB_NODES * MAX_PC * 16);
+constexpr size_t TAB_BYTES_CELL = tab_align((size_t)TAB_NODES * 4);
+constexpr size_t TAB_BYTES_SUB = tab_align((size_t)TAB_MAX_BLOCKS * TAB_SUB_NODES * MAX_PC * 16);
+constexpr size_t TAB_BYTES_SUB_BAD = tab_align((size_t)TAB_MAX_BLOCKS * TAB_SUB);
+constexpr size_t TAB_BYTES_BLOCKS = tab_align((size_t)(TAB_MAX_BLOCKS + 1) * 4);
+constexpr size_t TAB_BYTES =
+    TAB_BYTES_DATA + TAB_BYTES_CELL + TAB_BYTES_SUB + TAB_BYTES_SUB_BAD + TAB_BYTES_BLOCKS;
 
-struct PointTable {
+struct alignas(16) PointTable {
   int NR, NZ, ngroups;
   int status;  // 0 ok, else a PWA_E_* code
   // Blatt-Weisskopf orders L in use (bit L set): decay barriers of the Lambda* Breit-Wigners, their
   // production barriers, production barriers of the Pc entries, decay barriers of Pc Breit-Wigners;
   // needs_sigma_pi: a Lambda* below the pK threshold uses the Sigma pi channel momentum.
   int lmask_lstar_R, lmask_lstar_B, lmask_pc_B, lmask_pc_R, needs_sigma_pi;
+  // helicity slots m (bit m) with a non-zero coupling, per proton helicity k
+  int lstar_mmask[2], pc_mmask[2];
   double ffr, ffb;
   LstarEntry L[MAX_LSTAR];
   PcEntry Z[MAX_PC];
