@@ -241,15 +241,17 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     seg_time = {}
+    seg_deferred = {}
     kernel_ms = 0.0
     launches = 0
     for _ in range(args.steps):
         r = step()
         kernel_ms += ctx.last_kernel_ms()
         launches += ctx.last_launches()
-        for kind, n, ms in ctx.segments():
+        for (kind, n, ms), nd in zip(ctx.segments(), ctx.segments_deferred()):
             t, _ = seg_time.get(kind, (0.0, n))
             seg_time[kind] = (t + ms, n)
+            seg_deferred[kind] = nd
     e1.record(stream)
     torch.cuda.synchronize(dev)
     dev_ms = e0.elapsed_time(e1)
@@ -291,7 +293,8 @@ def main():
                                                                                "thresholds"},
            "gpu_launches": launches,
            "kernel_shares": shares,
-           "segments": {names[k]: {"events": int(n), "ms_per_step": round(t / args.steps, 4),
+           "segments": {names[k]: {"events": int(n), "deferred_to_exact": int(seg_deferred.get(k, 0)),
+                                   "ms_per_step": round(t / args.steps, 4),
                                    "ns_per_event": round(t / args.steps / max(n, 1) * 1e6, 3)}
                         for k, (t, n) in seg_time.items()},
            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -94,6 +94,9 @@ void* pwa_ctx_stream(pwa_ctx* ctx);
 int pwa_ctx_set_timing(pwa_ctx* ctx, int on);
 int pwa_ctx_segment_count(pwa_ctx* ctx);
 int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double* last_ms);
+/* With timing on: events of segment i that the last evaluation deferred from the table-only pass to
+ * the exact pass (lineshape masses the interpolation tables cannot serve).  No reference counterpart. */
+int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
 
 /* K-matrix lineshape tables (default on): each evaluation first tabulates the exact FP64 K-matrix
  * outputs on a 10 keV m(J/psi p) grid and interpolates them (6-point Lagrange), evaluating exactly

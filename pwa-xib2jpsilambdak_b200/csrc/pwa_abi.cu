@@ -70,6 +70,7 @@ struct pwa_ctx {
   int timing = 0;
   std::vector<cudaEvent_t> seg_ev;
   std::vector<double> seg_ms;
+  int h_defer_cnt[8] = {};  // deferred events per segment of the last timed evaluation
 };
 
 namespace {
@@ -323,6 +324,9 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
   c->last_ms = ms;
   if (c->timing) {
     c->seg_ms.assign(c->segs.size(), 0.0);
+    std::memset(c->h_defer_cnt, 0, sizeof(c->h_defer_cnt));
+    if (c->h_table->tab.enabled)
+      PWA_CUDA(cudaMemcpy(c->h_defer_cnt, c->d_defer_cnt, sizeof(c->h_defer_cnt), cudaMemcpyDeviceToHost));
     cudaEvent_t prev = c->e0;
     for (size_t i = 0; i < c->segs.size(); ++i) {
       float m = 0;
@@ -398,6 +402,12 @@ int pwa_ctx_segment_info(pwa_ctx* c, int i, int* kind, int64_t* events, double* 
   if (kind) *kind = c->segs[i].kind;
   if (events) *events = c->segs[i].end - c->segs[i].begin;
   if (last_ms) *last_ms = (i < (int)c->seg_ms.size()) ? c->seg_ms[i] : 0.0;
+  return PWA_OK;
+}
+
+int pwa_ctx_segment_deferred(pwa_ctx* c, int i, int64_t* deferred) {
+  if (!c || !deferred || i < 0 || i >= (int)c->segs.size() || i >= 8) return PWA_E_ARG;
+  *deferred = c->timing ? c->h_defer_cnt[i] : 0;
   return PWA_OK;
 }
 

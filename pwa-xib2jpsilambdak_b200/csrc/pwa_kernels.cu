@@ -386,17 +386,19 @@ __device__ __forceinline__ int64_t event_index(const int32_t* list, int64_t begi
   return list ? (int64_t)list[begin + p] : begin + p;
 }
 
-// Contiguous share [c0, c1) of a segment's count positions for this block, a whole number of rounds
-// long: consecutive rounds of a block take neighbouring events (masses), whose lineshape-table nodes
-// stay in L1.
+// Work of this warp: groups warp0, warp0 + wstep, ... of positions [c0, c1).  Segments give each block
+// a contiguous share, a whole number of rounds long, so consecutive rounds of a block take
+// neighbouring events (masses) whose lineshape-table nodes stay in L1.  Deferred lists (few events,
+// no mass order) are spread over all warps of the grid instead.
 struct Chunk {
-  int64_t c0, c1;
+  int64_t c0, c1, warp0, wstep;
 };
-__device__ __forceinline__ Chunk block_chunk(int64_t count, int per_round) {
+__device__ __forceinline__ Chunk block_chunk(int64_t count, int per_round, bool interleave) {
+  if (interleave) return Chunk{0, count, (int64_t)blockIdx.x * EV_WARPS + threadIdx.x / 32, (int64_t)gridDim.x * EV_WARPS};
   int64_t chunk = (count + gridDim.x - 1) / gridDim.x;
   chunk = (chunk + per_round - 1) / per_round * per_round;
   const int64_t c0 = (int64_t)blockIdx.x * chunk;
-  return Chunk{c0, min(count, c0 + chunk)};
+  return Chunk{c0, min(count, c0 + chunk), threadIdx.x / 32, EV_WARPS};
 }
 
 // Unsmeared events.  Lane l of a warp takes event l % 16 of the warp's 16 and proton helicity
@@ -421,10 +423,9 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
   load_table<EV_THREADS>(gtab, &T);
   const int lane = threadIdx.x & 31, k = lane >> 4, el = lane & 15;
   if (n_list) end = begin + *n_list;
-  const Chunk ch = block_chunk(end - begin, EV_WARPS * UNSMEARED_PER_WARP);
+  const Chunk ch = block_chunk(end - begin, EV_WARPS * UNSMEARED_PER_WARP, n_list != nullptr);
   Acc acc;
-  for (int64_t base = ch.c0 + (threadIdx.x / 32) * UNSMEARED_PER_WARP; base < ch.c1;
-       base += EV_WARPS * UNSMEARED_PER_WARP) {
+  for (int64_t base = ch.c0 + ch.warp0 * UNSMEARED_PER_WARP; base < ch.c1; base += ch.wstep * UNSMEARED_PER_WARP) {
     const int64_t p = base + el;
     const bool valid = p < ch.c1;
     const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? p : 0)};
@@ -574,14 +575,13 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
   const double wgt = wf;
   const double c2 = wgt * wgt * (double)(1.0f / wf);
   if (n_list) end = begin + *n_list;
-  const Chunk ch = block_chunk(end - begin, EV_WARPS * SMEARED_PER_WARP);
+  const Chunk ch = block_chunk(end - begin, EV_WARPS * SMEARED_PER_WARP, n_list != nullptr);
   cplx* R = W.raw + ei * RAW_EVENT;
   // band 0: lookup 0 is at the event's own mass (|A|^2 without interference for the MC check sum)
   const int shift = band ? 0 : 1;
   const int nlook = NB + shift;
   Acc acc;
-  for (int64_t base = ch.c0 + (threadIdx.x / 32) * SMEARED_PER_WARP; base < ch.c1;
-       base += EV_WARPS * SMEARED_PER_WARP) {
+  for (int64_t base = ch.c0 + ch.warp0 * SMEARED_PER_WARP; base < ch.c1; base += ch.wstep * SMEARED_PER_WARP) {
     const int64_t p = base + ei;
     const bool valid = p < ch.c1;
     const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? p : 0)};
@@ -687,12 +687,13 @@ __global__ void k_build_tables(const PointTable* __restrict__ T, int n_nodes) {
   }
 }
 
-// Interpolation check of one interval: stencil nodes base[0 .. 5] (node stride `stride`) against
-// exact evaluations at three interior points t of the interval [m0, m0 + step]; per Pc group, the
-// largest entry error must stay within TAB_CHECK_TOL of the group's largest entry.
+// Interpolation check of one interval: stencil nodes base[0 .. 5] (node stride `stride`) against an
+// exact evaluation at the midpoint of the interval [m0, m0 + step], where the error factor
+// prod_n (t - t_n) of the centred 6-point stencil peaks; per Pc group, the largest entry error must
+// stay within TAB_CHECK_TOL of the group's largest entry.
 __device__ bool interval_ok(const PointTable& T, const cplx* base, int stride, double m0, double step) {
-  const double ts[3] = {0.2, 0.5, 0.8};
-  for (int pt = 0; pt < 3; ++pt) {
+  const double ts[1] = {0.5};
+  for (int pt = 0; pt < 1; ++pt) {
     double w[6];
     lagrange6(ts[pt], w);
     const PcKin kin = pc_kin(T, m0 + ts[pt] * step);

@@ -17,7 +17,7 @@ LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().pare
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
             "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
-            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_point_table_bytes",
+            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
 
@@ -59,6 +59,7 @@ def load() -> C.CDLL:
         L.pwa_ctx_set_timing.argtypes = [C.c_void_p, C.c_int]
         L.pwa_ctx_set_lineshape_tables.argtypes = [C.c_void_p, C.c_int]
         L.pwa_ctx_segment_count.argtypes = [C.c_void_p]
+        L.pwa_ctx_segment_deferred.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]
         L.pwa_ctx_segment_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64),
                                            C.POINTER(C.c_double)]
         L.pwa_point_table_bytes.restype = C.c_int64
@@ -172,6 +173,15 @@ class Context:
             k, n, ms = C.c_int(), C.c_int64(), C.c_double()
             check(self.L.pwa_ctx_segment_info(self.h, i, C.byref(k), C.byref(n), C.byref(ms)), "segment_info")
             out.append((k.value, n.value, ms.value))
+        return out
+
+    def segments_deferred(self) -> list:
+        """Events per segment the last timed evaluation deferred to the exact pass."""
+        out = []
+        for i in range(self.L.pwa_ctx_segment_count(self.h)):
+            d = C.c_int64()
+            check(self.L.pwa_ctx_segment_deferred(self.h, i, C.byref(d)), "segment_deferred")
+            out.append(d.value)
         return out
 
     def stream(self) -> int:
