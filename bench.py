@@ -30,6 +30,9 @@ sys.path.insert(0, str(ROOT / "pwa-xib2jpsilambdak_b200"))
 METRIC = "NLL evals/s, 5M-event K-matrix model"
 WORKLOAD = {"name": "kmatrix", "n_data": 500_000, "n_mc": 5_000_000, "w_range": (0.2, 1.0)}
 CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
+# DRAM bytes read + written per event of a segment (table-only and exact passes together), from one
+# ncu capture of the 50k data + 500k MC case; the traffic of a launch scales with its events.
+DRAM_BYTES_PER_EVENT = {1: 1304.0}
 
 
 def parse():
@@ -248,10 +251,10 @@ def main():
         r = step()
         kernel_ms += ctx.last_kernel_ms()
         launches += ctx.last_launches()
-        for (kind, n, ms), nd in zip(ctx.segments(), ctx.segments_deferred()):
+        for (kind, n, ms), n_def in zip(ctx.segments(), ctx.segments_deferred()):
             t, _ = seg_time.get(kind, (0.0, n))
             seg_time[kind] = (t + ms, n)
-            seg_deferred[kind] = nd
+            seg_deferred[kind] = n_def
     e1.record(stream)
     torch.cuda.synchronize(dev)
     dev_ms = e0.elapsed_time(e1)
@@ -298,7 +301,10 @@ def main():
                                    "ns_per_event": round(t / args.steps / max(n, 1) * 1e6, 3)}
                         for k, (t, n) in seg_time.items()},
            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                        "frac": achieved / hbm, "traffic": None,
+                        "frac": achieved / hbm,
+                        "traffic": (DRAM_BYTES_PER_EVENT[dom] * seg_time[dom][1]
+                                    if dom in DRAM_BYTES_PER_EVENT else None),
+                        "traffic_unit": "bytes per step of this segment (ncu, scaled by events)",
                         "note": f"algorithmic bytes = {req_b} B per event (planes the model reads) of the "
                                 f"{full_b} B reference row; peak {peak_kind}"},
            "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(lib.load().pwa_point_table_bytes()),
