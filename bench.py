@@ -27,7 +27,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "pwa-xib2jpsilambdak_b200"))
 
-METRIC = "NLL evals/s, 5M-event K-matrix model"
+METRIC = "NLL evals/s, 5M-event K-matrix model: batched vs plain on B200, |dNLL|<=1e-4"
 WORKLOAD = {"name": "kmatrix", "n_data": 500_000, "n_mc": 5_000_000, "w_range": (0.2, 1.0)}
 CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
 # DRAM bytes read + written per event of a segment (table-only and exact passes together), from one
@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
     ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
+    ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
     return ap.parse_args()
 
 
@@ -263,11 +264,55 @@ def main():
     for _ in range(args.steps):
         step()
     e2e_ms = (time.perf_counter() - t0) * 1e3
+
+    # batched: one step = one batch of the 2N+1 points of Minuit's numerical gradient
+    bat = None
+    if not args.plain_only:
+        from pwa_b200 import gradient
+        labels, gblocks = gradient.gradient_blocks(mdl, vals)
+        npts = len(gblocks)
+        bsums = torch.zeros((npts, 3), dtype=torch.float64, device=dev)
+
+        def bstep():
+            res, ns = ctx.eval_nll_batch(gblocks)
+            if world > 1:
+                bsums.copy_(torch.tensor([[x.data_term, x.sumint, x.sum_noint] for x in res], dtype=torch.float64))
+                dist.all_reduce(bsums)
+            return res, ns
+
+        for _ in range(max(args.warmup, 3)):
+            bres, nstruct = bstep()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        blaunch = 0
+        for _ in range(args.steps):
+            bres, nstruct = bstep()
+            blaunch += ctx.last_launches()
+        b1.record(stream)
+        torch.cuda.synchronize(dev)
+        bdev_ms = b0.elapsed_time(b1)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            bstep()
+        be2e_ms = (time.perf_counter() - t0) * 1e3
+        # |dNLL| of the batched points against one-by-one evaluation, one point of every kind
+        probe = ["a_p1p1_1520", "m0_1670", "width_1810", "scRe", "a_L0_Pc4312", "p_Bp_ZM1SC1", "a_L1_ZM3SC1",
+                 "g1_Pc4312", "m0_Pc4440", "g3_Pc4500", "fsc_ZM3SC2"]
+        idx = [0] + [labels.index((n, +1)) for n in probe if (n, +1) in labels]
+        dmax = max(abs(bres[i].nll - ctx.eval_nll(gblocks[i]).nll) for i in idx)
+        bat = dict(npts=npts, nstruct=nstruct, dev_ms=bdev_ms, e2e_ms=be2e_ms, launches=blaunch, dnll=dmax,
+                   nprobe=len(idx))
     clocks = clk.stop()
     if world > 1:
-        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
+        t = torch.tensor([dev_ms, e2e_ms, bat["dev_ms"] if bat else 0.0, bat["e2e_ms"] if bat else 0.0],
+                         dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, e2e_ms = t.tolist()
+        dev_ms, e2e_ms, bd, be = t.tolist()
+        if bat:
+            bat["dev_ms"], bat["e2e_ms"] = bd, be
         dist.barrier()
     if rank != 0:
         if world > 1:
@@ -333,10 +378,48 @@ def main():
         except Exception as ex:  # the baseline is reported, never required for the GPU number
             out["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"failed: {ex}"}
+    if bat:
+        out = batched_line(out, bat, args, world, sample, req_b, hbm, peak_kind)
     print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, hbm: float, peak_kind: str) -> dict:
+    """The bench line with the batched gradient evaluation as the headline and the plain single-point
+    measurement kept under "plain"."""
+    from pwa_b200 import lib
+    npts = bat["npts"]
+    value = world * npts * args.steps / (bat["dev_ms"] / 1e3)
+    e2e = world * npts * args.steps / (bat["e2e_ms"] / 1e3)
+    ms_step = bat["dev_ms"] / args.steps
+    events = sample.n
+    achieved = events * req_b / (ms_step / 1e3) / 1e9
+    keep = ("value", "ms_per_step", "gpu_launches", "kernel_shares", "segments", "roofline", "e2e")
+    out = {k: v for k, v in plain.items() if k not in keep}
+    out["plain"] = {k: plain[k] for k in keep if k in plain}
+    out["plain"]["note"] = "one step = one single-point evaluation (pwa_ctx_eval_nll)"
+    pt_bytes = int(lib.load().pwa_point_table_bytes())
+    out.update({
+        "value": value, "ms_per_step": ms_step, "gpu_launches": bat["launches"],
+        "batched_vs_plain": value / plain["value"],
+        "batch": {"points_per_step": npts, "points_from_centre": bat["nstruct"],
+                  "points_one_by_one": npts - bat["nstruct"],
+                  "max_abs_dnll_vs_single_point": bat["dnll"], "probed_points": bat["nprobe"],
+                  "step": "the 2N+1 parameter points of Minuit's numerical gradient (centre, +-h per parameter) "
+                          "in one pwa_ctx_eval_nll_batch call; every point's NLL is computed in FP64"},
+        "roofline": {"bound": "hbm", "kernel": "k_batch (all launches of one gradient batch)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "note": f"algorithmic bytes = {req_b} B per event read once per batch; FP64-issue bound, "
+                             f"peak {peak_kind}"},
+        "e2e": {"value": e2e, "unit": "evals/s",
+                "h2d_bytes_per_step": (npts + 1) * pt_bytes + npts * (8 * 24 * 16 + 96),
+                "d2h_bytes_per_step": npts * 48},
+    })
+    out["config"] = dict(out["config"], precision="FP64; batched points formed from the centre's per-event terms",
+                         step="one Minuit gradient batch (2N+1 points)")
+    return out
 
 
 if __name__ == "__main__":

@@ -79,6 +79,23 @@ int pwa_ctx_eval_nll(pwa_ctx* ctx, const float* h_paraList, int para_size, int v
                      int NR, int NZ, int NX, float FFR, float FFB, double sum_w_mc, double sum_w_data,
                      double nll_shift, pwa_result* out, double* h_fx);
 
+/* Likelihood at npoints parameter points in one call; point p's float block starts at
+ * h_paraLists + p * block_stride (same sizes and model for all points).  Made for the 2N+1 points of
+ * Minuit's numerical gradient (RooMinuit/Minuit2 calling host_store_fx once per point,
+ * kernel_calEva.cu:1186-1363): points that differ from point 0 in the couplings or lineshape of one
+ * Lambda*, in the couplings of up to 8 Pc entries, or in the lineshapes of one Pc group are evaluated
+ * together in one pass over the events from the centre's per-event terms (exact FP64); other points
+ * go through pwa_ctx_eval_nll one by one.  n_structured (optional) receives the number of points of
+ * the first kind.  out: npoints results. */
+int pwa_ctx_eval_nll_batch(pwa_ctx* ctx, const float* h_paraLists, int npoints, int block_stride, int para_size,
+                           int vamp_size, int spline_size, int NR, int NZ, int NX, float FFR, float FFB,
+                           double sum_w_mc, double sum_w_data, double nll_shift, pwa_result* out,
+                           int* n_structured);
+
+/* Device time of the last pwa_ctx_eval_nll_batch in milliseconds (CUDA events; includes the points
+ * evaluated one by one). */
+double pwa_ctx_last_batch_ms(pwa_ctx* ctx);
+
 /* Per-event unsmeared |A|^2 for toy weights (host_store_amp2s, kernel_calEva.cu:1376-1419). */
 int pwa_ctx_amp2(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR,
                  int NZ, int NX, float FFR, float FFB, double* h_amp2);

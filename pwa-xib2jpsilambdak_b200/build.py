@@ -10,7 +10,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "pwa_b200" / "libpwa_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["pwa_kernels.cu", "pwa_abi.cu", "pwa_generate.cu", "pwa_noalloc.cu", "kernel_calEva_compat.cpp"]
+SOURCES = ["pwa_kernels.cu", "pwa_batch.cu", "pwa_abi.cu", "pwa_generate.cu", "pwa_noalloc.cu", "kernel_calEva_compat.cpp"]
 
 
 def needs_build() -> bool:

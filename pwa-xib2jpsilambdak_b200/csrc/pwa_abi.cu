@@ -71,6 +71,16 @@ struct pwa_ctx {
   std::vector<cudaEvent_t> seg_ev;
   std::vector<double> seg_ms;
   int h_defer_cnt[8] = {};  // deferred events per segment of the last timed evaluation
+  // batched evaluation (grow-only buffers)
+  std::vector<void*> bt_tabs;        // lineshape tables of points that move a Pc lineshape
+  PointTable* d_btables = nullptr;   // decoded tables of the points of one launch
+  BatchPoint* d_bpts = nullptr;
+  cplx* d_bdc = nullptr;             // coupling differences, 8 x 24 per point
+  EvalResult* d_bres = nullptr;
+  EvalResult* h_bres = nullptr;      // pinned
+  Partial* d_bparts = nullptr;
+  size_t bparts_cap = 0;
+  double last_batch_ms = 0;
 };
 
 namespace {
@@ -192,6 +202,13 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   if (!c) return PWA_OK;
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
+  for (void* t : c->bt_tabs) cudaFree(t);
+  cudaFree(c->d_btables);
+  cudaFree(c->d_bpts);
+  cudaFree(c->d_bdc);
+  cudaFree(c->d_bres);
+  cudaFree(c->d_bparts);
+  cudaFreeHost(c->h_bres);
   free_events(c);
   cudaFree(c->d_table);
   cudaFreeHost(c->h_table);
@@ -343,6 +360,144 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
   out->n_nonpos = (int64_t)c->h_res->n_nonpos;
   return PWA_OK;
 }
+
+// Lineshape tables for at most this many points of a batch that move a Pc lineshape; further such
+// points are evaluated one by one.
+constexpr int BATCH_MAX_TABLES = 48;
+
+int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_stride, int para_size,
+                           int vamp_size, int spline_size, int NR, int NZ, int NX, float FFR, float FFB,
+                           double sum_w_mc, double sum_w_data, double nll_shift, pwa_result* out,
+                           int* n_structured) {
+  if (!c || !pls || !out || npoints < 1 || block_stride < para_size + vamp_size + spline_size) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  if (spline_size != 0) return PWA_E_UNSUPPORTED;
+  PWA_CUDA(cudaSetDevice(c->device));
+  std::vector<PointTable> H(npoints);
+  for (int p = 0; p < npoints; ++p) {
+    const int rc = build_point_table(pls + (size_t)p * block_stride, para_size, vamp_size, spline_size, NR, NZ, NX,
+                                     FFR, FFB, &H[p]);
+    if (rc) return rc;
+  }
+  // structured points (relative to point 0) and points for the single-point path
+  std::vector<BatchPoint> bp(npoints);
+  std::vector<cplx> dch((size_t)npoints * 8 * 24);
+  std::vector<int> sidx, fidx;
+  int ntab = 0;
+  for (int p = 0; p < npoints; ++p) {
+    bool ok = classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
+    if (ok && bp[p].kind == BP_PCG && c->use_tables) ok = ntab++ < BATCH_MAX_TABLES;
+    (ok ? sidx : fidx).push_back(p);
+  }
+  if (n_structured) *n_structured = (int)sidx.size();
+  // lanes of a warp take consecutive points: order them by kind (and group / entry count) so that a
+  // warp's 32 points follow one code path
+  std::stable_sort(sidx.begin(), sidx.end(), [&](int a, int b) {
+    const BatchPoint &x = bp[a], &y = bp[b];
+    if (x.kind != y.kind) return x.kind < y.kind;
+    if (x.kind == BP_PCG) return x.group < y.group;
+    if (x.kind == BP_PCC) return x.nq < y.nq;
+    return false;
+  });
+  const bool tables = c->use_tables != 0 && H[0].NZ > 0;
+  const int chunk_cap = BATCH_MAX_POINTS;
+  if (!c->d_btables) {
+    PWA_CUDA(cudaMalloc(&c->d_btables, (size_t)chunk_cap * sizeof(PointTable)));
+    PWA_CUDA(cudaMalloc(&c->d_bpts, (size_t)chunk_cap * sizeof(BatchPoint)));
+    PWA_CUDA(cudaMalloc(&c->d_bdc, (size_t)chunk_cap * 8 * 24 * sizeof(cplx)));
+    PWA_CUDA(cudaMalloc(&c->d_bres, (size_t)chunk_cap * sizeof(EvalResult)));
+    PWA_CUDA(cudaMallocHost(&c->h_bres, (size_t)chunk_cap * sizeof(EvalResult)));
+  }
+  while (tables && (int)c->bt_tabs.size() < std::min(ntab, BATCH_MAX_TABLES)) {
+    void* t = nullptr;
+    PWA_CUDA(cudaMalloc(&t, TAB_BYTES));
+    c->bt_tabs.push_back(t);
+  }
+  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  PWA_CUDA(cudaEventRecord(c->e0, c->st));
+  // centre: the context's table and lineshape tables
+  *c->h_table = H[0];
+  int launches = 0, rc = 0;
+  if ((rc = upload_point(c, &launches))) return rc;
+  const PointTable& T0 = *c->h_table;
+  int tab_slot = 0;
+  for (size_t c0 = 0; c0 < sidx.size(); c0 += chunk_cap) {
+    const int nc = (int)std::min<size_t>(chunk_cap, sidx.size() - c0);
+    std::vector<PointTable> dt(nc);
+    std::vector<BatchPoint> dp(nc);
+    for (int j = 0; j < nc; ++j) {
+      const int p = sidx[c0 + j];
+      dt[j] = H[p];  // keeps the point's own guard intervals; tables stay off unless attached here
+      if (bp[p].kind == BP_PCG && tables) attach_tables(&dt[j], c->bt_tabs[tab_slot++]);
+      dp[j] = bp[p];
+      dp[j].T = c->d_btables + j;
+      dp[j].dc = c->d_bdc + (size_t)j * 8 * 24;
+    }
+    PWA_CUDA(cudaMemcpyAsync(c->d_btables, dt.data(), nc * sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
+    PWA_CUDA(cudaMemcpyAsync(c->d_bpts, dp.data(), nc * sizeof(BatchPoint), cudaMemcpyHostToDevice, c->st));
+    std::vector<cplx> dcc((size_t)nc * 8 * 24);
+    for (int j = 0; j < nc; ++j)
+      std::memcpy(dcc.data() + (size_t)j * 8 * 24, dch.data() + (size_t)sidx[c0 + j] * 8 * 24, 8 * 24 * sizeof(cplx));
+    PWA_CUDA(cudaMemcpyAsync(c->d_bdc, dcc.data(), dcc.size() * sizeof(cplx), cudaMemcpyHostToDevice, c->st));
+    for (int j = 0; j < nc; ++j)
+      if (dt[j].tab.enabled) {
+        PWA_CUDA(launch_build_tables(c->d_btables + j, TAB_NODES, c->sm_count, c->st));
+        launches += 4;
+      }
+    // partial rows of all segments
+    std::vector<size_t> row_off;
+    size_t rows = 0;
+    for (auto& sg : c->segs) {
+      row_off.push_back(rows);
+      rows += batch_segment_rows(sg, T0, nc, c->sm_count, tables);
+    }
+    if (rows * nc > c->bparts_cap) {
+      cudaFree(c->d_bparts);
+      c->d_bparts = nullptr;
+      PWA_CUDA(cudaMalloc(&c->d_bparts, rows * nc * sizeof(Partial)));
+      c->bparts_cap = rows * nc;
+    }
+    PWA_CUDA(cudaMemsetAsync(c->d_bparts, 0, rows * nc * sizeof(Partial), c->st));
+    PWA_CUDA(cudaMemsetAsync(c->d_defer_cnt, 0, 8 * sizeof(int), c->st));
+    for (size_t i = 0; i < c->segs.size(); ++i) {
+      int32_t* dq = tables ? c->d_defer + c->seg_defer_off[i] : nullptr;
+      int* dcnt = tables ? c->d_defer_cnt + i : nullptr;
+      PWA_CUDA(launch_batch_segment(ev, c->segs[i], c->d_table, T0, c->d_bpts, nc, c->d_bparts + row_off[i] * nc,
+                                    dq, dcnt, c->sm_count, c->st));
+      launches += tables ? 2 : 1;
+    }
+    PWA_CUDA(launch_finalize_points(c->d_bparts, (int)std::max<size_t>(rows, 1), nc, sum_w_mc, sum_w_data, nll_shift,
+                                    c->d_bres, c->st));
+    ++launches;
+    PWA_CUDA(cudaMemcpyAsync(c->h_bres, c->d_bres, nc * sizeof(EvalResult), cudaMemcpyDeviceToHost, c->st));
+    PWA_CUDA(cudaStreamSynchronize(c->st));
+    for (int j = 0; j < nc; ++j) {
+      const EvalResult& r = c->h_bres[j];
+      pwa_result& o = out[sidx[c0 + j]];
+      o.nll = r.nll;
+      o.sumint = r.sumint;
+      o.sum_noint = r.sum_noint;
+      o.data_term = r.data_term;
+      o.n_nonpos = (int64_t)r.n_nonpos;
+    }
+  }
+  PWA_CUDA(cudaEventRecord(c->e1, c->st));
+  PWA_CUDA(cudaEventSynchronize(c->e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->e0, c->e1);
+  c->last_batch_ms = ms;
+  for (int p : fidx) {
+    if ((rc = pwa_ctx_eval_nll(c, pls + (size_t)p * block_stride, para_size, vamp_size, spline_size, NR, NZ, NX,
+                               FFR, FFB, sum_w_mc, sum_w_data, nll_shift, &out[p], nullptr)))
+      return rc;
+    c->last_batch_ms += c->last_ms;
+    launches += c->last_launches;
+  }
+  c->last_launches = launches;
+  return PWA_OK;
+}
+
+double pwa_ctx_last_batch_ms(pwa_ctx* c) { return c ? c->last_batch_ms : 0.0; }
 
 int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                  float FFR, float FFB, double* h_amp2) {

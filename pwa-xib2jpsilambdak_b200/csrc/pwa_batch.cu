@@ -1,0 +1,590 @@
+// Batched NLL evaluation at many parameter points in one pass over the events.
+//
+// Minuit's numerical gradient evaluates the likelihood at a centre point and at 2N points that each
+// move one parameter.  A moved parameter touches one part of the amplitude: the couplings or the
+// lineshape of one Lambda* (or the Lambda* scale shared by all of them), the couplings of one set of
+// Pc entries, or the lineshapes of one Pc group (a K-matrix J^P group or one Breit-Wigner Pc).  Per
+// event the centre is evaluated once and every point is formed from it by exact FP64 algebra on the
+// difference of its float parameter block and the centre's:
+//   Lambda* point:  H_L[h] += q_r^p f_r^p[h] - q_r^0 f_r^0[h] for the changed resonances r
+//                   (f_r[h] = sum_m c_rkm A_ijm DL_rkm, q_r the lineshape); the Pc sums stay.
+//   Pc couplings:   S_b[h] += sum_{q in Q} R_q(m_b) dHZ_q[h], dHZ_q[h] = sum_m dc_qkm AZ_ijm DZ_qkm,
+//                   at every resolution offset b (R_q the entry lineshape, from the centre).
+//   Pc lineshapes:  S_b[h] += sum_{q in g} (R_q^p(m_b) - R_q^0(m_b)) HZ_q[h], R^p from the point's own
+//                   lineshape table.
+// |A|^2 then follows as in the single-point kernels: sum_h |H_L + S_0|^2 for unsmeared events, and
+// sum_h |H_L|^2 + 2 w Re(conj(H_L) sum_b S_b) + w^2 u sum_b |S_b|^2 for smeared ones (the reference's
+// BW1/BW2 form, kernel_calEva.cu:676-810).  Points that differ from the centre in anything else are
+// evaluated by the single-point path.
+//
+// Work split: one warp per event.  The warp stages the event's 303 basis planes in shared memory,
+// evaluates the centre (Lambda* terms, Pc angular amplitudes HZ_q[h], the entry lineshapes R at up to
+// 32 masses per round and S_b[h] = sum_q R_q(m_b) HZ_q[h]), then each lane takes one parameter point.
+// Per-point results go to per-block FP64 sums; a finalize kernel reduces them per point.
+#include <cstring>
+#include <vector>
+
+#include "pwa_device.cuh"
+
+namespace pwa {
+
+constexpr int BATCH_WARPS = 4;
+constexpr int BATCH_THREADS = BATCH_WARPS * 32;
+constexpr int BATCH_MAXQ = 8;  // Pc entries per coupling point
+constexpr int N_PLANES = 303;  // pp 111 + pp1 96 + pp2 96
+
+// Per-warp shared-memory layout of the batched kernel for a model with NR Lambda* and NZ Pc entries.
+struct BatchLayout {
+  int nzp, rs;  // Pc entries rounded up to 4; row stride of R (odd, conflict-free row writes)
+  size_t bs, q0, f0, hl0, a10, a20, hz, R, S0, vbuf, warp_bytes, acc, total;
+};
+__host__ __device__ inline size_t bal16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
+  BatchLayout L;
+  L.nzp = (NZ + 3) & ~3;
+  L.rs = L.nzp + 1;
+  size_t o = 0;
+  L.bs = o;
+  o = bal16(o + N_PLANES * sizeof(float));
+  L.q0 = o;
+  o = bal16(o + (size_t)(NR > 0 ? NR : 1) * sizeof(cplx));
+  L.f0 = o;
+  o = bal16(o + (size_t)(NR > 0 ? NR : 1) * 8 * sizeof(cplx));
+  L.hl0 = o;
+  o = bal16(o + 8 * sizeof(cplx));
+  L.a10 = o;
+  o = bal16(o + 8 * sizeof(cplx));
+  L.a20 = o;
+  o = bal16(o + 8 * sizeof(double));
+  L.hz = o;
+  o = bal16(o + (size_t)(L.nzp > 0 ? L.nzp : 1) * 8 * sizeof(cplx));
+  L.R = o;
+  o = bal16(o + (size_t)32 * L.rs * sizeof(cplx));
+  L.S0 = o;
+  o = bal16(o + (size_t)32 * 9 * sizeof(cplx));
+  L.vbuf = o;
+  o = bal16(o + (size_t)npts * 2 * sizeof(double));
+  L.warp_bytes = o;
+  L.acc = BATCH_WARPS * L.warp_bytes;
+  L.total = L.acc + (size_t)npts * 4 * sizeof(double);
+  return L;
+}
+
+// Event accessors on the staged planes.
+struct StagedEv {
+  const float* s;
+  __device__ __forceinline__ double mkp() const { return (double)s[0]; }
+  __device__ __forceinline__ double mz() const { return (double)s[1]; }
+  __device__ __forceinline__ float w() const { return s[2]; }
+  __device__ __forceinline__ cplx A(int i, int j, int m) const {
+    const int a = 3 + (i * 12 + j * 6 + m) * 2;
+    return mk((double)s[a], (double)s[a + 1]);
+  }
+  __device__ __forceinline__ double DL(int sx, int k, int m) const { return (double)s[51 + sx * 12 + k * 6 + m]; }
+  __device__ __forceinline__ cplx AZ(int i, int j, int m) const {
+    const int a = 111 + (i * 24 + j * 12 + m) * 2;
+    return mk((double)s[a], (double)s[a + 1]);
+  }
+  __device__ __forceinline__ double DZ(int sx, int k, int m) const { return (double)s[207 + sx * 24 + k * 12 + m]; }
+};
+
+// f_r[h] = sum_m c_rkm A_ijm DL_{s_r,k,m} for helicity h = (i, j, k).
+__device__ __forceinline__ cplx lstar_angular(const LstarEntry& L, const StagedEv& E, int h) {
+  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
+  cplx f = mk(0, 0);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const cplx c = L.c[k * 6 + m];
+    if (nonzero(c)) cmac(f, c, E.A(i, j, m) * E.DL(L.sidx, k, m));
+  }
+  return f;
+}
+
+// sum_m c_m AZ_ijm DZ_{sx,k,m} for helicity h and a 24-slot coupling array c[k * 12 + m].
+__device__ __forceinline__ cplx pc_angular(const cplx* c, int sx, const StagedEv& E, int h) {
+  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
+  cplx v = mk(0, 0);
+#pragma unroll
+  for (int m = 0; m < 12; ++m) {
+    const cplx cc = c[k * 12 + m];
+    if (nonzero(cc)) cmac(v, cc, E.AZ(i, j, m) * E.DZ(sx, k, m));
+  }
+  return v;
+}
+
+// Lineshape of every entry of group g at mass m from the point's table (false when it cannot serve
+// m), or exactly.
+template <bool FIX>
+__device__ __forceinline__ bool group_lineshapes(const PointTable& T, int g, double m, cplx* out) {
+  const PcGroup& gr = T.grp[g];
+  TabAt ta;
+  if (tab_at(T.tab, m, ta)) {
+    for (int q = 0; q < gr.count; ++q) out[q] = tab_get(ta, T.tab.stride, gr.first + q);
+    return true;
+  }
+  if (!FIX) return false;
+  pc_group_exact(T, g, pc_kin(T, m), out);
+  return true;
+}
+
+template <int NB>
+__device__ __forceinline__ const float* batch_offsets() {
+  if constexpr (NB == 0) {
+    return nullptr;
+  } else {
+    return smear_table<NB>();
+  }
+}
+
+// NB = 0: unsmeared events (row 0 = the event mass).  NB > 0: NB resolution offsets; band 0 (tail
+// window events) adds row 0 at the event mass for the non-interfering MC term, band 1 (data bands)
+// does not.  FIX = false: table lookups only, events with a mass no table can serve (centre or a
+// lineshape point's) are appended to defer[]; FIX = true evaluates those masses exactly and runs over
+// the deferred list (events [0, *n_list)) or, without tables, over the whole segment.
+template <int NB, bool FIX>
+__global__ void __launch_bounds__(BATCH_THREADS)
+    k_batch(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
+            const PointTable* __restrict__ T0p, const BatchPoint* __restrict__ pts, int npts, Partial* parts,
+            int band, int32_t* defer, int* defer_count) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const PointTable& T0 = *T0p;
+  const int NR = T0.NR, NZ = T0.NZ;
+  const BatchLayout Ly = batch_layout(NR, NZ, npts);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+  unsigned char* wb = sm + warp * Ly.warp_bytes;
+  float* bs = reinterpret_cast<float*>(wb + Ly.bs);
+  cplx* q0 = reinterpret_cast<cplx*>(wb + Ly.q0);
+  cplx* f0 = reinterpret_cast<cplx*>(wb + Ly.f0);  // [r][h]
+  cplx* hl0 = reinterpret_cast<cplx*>(wb + Ly.hl0);
+  cplx* a10 = reinterpret_cast<cplx*>(wb + Ly.a10);
+  double* a20 = reinterpret_cast<double*>(wb + Ly.a20);
+  cplx* hz = reinterpret_cast<cplx*>(wb + Ly.hz);  // [q][h]
+  cplx* R = reinterpret_cast<cplx*>(wb + Ly.R);    // [row][q], stride Ly.rs
+  cplx* S0 = reinterpret_cast<cplx*>(wb + Ly.S0);  // [row][h], stride 9
+  double* vbuf = reinterpret_cast<double*>(wb + Ly.vbuf);
+  double* acc = reinterpret_cast<double*>(sm + Ly.acc);  // [p][4]
+  for (int i = threadIdx.x; i < npts * 4; i += BATCH_THREADS) acc[i] = 0.0;
+  __syncthreads();
+
+  const StagedEv E{bs};
+  const int h8 = lane & 7, part = lane >> 3;
+  const float* qoff = batch_offsets<NB>();
+  const float wf = (float)(1.0 / (NB > 0 ? NB : 1));
+  const double wgt = wf;
+  const double c2 = wgt * wgt * (double)(1.0f / wf);
+  const int shift = (NB == 0 || band == 0) ? 1 : 0;  // row 0 at the event mass
+  const int nlook = (NB == 0) ? 1 : NB + shift;
+  const int nrounds = (nlook + 31) / 32;
+  const int nzp = Ly.nzp, rs = Ly.rs;
+
+  if (n_list) end = begin + *n_list;
+  const int64_t count = end - begin;
+  int64_t c0, c1, w0, wstep;
+  if (n_list) {
+    c0 = 0;
+    c1 = count;
+    w0 = (int64_t)blockIdx.x * BATCH_WARPS + warp;
+    wstep = (int64_t)gridDim.x * BATCH_WARPS;
+  } else {
+    int64_t chunk = (count + gridDim.x - 1) / gridDim.x;
+    c0 = (int64_t)blockIdx.x * chunk;
+    c1 = min(count, c0 + chunk);
+    w0 = warp;
+    wstep = BATCH_WARPS;
+  }
+
+  for (int64_t p = c0 + w0; p < c1; p += wstep) {
+    const int64_t e = event_index(list, begin, p);
+    for (int i = lane; i < N_PLANES; i += 32) {
+      const float* src = i < 111 ? ev.pp + (int64_t)i * ev.n_size
+                                 : (i < 207 ? ev.pp1 + (int64_t)(i - 111) * ev.n_size
+                                            : ev.pp2 + (int64_t)(i - 207) * ev.n_size);
+      bs[i] = __ldg(src + e);
+    }
+    __syncwarp();
+    const double mkp = E.mkp(), mz = E.mz();
+    const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
+    // centre: Lambda* lineshapes, f_r[h], H_L[h]; Pc angular amplitudes HZ_q[h]
+    if (lane < NR) q0[lane] = lstar_lineshape(T0.L[lane], lstar_kin(T0, mkp));
+    __syncwarp();
+    {
+      cplx hl = mk(0, 0);
+      for (int r = part; r < NR; r += 4) {
+        const cplx f = lstar_angular(T0.L[r], E, h8);
+        f0[r * 8 + h8] = f;
+        cmac(hl, q0[r], f);
+      }
+      hl += shfl_xor(hl, 8);
+      hl += shfl_xor(hl, 16);
+      if (part == 0) hl0[h8] = hl;
+      for (int q = part; q < nzp; q += 4)
+        hz[q * 8 + h8] = q < NZ ? pc_angular(T0.Z[T0.order[q]].c, T0.Z[T0.order[q]].sidx, E, h8) : mk(0, 0);
+    }
+    __syncwarp();
+    bool fail = false;
+    // one round of centre rows: R[b][q] at lookup l0 + b, S0[b][h]; the centre's smeared sums
+    auto centre_round = [&](int l0, bool sums) {
+      const int l = l0 + lane;
+      cplx* row = R + lane * rs;
+      if (l < nlook) {
+        const int b = l - shift;
+        const double m = b < 0 ? mz : mz + (double)qoff[b] * mres;
+        if (FIX)
+          lookup_entries(T0, m, row);
+        else
+          fail |= !lookup_table(T0, m, row);
+      } else {
+        for (int q = 0; q < NZ; ++q) row[q] = mk(0, 0);
+      }
+      for (int q = NZ; q < nzp; ++q) row[q] = mk(0, 0);
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        cplx s = mk(0, 0);
+        for (int q = 0; q < NZ; ++q) cmac(s, row[q], hz[q * 8 + h]);
+        S0[lane * 9 + h] = s;
+      }
+      __syncwarp();
+      if (sums && NB > 0) {
+        // lane (h, part) sums the offset rows b = part, part + 4, ... of this round
+        cplx a1 = mk(0, 0);
+        double a2 = 0;
+        for (int b = part; b < 32; b += 4) {
+          const int ll = l0 + b;
+          if (ll < shift || ll >= nlook) continue;
+          const cplx s = S0[b * 9 + h8];
+          a1 += s;
+          a2 += norm2(s);
+        }
+        a1 += shfl_xor(a1, 8);
+        a1 += shfl_xor(a1, 16);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 8);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 16);
+        if (part == 0) {
+          a10[h8] = (l0 == 0 ? mk(0, 0) : a10[h8]) + a1;
+          a20[h8] = (l0 == 0 ? 0.0 : a20[h8]) + a2;
+        }
+        __syncwarp();
+      }
+    };
+    if (nrounds == 1) centre_round(0, true);
+    const bool centre_fail = !FIX && __any_sync(0xffffffffu, fail);
+    if (!centre_fail) {
+      for (int pass = 0; pass < npts; pass += 32) {
+        const int pidx = pass + lane;
+        const bool act = pidx < npts;
+        const BatchPoint& bp = pts[act ? pidx : 0];
+        const int kind = act ? bp.kind : BP_SAME;
+        const bool own = kind == BP_PCC || kind == BP_PCG;  // sums over the rows are the point's own
+        cplx a1[8];
+        double a2[8];
+        double vns = 0;  // sum_h |S_0[h]|^2 at the event mass (non-interfering term, smeared band 0)
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          a1[h] = mk(0, 0);
+          a2[h] = 0;
+        }
+        for (int rd = 0; rd < nrounds; ++rd) {
+          const int l0 = rd * 32;
+          if (nrounds > 1) centre_round(l0, pass == 0);
+          const int rows = min(32, nlook - l0);
+          if (kind == BP_PCC) {
+            const int nq = bp.nq;
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+              cplx d[BATCH_MAXQ];
+              int pos[BATCH_MAXQ];
+#pragma unroll
+              for (int u = 0; u < BATCH_MAXQ; ++u) {
+                pos[u] = u < nq ? bp.qpos[u] : 0;
+                d[u] = u < nq ? pc_angular(bp.dc + u * 24, bp.qsidx[u], E, h) : mk(0, 0);
+              }
+              for (int b = 0; b < rows; ++b) {
+                cplx sv = S0[b * 9 + h];
+#pragma unroll
+                for (int u = 0; u < BATCH_MAXQ; ++u)
+                  if (u < nq) cmac(sv, R[b * rs + pos[u]], d[u]);
+                if (NB == 0) {
+                  a1[h] = sv;
+                } else if (l0 + b < shift) {
+                  vns += norm2(sv);
+                } else {
+                  a1[h] += sv;
+                  a2[h] += norm2(sv);
+                }
+              }
+            }
+          } else if (kind == BP_PCG) {
+            const PointTable& Tp = *bp.T;
+            const int g = bp.group;
+            const int first = Tp.grp[g].first, cnt = Tp.grp[g].count;
+            for (int b = 0; b < rows; ++b) {
+              const int l = l0 + b;
+              const int bo = l - shift;
+              const double m = (NB == 0 || bo < 0) ? mz : mz + (double)qoff[bo] * mres;
+              cplx dr[MAX_GROUP_ENTRIES];
+              if (!group_lineshapes<FIX>(Tp, g, m, dr)) {
+                fail = true;
+#pragma unroll
+                for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) dr[q] = mk(0, 0);
+              }
+#pragma unroll
+              for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
+                if (q < cnt) dr[q] -= R[b * rs + first + q];
+#pragma unroll
+              for (int h = 0; h < 8; ++h) {
+                cplx sv = S0[b * 9 + h];
+#pragma unroll
+                for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
+                  if (q < cnt) cmac(sv, dr[q], hz[(first + q) * 8 + h]);
+                if (NB == 0) {
+                  a1[h] = sv;
+                } else if (l < shift) {
+                  vns += norm2(sv);
+                } else {
+                  a1[h] += sv;
+                  a2[h] += norm2(sv);
+                }
+              }
+            }
+          }
+        }
+        // the point's Lambda* amplitudes, then |A|^2 with and without interference
+        if (act) {
+          cplx hlp[8];
+#pragma unroll
+          for (int h = 0; h < 8; ++h) hlp[h] = hl0[h];
+          if (kind == BP_LSTAR) {
+            const PointTable& Tp = *bp.T;
+            const LstarKin lk = lstar_kin(Tp, mkp);
+            const unsigned lm = bp.lmask;
+            for (int r = 0; r < NR; ++r) {
+              if (!(lm >> r & 1)) continue;
+              const cplx qp = lstar_lineshape(Tp.L[r], lk);
+#pragma unroll
+              for (int h = 0; h < 8; ++h) {
+                cmac(hlp[h], qp, lstar_angular(Tp.L[r], E, h));
+                cmac(hlp[h], mk(-q0[r].re, -q0[r].im), f0[r * 8 + h]);
+              }
+            }
+          }
+          if (!own && NB > 0 && shift) {
+#pragma unroll
+            for (int h = 0; h < 8; ++h) vns += norm2(S0[h]);
+          }
+          double v = 0, vn = (NB > 0) ? vns : 0.0;
+#pragma unroll
+          for (int h = 0; h < 8; ++h) {
+            if (NB == 0) {
+              const cplx hzp = own ? a1[h] : S0[h];
+              v += norm2(hlp[h] + hzp);
+              vn += norm2(hlp[h]) + norm2(hzp);
+            } else {
+              const cplx s1 = own ? a1[h] : a10[h];
+              const double s2 = own ? a2[h] : a20[h];
+              v += norm2(hlp[h]) + 2.0 * wgt * (hlp[h].re * s1.re + hlp[h].im * s1.im) + c2 * s2;
+              vn += norm2(hlp[h]);
+            }
+          }
+          vbuf[pidx * 2] = v;
+          vbuf[pidx * 2 + 1] = vn;
+        }
+      }
+    }
+    const bool deferred = !FIX && (centre_fail || __any_sync(0xffffffffu, fail));
+    if (deferred) {
+      if (lane == 0) defer[atomicAdd(defer_count, 1)] = (int32_t)e;
+    } else {
+      const float wfe = E.w();
+      const bool data_w = wfe <= -1000.f;
+      for (int pi = lane; pi < npts; pi += 32) {
+        const double v = vbuf[pi * 2], vn = vbuf[pi * 2 + 1];
+        double fxe = v, vnw = 0;
+        if (!(NB > 0 && band) && !data_w) {
+          fxe = v * (double)wfe;
+          vnw = vn * (double)wfe;
+        }
+        double* a = acc + pi * 4;
+        if (!(fxe > 0) || !isfinite(fxe)) atomicAdd(a + 3, 1.0);
+        if (e < ev.nda) {
+          atomicAdd(a + 0, (fxe > 0) ? log(fxe) * (double)__ldg(ev.sw + e) : -1e12);
+        } else {
+          atomicAdd(a + 1, fxe);
+          if (!(NB > 0 && band)) atomicAdd(a + 2, vnw);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int pi = threadIdx.x; pi < npts; pi += BATCH_THREADS) {
+    const double* a = acc + pi * 4;
+    parts[(size_t)blockIdx.x * npts + pi] = Partial{a[0], a[1], a[2], a[3]};
+  }
+}
+
+// ------------------------------------------------------------------------------- host side
+template <int NB, bool FIX>
+static cudaError_t set_batch_smem(int optin) {
+  return cudaFuncSetAttribute(k_batch<NB, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+}
+
+cudaError_t configure_batch_kernels() {
+  int dev = 0, optin = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev))) return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+  optin -= 1024;  // the kernels' static shared memory stays below 1 KB
+  if ((e = set_batch_smem<0, false>(optin)) || (e = set_batch_smem<0, true>(optin)) ||
+      (e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
+      (e = set_batch_smem<30, false>(optin)) || (e = set_batch_smem<30, true>(optin)) ||
+      (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)))
+    return e;
+  return cudaSuccess;
+}
+
+static bool same_bytes(const void* a, const void* b, size_t n) { return std::memcmp(a, b, n) == 0; }
+
+bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, cplx* dc_host) {
+  *bp = BatchPoint{};
+  // structure and global constants must agree
+  if (T0.NR != Tp.NR || T0.NZ != Tp.NZ || T0.ngroups != Tp.ngroups || T0.ffr != Tp.ffr || T0.ffb != Tp.ffb ||
+      T0.lmask_lstar_R != Tp.lmask_lstar_R || T0.lmask_lstar_B != Tp.lmask_lstar_B ||
+      T0.lmask_pc_B != Tp.lmask_pc_B || T0.lmask_pc_R != Tp.lmask_pc_R || T0.needs_sigma_pi != Tp.needs_sigma_pi ||
+      !same_bytes(T0.order, Tp.order, sizeof(T0.order)))
+    return false;
+  for (int g = 0; g < T0.ngroups; ++g) {
+    const PcGroup &a = T0.grp[g], &b = Tp.grp[g];
+    if (a.km != b.km || a.sidx != b.sidx || a.first != b.first || a.count != b.count) return false;
+  }
+  unsigned lmask = 0;
+  for (int r = 0; r < T0.NR; ++r)
+    if (!same_bytes(&T0.L[r], &Tp.L[r], sizeof(LstarEntry))) lmask |= 1u << r;
+  // Pc entries by order position: couplings changed, anything else changed
+  int ncoup = 0, nconst = 0, cgroup = -1;
+  bool multi_group = false;
+  int qpos[MAX_PC];
+  for (int pos = 0; pos < T0.NZ; ++pos) {
+    const int i = T0.order[pos];
+    PcEntry a = T0.Z[i], b = Tp.Z[i];
+    const bool coup = !same_bytes(a.c, b.c, sizeof(a.c));
+    std::memset(a.c, 0, sizeof(a.c));
+    std::memset(b.c, 0, sizeof(b.c));
+    const bool cons = !same_bytes(&a, &b, sizeof(PcEntry));
+    if (coup) qpos[ncoup++] = pos;
+    if (cons) {
+      ++nconst;
+      int g = 0;
+      while (g < T0.ngroups && !(pos >= T0.grp[g].first && pos < T0.grp[g].first + T0.grp[g].count)) ++g;
+      if (cgroup >= 0 && cgroup != g) multi_group = true;
+      cgroup = g;
+    }
+  }
+  for (int ik = 0; ik < 4; ++ik) {
+    if (same_bytes(&T0.G[ik], &Tp.G[ik], sizeof(KmGroup))) continue;
+    int g = 0;
+    while (g < T0.ngroups && T0.grp[g].km != ik) ++g;
+    if (g == T0.ngroups) continue;  // group not in the model
+    if (cgroup >= 0 && cgroup != g) multi_group = true;
+    cgroup = g;
+    ++nconst;
+  }
+  const int parts = (lmask ? 1 : 0) + (ncoup ? 1 : 0) + (nconst ? 1 : 0);
+  if (parts == 0) {
+    bp->kind = BP_SAME;
+    return true;
+  }
+  if (parts > 1 || multi_group) return false;
+  if (lmask) {
+    bp->kind = BP_LSTAR;
+    bp->lmask = lmask;
+    return true;
+  }
+  if (ncoup) {
+    if (ncoup > BATCH_MAXQ) return false;
+    bp->kind = BP_PCC;
+    bp->nq = ncoup;
+    for (int u = 0; u < ncoup; ++u) {
+      const int i = T0.order[qpos[u]];
+      bp->qpos[u] = qpos[u];
+      bp->qsidx[u] = T0.Z[i].sidx;
+      for (int s = 0; s < 24; ++s) dc_host[u * 24 + s] = Tp.Z[i].c[s] - T0.Z[i].c[s];
+    }
+    return true;
+  }
+  bp->kind = BP_PCG;
+  bp->group = cgroup;
+  return true;
+}
+
+static int batch_nb(int kind) { return kind == SMEAR_20 ? 20 : kind == SMEAR_30 ? 30 : kind == SMEAR_150 ? 150 : 0; }
+
+static int batch_grid(const Segment& s, const PointTable& T0, int npts, int sm_count) {
+  const int64_t n = s.end - s.begin;
+  int64_t b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
+  int occ = 1;
+  const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
+  switch (batch_nb(s.kind)) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<0, false>, BATCH_THREADS, smem); break;
+    case 20: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<20, false>, BATCH_THREADS, smem); break;
+    case 30: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<30, false>, BATCH_THREADS, smem); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<150, false>, BATCH_THREADS, smem); break;
+  }
+  if (occ < 1) occ = 1;
+  const int64_t cap = (int64_t)sm_count * occ;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+int batch_segment_rows(const Segment& s, const PointTable& T0, int npts, int sm_count, bool deferred) {
+  const int g = batch_grid(s, T0, npts, sm_count);
+  return deferred ? 2 * g : g;
+}
+
+template <int NB>
+static void launch_batch_kind(const EventSet& ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
+                              const PointTable* d_T0, const BatchPoint* d_pts, int npts, Partial* out, int band,
+                              int32_t* defer, int* defer_count, bool fix, int grid, size_t smem, cudaStream_t st) {
+  if (fix)
+    k_batch<NB, true><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
+                                                         defer, defer_count);
+  else
+    k_batch<NB, false><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
+                                                          defer, defer_count);
+}
+
+static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t end, const int32_t* list,
+                            const int* n_list, const PointTable* d_T0, const BatchPoint* d_pts, int npts, Partial* out,
+                            int band, int32_t* defer, int* defer_count, bool fix, int grid, size_t smem,
+                            cudaStream_t st) {
+  switch (nb) {
+    case 0: launch_batch_kind<0>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+    case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+    case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+    default: launch_batch_kind<150>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+  }
+}
+
+cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
+                                 const BatchPoint* d_pts, int npts, Partial* out, int32_t* defer, int* defer_count,
+                                 int sm_count, cudaStream_t st) {
+  if (seg.end <= seg.begin) return cudaSuccess;
+  if (npts < 1 || npts > BATCH_MAX_POINTS) return cudaErrorInvalidValue;
+  const int nb = batch_nb(seg.kind);
+  const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
+  const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
+  const int grid = batch_grid(seg, T0, npts, sm_count);
+  if (defer) {
+    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, d_pts, npts, out, band, defer, defer_count,
+                    false, grid, smem, st);
+    launch_batch_nb(nb, ev, 0, 0, defer, defer_count, d_T0, d_pts, npts, out + (size_t)grid * npts, band, nullptr,
+                    nullptr, true, grid, smem, st);
+  } else {
+    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, d_pts, npts, out, band, nullptr, nullptr,
+                    true, grid, smem, st);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pwa

@@ -77,6 +77,43 @@ cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, d
 // Host evaluation of the decoded lineshapes (see pwa_kernels.cu).
 void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cplx* pc);
 
+// ------------------------------------------------------------------ batched evaluation
+// A parameter point of a batch that differs from the batch centre (point 0) in one part of the
+// amplitude only (pwa_batch.cu).
+enum BatchKind : int { BP_SAME = 0, BP_LSTAR = 1, BP_PCC = 2, BP_PCG = 3 };
+struct BatchPoint {
+  int kind;
+  unsigned lmask;          // BP_LSTAR: changed Lambda* (bit r)
+  int group;               // BP_PCG: Pc group whose lineshapes changed
+  int nq;                  // BP_PCC: Pc entries whose couplings changed (at most 8)
+  int qpos[8], qsidx[8];   // their order positions and d-function spin indices
+  const cplx* dc;          // BP_PCC: coupling differences point - centre, [nq][24] (device)
+  const PointTable* T;     // device copy of the point's table (BP_LSTAR, BP_PCG)
+};
+
+// Classifies point Tp against the batch centre T0: fills bp (kind, masks; bp->dc and bp->T are left
+// for the caller) and, for BP_PCC, the coupling differences dc_host[nq][24].  Returns false when the
+// point differs in more than one part of the amplitude (evaluate it with the single-point path).
+bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, cplx* dc_host);
+
+// Largest number of points one batched launch takes (shared memory holds per-point sums).
+constexpr int BATCH_MAX_POINTS = 320;
+
+// Partial rows a segment of a batched evaluation writes (its pass, plus the deferred pass when
+// deferred is true); each row holds npts partials.
+int batch_segment_rows(const Segment& s, const PointTable& T0, int npts, int sm_count, bool deferred);
+
+// Launches the batched passes over one segment: partial rows out[0 .. batch_segment_rows) x npts.
+cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
+                                 const BatchPoint* d_pts, int npts, Partial* out, int32_t* defer, int* defer_count,
+                                 int sm_count, cudaStream_t st);
+
+// Reduces rows x npts partials (row-major) into npts results.
+cudaError_t launch_finalize_points(const Partial* parts, int rows, int npts, double sum_w_mc, double sum_w_data,
+                                   double nll_shift, EvalResult* res, cudaStream_t st);
+
+cudaError_t configure_batch_kernels();
+
 // Per-event unsmeared |A|^2 without weights (host_store_amp2s semantics) for n events.
 cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int32_t* defer, int* defer_count,
                         int sm_count, cudaStream_t st);

@@ -16,7 +16,7 @@ import os
 LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
-            "pwa_ctx_eval_nll", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
+            "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
@@ -53,6 +53,11 @@ def load() -> C.CDLL:
                                        C.POINTER(PwaResult), _dp]
         L.pwa_ctx_amp2.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_float, C.c_float, _dp]
+        L.pwa_ctx_eval_nll_batch.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
+                                             C.c_double, C.POINTER(PwaResult), C.POINTER(C.c_int)]
+        L.pwa_ctx_last_batch_ms.restype = C.c_double
+        L.pwa_ctx_last_batch_ms.argtypes = [C.c_void_p]
         L.pwa_ctx_last_kernel_ms.restype = C.c_double
         L.pwa_ctx_last_kernel_ms.argtypes = [C.c_void_p]
         L.pwa_ctx_last_launches.argtypes = [C.c_void_p]
@@ -152,6 +157,28 @@ class Context:
                                       block.NZ, block.NX, block.ffr, block.ffb, s.sum_w_mc, s.sum_w_data, nll_shift,
                                       C.byref(r), fx.ctypes.data_as(_dp) if want_fx else None), "pwa_ctx_eval_nll")
         return (r, fx) if want_fx else r
+
+    def eval_nll_batch(self, blocks, nll_shift: float = 1e7):
+        """Likelihood at several parameter points of one model in one call (pwa_ctx_eval_nll_batch).
+        blocks: ParamBlocks with equal sizes; returns (results, number of points evaluated together
+        from the first point's per-event terms)."""
+        s = self.sample
+        b0 = blocks[0]
+        stride = len(b0.data)
+        for b in blocks:
+            if len(b.data) != stride or (b.para_size, b.vamp_size, b.NR, b.NZ) != (b0.para_size, b0.vamp_size,
+                                                                                    b0.NR, b0.NZ):
+                raise PwaError("eval_nll_batch: parameter blocks of different models")
+        pl = np.ascontiguousarray(np.stack([np.asarray(b.data, np.float32) for b in blocks]))
+        res = (PwaResult * len(blocks))()
+        ns = C.c_int()
+        check(self.L.pwa_ctx_eval_nll_batch(self.h, _f(pl), len(blocks), stride, b0.para_size, b0.vamp_size,
+                                            b0.spline_size, b0.NR, b0.NZ, b0.NX, b0.ffr, b0.ffb, s.sum_w_mc,
+                                            s.sum_w_data, nll_shift, res, C.byref(ns)), "pwa_ctx_eval_nll_batch")
+        return list(res), ns.value
+
+    def last_batch_ms(self) -> float:
+        return self.L.pwa_ctx_last_batch_ms(self.h)
 
     def amp2(self, block) -> np.ndarray:
         pl = np.ascontiguousarray(block.data, np.float32)
