@@ -423,6 +423,245 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   }
 }
 
+// ------------------------------------------------------------------------------- unsmeared events
+// Unsmeared events: lane = event (32 consecutive events per warp), all lanes walk the points
+// together, so the point data and couplings are warp-uniform reads and the lanes never diverge.
+// Per lane the centre's H_L[h], H_Z[h] stay in registers; the entry lineshapes R_q and the Lambda*
+// lineshapes q_r go to per-warp shared memory ([q][lane]), and the Pc angular amplitudes HZ_q[h] of
+// the group a lineshape point moves are rebuilt when the group changes (points come sorted by kind
+// and group).  Per point the warp sums the events' contributions with shuffles and one lane adds
+// them to the block's per-point sums.
+constexpr int BU_WARPS = 4;
+constexpr int BU_THREADS = BU_WARPS * 32;
+
+struct BatchUnLayout {
+  size_t q0, r0, hzg, warp_bytes, acc, total;
+};
+__host__ __device__ inline BatchUnLayout batch_un_layout(int NR, int NZ, int gmax, int npts) {
+  BatchUnLayout L;
+  size_t o = 0;
+  L.q0 = o;
+  o = bal16(o + (size_t)(NR > 0 ? NR : 1) * 32 * sizeof(cplx));
+  L.r0 = o;
+  o = bal16(o + (size_t)(NZ > 0 ? NZ : 1) * 32 * sizeof(cplx));
+  L.hzg = o;
+  o = bal16(o + (size_t)(gmax > 0 ? gmax : 1) * 8 * 32 * sizeof(cplx));
+  L.warp_bytes = o;
+  L.acc = BU_WARPS * o;
+  L.total = L.acc + (size_t)npts * 4 * sizeof(double);
+  return L;
+}
+
+// Largest Pc group of a point table.
+__host__ __device__ inline int max_group(const PointTable& T) {
+  int g = 0;
+  for (int i = 0; i < T.ngroups; ++i) g = T.grp[i].count > g ? T.grp[i].count : g;
+  return g;
+}
+
+// out[h] += q * sum_m c_{r,k,m} A_ijm DL_{s_r,k,m} for all 8 helicities h = (i, j, k): per m the four
+// A_ijm and the two DL values are loaded once.
+__device__ __forceinline__ void lstar_acc(const LstarEntry& L, const Ev& E, cplx q, cplx* out) {
+#pragma unroll 1
+  for (int m = 0; m < 6; ++m) {
+    const cplx c0 = L.c[m], c1 = L.c[6 + m];
+    const bool n0 = nonzero(c0), n1 = nonzero(c1);
+    if (!n0 && !n1) continue;
+    const cplx w0 = (q * c0) * E.DL(L.sidx, 0, m), w1 = (q * c1) * E.DL(L.sidx, 1, m);
+#pragma unroll
+    for (int ij = 0; ij < 4; ++ij) {
+      const cplx a = E.A(ij >> 1, ij & 1, m);
+      cmac(out[2 * ij], a, w0);
+      cmac(out[2 * ij + 1], a, w1);
+    }
+  }
+}
+
+// out[h] += q * sum_m c[k * 12 + m] AZ_ijm DZ_{sx,k,m} for all 8 helicities.
+__device__ __forceinline__ void pc_acc(const cplx* c, int sx, const Ev& E, cplx q, cplx* out) {
+#pragma unroll 1
+  for (int m = 0; m < 12; ++m) {
+    const cplx c0 = c[m], c1 = c[12 + m];
+    if (!nonzero(c0) && !nonzero(c1)) continue;
+    const cplx w0 = (q * c0) * E.DZ(sx, 0, m), w1 = (q * c1) * E.DZ(sx, 1, m);
+#pragma unroll
+    for (int ij = 0; ij < 4; ++ij) {
+      const cplx a = E.AZ(ij >> 1, ij & 1, m);
+      cmac(out[2 * ij], a, w0);
+      cmac(out[2 * ij + 1], a, w1);
+    }
+  }
+}
+
+template <bool FIX>
+__global__ void __launch_bounds__(BU_THREADS)
+    k_batch_un(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
+               const PointTable* __restrict__ T0p, const BatchPoint* __restrict__ pts, int npts, Partial* parts,
+               int32_t* defer, int* defer_count) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const PointTable& T0 = *T0p;
+  const int NR = T0.NR, NZ = T0.NZ;
+  const BatchUnLayout Ly = batch_un_layout(NR, NZ, max_group(T0), npts);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+  unsigned char* wb = sm + warp * Ly.warp_bytes;
+  cplx* q0s = reinterpret_cast<cplx*>(wb + Ly.q0);   // [r][lane]
+  cplx* r0s = reinterpret_cast<cplx*>(wb + Ly.r0);   // [q][lane]
+  cplx* hzg = reinterpret_cast<cplx*>(wb + Ly.hzg);  // [entry of group][h][lane]
+  double* acc = reinterpret_cast<double*>(sm + Ly.acc);
+  for (int i = threadIdx.x; i < npts * 4; i += BU_THREADS) acc[i] = 0.0;
+  __syncthreads();
+
+  if (n_list) end = begin + *n_list;
+  const int64_t count = end - begin;
+  int64_t c0, c1, w0, wstep;
+  if (n_list) {
+    c0 = 0;
+    c1 = count;
+    w0 = ((int64_t)blockIdx.x * BU_WARPS + warp) * 32;
+    wstep = (int64_t)gridDim.x * BU_WARPS * 32;
+  } else {
+    int64_t chunk = (count + gridDim.x - 1) / gridDim.x;
+    chunk = (chunk + BU_THREADS - 1) / BU_THREADS * BU_THREADS;
+    c0 = (int64_t)blockIdx.x * chunk;
+    c1 = min(count, c0 + chunk);
+    w0 = warp * 32;
+    wstep = BU_THREADS;
+  }
+  for (int64_t base = c0 + w0; base < c1; base += wstep) {
+    const int64_t pp = base + lane;
+    const bool valid = pp < c1;
+    const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? pp : c0)};
+    const double mkp = E.mkp(), mz = E.mz();
+    // centre
+    cplx HL0[8], HZ0[8];
+#pragma unroll
+    for (int h = 0; h < 8; ++h) HL0[h] = HZ0[h] = mk(0, 0);
+    {
+      const LstarKin lk = lstar_kin(T0, mkp);
+      for (int r = 0; r < NR; ++r) {
+        const cplx q = lstar_lineshape(T0.L[r], lk);
+        q0s[r * 32 + lane] = q;
+        lstar_acc(T0.L[r], E, q, HL0);
+      }
+    }
+    bool fail = false;
+    if (NZ > 0) {
+      cplx rr[MAX_PC];
+      if (FIX)
+        lookup_entries(T0, mz, rr);
+      else
+        fail = !lookup_table(T0, mz, rr);
+      for (int q = 0; q < NZ; ++q) {
+        r0s[q * 32 + lane] = rr[q];
+        const PcEntry& Z = T0.Z[T0.order[q]];
+        pc_acc(Z.c, Z.sidx, E, rr[q], HZ0);
+      }
+    }
+    if (!FIX) {
+      // a point's lineshape table must serve this mass too (checked before anything is summed)
+      for (int pi = 0; pi < npts; ++pi) {
+        const BatchPoint& bp = pts[pi];
+        if (bp.kind != BP_PCG) continue;
+        TabAt ta;
+        fail |= !tab_at(bp.T->tab, mz, ta);
+      }
+    }
+    const bool deferred = !FIX && valid && fail;
+    if (deferred) defer[atomicAdd(defer_count, 1)] = (int32_t)E.e;
+    const bool live = valid && !deferred;
+    const float wf = E.w();
+    const bool data_w = wf <= -1000.f;
+    const bool is_data = E.e < ev.nda;
+    const double swe = (live && is_data) ? (double)__ldg(ev.sw + E.e) : 0.0;
+    int cur_group = -1;
+    __syncwarp();
+    for (int pi = 0; pi < npts; ++pi) {
+      const BatchPoint& bp = pts[pi];
+      const int kind = bp.kind;
+      cplx d[8];  // change of H_L (Lambda* points) or of H_Z (Pc points)
+#pragma unroll
+      for (int h = 0; h < 8; ++h) d[h] = mk(0, 0);
+      if (kind == BP_LSTAR) {
+        const PointTable& Tp = *bp.T;
+        const LstarKin lk = lstar_kin(Tp, mkp);
+        const unsigned lm = bp.lmask;
+        for (int r = 0; r < NR; ++r) {
+          if (!(lm >> r & 1)) continue;
+          const cplx qp = lstar_lineshape(Tp.L[r], lk);
+          const cplx q0 = q0s[r * 32 + lane];
+          lstar_acc(Tp.L[r], E, qp, d);
+          lstar_acc(T0.L[r], E, mk(-q0.re, -q0.im), d);
+        }
+      } else if (kind == BP_PCC) {
+        for (int u = 0; u < bp.nq; ++u) {
+          pc_acc(bp.dc + u * 24, bp.qsidx[u], E, r0s[bp.qpos[u] * 32 + lane], d);
+        }
+      } else if (kind == BP_PCG) {
+        const PointTable& Tp = *bp.T;
+        const int g = bp.group;
+        const int first = T0.grp[g].first, cnt = T0.grp[g].count;
+        if (g != cur_group) {
+          for (int q = 0; q < cnt; ++q) {
+            const PcEntry& Z = T0.Z[T0.order[first + q]];
+            cplx t[8];
+#pragma unroll
+            for (int h = 0; h < 8; ++h) t[h] = mk(0, 0);
+            pc_acc(Z.c, Z.sidx, E, mk(1, 0), t);
+#pragma unroll
+            for (int h = 0; h < 8; ++h) hzg[(q * 8 + h) * 32 + lane] = t[h];
+          }
+          cur_group = g;
+        }
+        cplx dr[MAX_GROUP_ENTRIES];
+        if (!group_lineshapes<FIX>(Tp, g, mz, dr))
+          for (int q = 0; q < cnt; ++q) dr[q] = r0s[(first + q) * 32 + lane];
+        for (int q = 0; q < cnt; ++q) {
+          const cplx dq = dr[q] - r0s[(first + q) * 32 + lane];
+#pragma unroll
+          for (int h = 0; h < 8; ++h) cmac(d[h], dq, hzg[(q * 8 + h) * 32 + lane]);
+        }
+      }
+      const bool to_hl = kind == BP_LSTAR;
+      double v = 0, vn = 0;
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const cplx hl = to_hl ? HL0[h] + d[h] : HL0[h], hz = to_hl ? HZ0[h] : HZ0[h] + d[h];
+        v += norm2(hl + hz);
+        vn += norm2(hl) + norm2(hz);
+      }
+      const double fxe = data_w ? v : v * (double)wf;
+      double a0 = 0, a1 = 0, a2 = 0;
+      bool bad = false;
+      if (live) {
+        bad = !(fxe > 0) || !isfinite(fxe);
+        if (is_data) {
+          a0 = (fxe > 0) ? log(fxe) * swe : -1e12;
+        } else {
+          a1 = fxe;
+          a2 = data_w ? 0.0 : vn * (double)wf;
+        }
+      }
+      a0 = warp_sum(a0);
+      a1 = warp_sum(a1);
+      a2 = warp_sum(a2);
+      const int nbad = __popc(__ballot_sync(0xffffffffu, bad));
+      if (lane == 0) {
+        double* a = acc + pi * 4;
+        atomicAdd(a + 0, a0);
+        atomicAdd(a + 1, a1);
+        atomicAdd(a + 2, a2);
+        if (nbad) atomicAdd(a + 3, (double)nbad);
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int pi = threadIdx.x; pi < npts; pi += BU_THREADS) {
+    const double* a = acc + pi * 4;
+    parts[(size_t)blockIdx.x * npts + pi] = Partial{a[0], a[1], a[2], a[3]};
+  }
+}
+
 // ------------------------------------------------------------------------------- host side
 template <int NB, bool FIX>
 static cudaError_t set_batch_smem(int optin) {
@@ -439,6 +678,9 @@ cudaError_t configure_batch_kernels() {
       (e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
       (e = set_batch_smem<30, false>(optin)) || (e = set_batch_smem<30, true>(optin)) ||
       (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)))
+    return e;
+  if ((e = cudaFuncSetAttribute(k_batch_un<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
+      (e = cudaFuncSetAttribute(k_batch_un<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)))
     return e;
   return cudaSuccess;
 }
@@ -521,14 +763,20 @@ static int batch_nb(int kind) { return kind == SMEAR_20 ? 20 : kind == SMEAR_30 
 
 static int batch_grid(const Segment& s, const PointTable& T0, int npts, int sm_count) {
   const int64_t n = s.end - s.begin;
-  int64_t b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
   int occ = 1;
-  const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
-  switch (batch_nb(s.kind)) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<0, false>, BATCH_THREADS, smem); break;
-    case 20: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<20, false>, BATCH_THREADS, smem); break;
-    case 30: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<30, false>, BATCH_THREADS, smem); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<150, false>, BATCH_THREADS, smem); break;
+  int64_t b;
+  if (batch_nb(s.kind) == 0) {
+    b = (n + BU_THREADS - 1) / BU_THREADS;
+    const size_t smem = batch_un_layout(T0.NR, T0.NZ, max_group(T0), npts).total;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_un<false>, BU_THREADS, smem);
+  } else {
+    b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
+    const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
+    switch (batch_nb(s.kind)) {
+      case 20: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<20, false>, BATCH_THREADS, smem); break;
+      case 30: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<30, false>, BATCH_THREADS, smem); break;
+      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<150, false>, BATCH_THREADS, smem); break;
+    }
   }
   if (occ < 1) occ = 1;
   const int64_t cap = (int64_t)sm_count * occ;
@@ -559,7 +807,14 @@ static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t e
                             int band, int32_t* defer, int* defer_count, bool fix, int grid, size_t smem,
                             cudaStream_t st) {
   switch (nb) {
-    case 0: launch_batch_kind<0>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+    case 0:
+      if (fix)
+        k_batch_un<true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, defer,
+                                                          defer_count);
+      else
+        k_batch_un<false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, defer,
+                                                           defer_count);
+      break;
     case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
     case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
     default: launch_batch_kind<150>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
@@ -573,7 +828,8 @@ cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const P
   if (npts < 1 || npts > BATCH_MAX_POINTS) return cudaErrorInvalidValue;
   const int nb = batch_nb(seg.kind);
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
-  const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
+  const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, max_group(T0), npts).total
+                              : batch_layout(T0.NR, T0.NZ, npts).total;
   const int grid = batch_grid(seg, T0, npts, sm_count);
   if (defer) {
     launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, d_pts, npts, out, band, defer, defer_count,
