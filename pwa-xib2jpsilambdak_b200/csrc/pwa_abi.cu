@@ -420,6 +420,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   int launches = 0, rc = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const PointTable& T0 = *c->h_table;
+  const BatchGroupMap gm = batch_group_map(T0);
   int tab_slot = 0;
   for (size_t c0 = 0; c0 < sidx.size(); c0 += chunk_cap) {
     const int nc = (int)std::min<size_t>(chunk_cap, sidx.size() - c0);
@@ -449,7 +450,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     size_t rows = 0;
     for (auto& sg : c->segs) {
       row_off.push_back(rows);
-      rows += batch_segment_rows(sg, T0, nc, c->sm_count, tables);
+      rows += batch_segment_rows(sg, T0, gm, nc, c->sm_count, tables);
     }
     if (rows * nc > c->bparts_cap) {
       cudaFree(c->d_bparts);
@@ -462,8 +463,8 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     for (size_t i = 0; i < c->segs.size(); ++i) {
       int32_t* dq = tables ? c->d_defer + c->seg_defer_off[i] : nullptr;
       int* dcnt = tables ? c->d_defer_cnt + i : nullptr;
-      PWA_CUDA(launch_batch_segment(ev, c->segs[i], c->d_table, T0, c->d_bpts, nc, c->d_bparts + row_off[i] * nc,
-                                    dq, dcnt, c->sm_count, c->st));
+      PWA_CUDA(launch_batch_segment(ev, c->segs[i], c->d_table, T0, gm, c->d_bpts, nc,
+                                    c->d_bparts + row_off[i] * nc, dq, dcnt, c->sm_count, c->st));
       launches += tables ? 2 : 1;
     }
     PWA_CUDA(launch_finalize_points(c->d_bparts, (int)std::max<size_t>(rows, 1), nc, sum_w_mc, sum_w_data, nll_shift,

@@ -115,16 +115,33 @@ __device__ __forceinline__ cplx pc_angular(const cplx* c, int sx, const StagedEv
 // Lineshape of every entry of group g at mass m from the point's table (false when it cannot serve
 // m), or exactly.
 template <bool FIX>
-__device__ __forceinline__ bool group_lineshapes(const PointTable& T, int g, double m, cplx* out) {
+__device__ __forceinline__ bool group_lineshapes(const PointTable& T, int g, double m, cplx (&out)[MAX_GROUP_ENTRIES]) {
   const PcGroup& gr = T.grp[g];
+  const int first = gr.first, cnt = gr.count;
   TabAt ta;
   if (tab_at(T.tab, m, ta)) {
-    for (int q = 0; q < gr.count; ++q) out[q] = tab_get(ta, T.tab.stride, gr.first + q);
+#pragma unroll
+    for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) out[q] = q < cnt ? tab_get(ta, T.tab.stride, first + q) : mk(0, 0);
     return true;
   }
   if (!FIX) return false;
-  pc_group_exact(T, g, pc_kin(T, m), out);
+  cplx ex[MAX_GROUP_ENTRIES];
+  pc_group_exact(T, g, pc_kin(T, m), ex);
+#pragma unroll
+  for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) out[q] = q < cnt ? ex[q] : mk(0, 0);
   return true;
+}
+
+// sum_m c[k * 6 + m] A_ijm DL_{sx,k,m} for helicity h (c: a Lambda* coupling array).
+__device__ __forceinline__ cplx lstar_angular_c(const cplx* c, int sx, const StagedEv& E, int h) {
+  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
+  cplx f = mk(0, 0);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const cplx cc = c[k * 6 + m];
+    if (nonzero(cc)) cmac(f, cc, E.A(i, j, m) * E.DL(sx, k, m));
+  }
+  return f;
 }
 
 template <int NB>
@@ -355,16 +372,32 @@ __global__ void __launch_bounds__(BATCH_THREADS)
 #pragma unroll
           for (int h = 0; h < 8; ++h) hlp[h] = hl0[h];
           if (kind == BP_LSTAR) {
+            // the kinematic inputs of the lineshapes (barrier orders, radii) equal the centre's
             const PointTable& Tp = *bp.T;
-            const LstarKin lk = lstar_kin(Tp, mkp);
-            const unsigned lm = bp.lmask;
+            const LstarKin lk = lstar_kin(T0, mkp);
+            const unsigned lm = bp.lmask, lsm = bp.lsmask, lcm = bp.lcmask;
+            int u = 0;
             for (int r = 0; r < NR; ++r) {
               if (!(lm >> r & 1)) continue;
-              const cplx qp = lstar_lineshape(Tp.L[r], lk);
+              const bool ls = lsm >> r & 1, cc = lcm >> r & 1;
+              if (!ls && cc && bp.ldc) {  // couplings only: q_r * f(dc)
+                const cplx* dc = bp.dc + 24 * u++;
 #pragma unroll
-              for (int h = 0; h < 8; ++h) {
-                cmac(hlp[h], qp, lstar_angular(Tp.L[r], E, h));
-                cmac(hlp[h], mk(-q0[r].re, -q0[r].im), f0[r * 8 + h]);
+                for (int h = 0; h < 8; ++h) cmac(hlp[h], q0[r], lstar_angular_c(dc, T0.L[r].sidx, E, h));
+              } else {
+                if (cc) ++u;
+                const cplx qp = lstar_lineshape(Tp.L[r], lk);
+                if (!cc) {  // lineshape only: (q^p - q^0) f_r
+                  const cplx dq = qp - q0[r];
+#pragma unroll
+                  for (int h = 0; h < 8; ++h) cmac(hlp[h], dq, f0[r * 8 + h]);
+                } else {
+#pragma unroll
+                  for (int h = 0; h < 8; ++h) {
+                    cmac(hlp[h], qp, lstar_angular(Tp.L[r], E, h));
+                    cmac(hlp[h], mk(-q0[r].re, -q0[r].im), f0[r * 8 + h]);
+                  }
+                }
               }
             }
           }
@@ -459,15 +492,15 @@ __host__ __device__ inline int max_group(const PointTable& T) {
   return g;
 }
 
-// out[h] += q * sum_m c_{r,k,m} A_ijm DL_{s_r,k,m} for all 8 helicities h = (i, j, k): per m the four
+// out[h] += q * sum_m c[k * 6 + m] A_ijm DL_{sx,k,m} for all 8 helicities h = (i, j, k): per m the four
 // A_ijm and the two DL values are loaded once.
-__device__ __forceinline__ void lstar_acc(const LstarEntry& L, const Ev& E, cplx q, cplx* out) {
+__device__ __forceinline__ void lstar_acc(const cplx* c, int sx, const Ev& E, cplx q, cplx* out) {
 #pragma unroll 1
   for (int m = 0; m < 6; ++m) {
-    const cplx c0 = L.c[m], c1 = L.c[6 + m];
+    const cplx c0 = c[m], c1 = c[6 + m];
     const bool n0 = nonzero(c0), n1 = nonzero(c1);
     if (!n0 && !n1) continue;
-    const cplx w0 = (q * c0) * E.DL(L.sidx, 0, m), w1 = (q * c1) * E.DL(L.sidx, 1, m);
+    const cplx w0 = (q * c0) * E.DL(sx, 0, m), w1 = (q * c1) * E.DL(sx, 1, m);
 #pragma unroll
     for (int ij = 0; ij < 4; ++ij) {
       const cplx a = E.A(ij >> 1, ij & 1, m);
@@ -496,12 +529,12 @@ __device__ __forceinline__ void pc_acc(const cplx* c, int sx, const Ev& E, cplx 
 template <bool FIX>
 __global__ void __launch_bounds__(BU_THREADS)
     k_batch_un(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
-               const PointTable* __restrict__ T0p, const BatchPoint* __restrict__ pts, int npts, Partial* parts,
-               int32_t* defer, int* defer_count) {
+               const PointTable* __restrict__ T0p, const __grid_constant__ BatchGroupMap gm,
+               const BatchPoint* __restrict__ pts, int npts, Partial* parts, int32_t* defer, int* defer_count) {
   extern __shared__ __align__(16) unsigned char sm[];
   const PointTable& T0 = *T0p;
   const int NR = T0.NR, NZ = T0.NZ;
-  const BatchUnLayout Ly = batch_un_layout(NR, NZ, max_group(T0), npts);
+  const BatchUnLayout Ly = batch_un_layout(NR, NZ, gm.max_slots, npts);
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   unsigned char* wb = sm + warp * Ly.warp_bytes;
   cplx* q0s = reinterpret_cast<cplx*>(wb + Ly.q0);   // [r][lane]
@@ -536,12 +569,13 @@ __global__ void __launch_bounds__(BU_THREADS)
     cplx HL0[8], HZ0[8];
 #pragma unroll
     for (int h = 0; h < 8; ++h) HL0[h] = HZ0[h] = mk(0, 0);
+    // the kinematic inputs of the Lambda* lineshapes are the same for every point of the batch
+    const LstarKin lk0 = lstar_kin(T0, mkp);
     {
-      const LstarKin lk = lstar_kin(T0, mkp);
       for (int r = 0; r < NR; ++r) {
-        const cplx q = lstar_lineshape(T0.L[r], lk);
+        const cplx q = lstar_lineshape(T0.L[r], lk0);
         q0s[r * 32 + lane] = q;
-        lstar_acc(T0.L[r], E, q, HL0);
+        lstar_acc(T0.L[r].c, T0.L[r].sidx, E, q, HL0);
       }
     }
     bool fail = false;
@@ -583,14 +617,25 @@ __global__ void __launch_bounds__(BU_THREADS)
       for (int h = 0; h < 8; ++h) d[h] = mk(0, 0);
       if (kind == BP_LSTAR) {
         const PointTable& Tp = *bp.T;
-        const LstarKin lk = lstar_kin(Tp, mkp);
-        const unsigned lm = bp.lmask;
+        const unsigned lm = bp.lmask, lsm = bp.lsmask, lcm = bp.lcmask;
+        int u = 0;
         for (int r = 0; r < NR; ++r) {
           if (!(lm >> r & 1)) continue;
-          const cplx qp = lstar_lineshape(Tp.L[r], lk);
+          const bool ls = lsm >> r & 1, cc = lcm >> r & 1;
           const cplx q0 = q0s[r * 32 + lane];
-          lstar_acc(Tp.L[r], E, qp, d);
-          lstar_acc(T0.L[r], E, mk(-q0.re, -q0.im), d);
+          const int sx = T0.L[r].sidx;
+          if (!ls && cc && bp.ldc) {  // couplings only
+            lstar_acc(bp.dc + 24 * u++, sx, E, q0, d);
+          } else {
+            if (cc) ++u;
+            const cplx qp = lstar_lineshape(Tp.L[r], lk0);
+            if (!cc) {
+              lstar_acc(T0.L[r].c, sx, E, qp - q0, d);
+            } else {
+              lstar_acc(Tp.L[r].c, sx, E, qp, d);
+              lstar_acc(T0.L[r].c, sx, E, mk(-q0.re, -q0.im), d);
+            }
+          }
         }
       } else if (kind == BP_PCC) {
         for (int u = 0; u < bp.nq; ++u) {
@@ -600,25 +645,41 @@ __global__ void __launch_bounds__(BU_THREADS)
         const PointTable& Tp = *bp.T;
         const int g = bp.group;
         const int first = T0.grp[g].first, cnt = T0.grp[g].count;
+        const int ns = gm.nslot[g];
         if (g != cur_group) {
-          for (int q = 0; q < cnt; ++q) {
-            const PcEntry& Z = T0.Z[T0.order[first + q]];
+          for (int sl = 0; sl < ns; ++sl) {
+            const PcEntry& Z = T0.Z[T0.order[gm.rep[g * 8 + sl]]];
             cplx t[8];
 #pragma unroll
             for (int h = 0; h < 8; ++h) t[h] = mk(0, 0);
             pc_acc(Z.c, Z.sidx, E, mk(1, 0), t);
 #pragma unroll
-            for (int h = 0; h < 8; ++h) hzg[(q * 8 + h) * 32 + lane] = t[h];
+            for (int h = 0; h < 8; ++h) hzg[(sl * 8 + h) * 32 + lane] = t[h];
           }
           cur_group = g;
         }
         cplx dr[MAX_GROUP_ENTRIES];
-        if (!group_lineshapes<FIX>(Tp, g, mz, dr))
-          for (int q = 0; q < cnt; ++q) dr[q] = r0s[(first + q) * 32 + lane];
-        for (int q = 0; q < cnt; ++q) {
-          const cplx dq = dr[q] - r0s[(first + q) * 32 + lane];
+        if (!group_lineshapes<FIX>(Tp, g, mz, dr)) {
 #pragma unroll
-          for (int h = 0; h < 8; ++h) cmac(d[h], dq, hzg[(q * 8 + h) * 32 + lane]);
+          for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) dr[q] = q < cnt ? r0s[(first + q) * 32 + lane] : mk(0, 0);
+        }
+        cplx dsl[MAX_GROUP_ENTRIES];  // lineshape change summed per coupling slot
+#pragma unroll
+        for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) dsl[q] = mk(0, 0);
+#pragma unroll
+        for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) {
+          if (q >= cnt) break;
+          const cplx dq = dr[q] - r0s[(first + q) * 32 + lane];
+          const int sl = gm.slot[first + q];
+#pragma unroll
+          for (int t = 0; t < MAX_GROUP_ENTRIES; ++t)
+            if (t == sl) dsl[t] += dq;
+        }
+#pragma unroll
+        for (int sl = 0; sl < MAX_GROUP_ENTRIES; ++sl) {
+          if (sl >= ns) break;
+#pragma unroll
+          for (int h = 0; h < 8; ++h) cmac(d[h], dsl[sl], hzg[(sl * 8 + h) * 32 + lane]);
         }
       }
       const bool to_hl = kind == BP_LSTAR;
@@ -674,8 +735,7 @@ cudaError_t configure_batch_kernels() {
   if ((e = cudaGetDevice(&dev))) return e;
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
   optin -= 1024;  // the kernels' static shared memory stays below 1 KB
-  if ((e = set_batch_smem<0, false>(optin)) || (e = set_batch_smem<0, true>(optin)) ||
-      (e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
+  if ((e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
       (e = set_batch_smem<30, false>(optin)) || (e = set_batch_smem<30, true>(optin)) ||
       (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)))
     return e;
@@ -686,6 +746,26 @@ cudaError_t configure_batch_kernels() {
 }
 
 static bool same_bytes(const void* a, const void* b, size_t n) { return std::memcmp(a, b, n) == 0; }
+
+BatchGroupMap batch_group_map(const PointTable& T0) {
+  BatchGroupMap m;
+  std::memset(&m, 0, sizeof(m));
+  for (int g = 0; g < T0.ngroups; ++g) {
+    const PcGroup& gr = T0.grp[g];
+    int ns = 0;
+    for (int q = 0; q < gr.count; ++q) {
+      const int pos = gr.first + q;
+      const cplx* c = T0.Z[T0.order[pos]].c;
+      int sl = 0;
+      while (sl < ns && !same_bytes(T0.Z[T0.order[m.rep[g * 8 + sl]]].c, c, 24 * sizeof(cplx))) ++sl;
+      if (sl == ns) m.rep[g * 8 + ns++] = pos;
+      m.slot[pos] = sl;
+    }
+    m.nslot[g] = ns;
+    m.max_slots = ns > m.max_slots ? ns : m.max_slots;
+  }
+  return m;
+}
 
 bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, cplx* dc_host) {
   *bp = BatchPoint{};
@@ -740,6 +820,22 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
   if (lmask) {
     bp->kind = BP_LSTAR;
     bp->lmask = lmask;
+    int u = 0;
+    for (int r = 0; r < T0.NR; ++r) {
+      if (!(lmask >> r & 1)) continue;
+      LstarEntry a = T0.L[r], b = Tp.L[r];
+      const bool coup = !same_bytes(a.c, b.c, sizeof(a.c));
+      std::memset(a.c, 0, sizeof(a.c));
+      std::memset(b.c, 0, sizeof(b.c));
+      if (!same_bytes(&a, &b, sizeof(LstarEntry))) bp->lsmask |= 1u << r;
+      if (coup) {
+        bp->lcmask |= 1u << r;
+        if (u < BATCH_MAXQ)
+          for (int sl = 0; sl < 12; ++sl) dc_host[u * 24 + sl] = Tp.L[r].c[sl] - T0.L[r].c[sl];
+        ++u;
+      }
+    }
+    bp->ldc = u <= BATCH_MAXQ ? 1 : 0;
     return true;
   }
   if (ncoup) {
@@ -761,13 +857,13 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
 
 static int batch_nb(int kind) { return kind == SMEAR_20 ? 20 : kind == SMEAR_30 ? 30 : kind == SMEAR_150 ? 150 : 0; }
 
-static int batch_grid(const Segment& s, const PointTable& T0, int npts, int sm_count) {
+static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count) {
   const int64_t n = s.end - s.begin;
   int occ = 1;
   int64_t b;
   if (batch_nb(s.kind) == 0) {
     b = (n + BU_THREADS - 1) / BU_THREADS;
-    const size_t smem = batch_un_layout(T0.NR, T0.NZ, max_group(T0), npts).total;
+    const size_t smem = batch_un_layout(T0.NR, T0.NZ, gm.max_slots, npts).total;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_un<false>, BU_THREADS, smem);
   } else {
     b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
@@ -785,8 +881,9 @@ static int batch_grid(const Segment& s, const PointTable& T0, int npts, int sm_c
   return (int)b;
 }
 
-int batch_segment_rows(const Segment& s, const PointTable& T0, int npts, int sm_count, bool deferred) {
-  const int g = batch_grid(s, T0, npts, sm_count);
+int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count,
+                       bool deferred) {
+  const int g = batch_grid(s, T0, gm, npts, sm_count);
   return deferred ? 2 * g : g;
 }
 
@@ -803,17 +900,18 @@ static void launch_batch_kind(const EventSet& ev, int64_t begin, int64_t end, co
 }
 
 static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t end, const int32_t* list,
-                            const int* n_list, const PointTable* d_T0, const BatchPoint* d_pts, int npts, Partial* out,
+                            const int* n_list, const PointTable* d_T0, const BatchGroupMap& gm,
+                            const BatchPoint* d_pts, int npts, Partial* out,
                             int band, int32_t* defer, int* defer_count, bool fix, int grid, size_t smem,
                             cudaStream_t st) {
   switch (nb) {
     case 0:
       if (fix)
-        k_batch_un<true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, defer,
-                                                          defer_count);
+        k_batch_un<true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts, out,
+                                                          defer, defer_count);
       else
-        k_batch_un<false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, defer,
-                                                           defer_count);
+        k_batch_un<false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts, out,
+                                                           defer, defer_count);
       break;
     case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
     case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
@@ -822,23 +920,23 @@ static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t e
 }
 
 cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
-                                 const BatchPoint* d_pts, int npts, Partial* out, int32_t* defer, int* defer_count,
-                                 int sm_count, cudaStream_t st) {
+                                 const BatchGroupMap& gm, const BatchPoint* d_pts, int npts, Partial* out,
+                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st) {
   if (seg.end <= seg.begin) return cudaSuccess;
   if (npts < 1 || npts > BATCH_MAX_POINTS) return cudaErrorInvalidValue;
   const int nb = batch_nb(seg.kind);
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
-  const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, max_group(T0), npts).total
+  const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, gm.max_slots, npts).total
                               : batch_layout(T0.NR, T0.NZ, npts).total;
-  const int grid = batch_grid(seg, T0, npts, sm_count);
+  const int grid = batch_grid(seg, T0, gm, npts, sm_count);
   if (defer) {
-    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, d_pts, npts, out, band, defer, defer_count,
-                    false, grid, smem, st);
-    launch_batch_nb(nb, ev, 0, 0, defer, defer_count, d_T0, d_pts, npts, out + (size_t)grid * npts, band, nullptr,
-                    nullptr, true, grid, smem, st);
+    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, defer,
+                    defer_count, false, grid, smem, st);
+    launch_batch_nb(nb, ev, 0, 0, defer, defer_count, d_T0, gm, d_pts, npts, out + (size_t)grid * npts, band,
+                    nullptr, nullptr, true, grid, smem, st);
   } else {
-    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, d_pts, npts, out, band, nullptr, nullptr,
-                    true, grid, smem, st);
+    launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, nullptr,
+                    nullptr, true, grid, smem, st);
   }
   return cudaGetLastError();
 }

@@ -84,12 +84,26 @@ enum BatchKind : int { BP_SAME = 0, BP_LSTAR = 1, BP_PCC = 2, BP_PCG = 3 };
 struct BatchPoint {
   int kind;
   unsigned lmask;          // BP_LSTAR: changed Lambda* (bit r)
+  unsigned lsmask;         // BP_LSTAR: ... whose lineshape constants changed
+  unsigned lcmask;         // BP_LSTAR: ... whose couplings changed
+  int ldc;                 // BP_LSTAR: 1 when dc holds the coupling differences of the lcmask resonances
+                           // (in r order, 12 used of each 24), 0 when more than 8 changed
   int group;               // BP_PCG: Pc group whose lineshapes changed
   int nq;                  // BP_PCC: Pc entries whose couplings changed (at most 8)
   int qpos[8], qsidx[8];   // their order positions and d-function spin indices
   const cplx* dc;          // BP_PCC: coupling differences point - centre, [nq][24] (device)
   const PointTable* T;     // device copy of the point's table (BP_LSTAR, BP_PCG)
 };
+
+// Per Pc group of the batch centre: entries with identical couplings (the non-resonant K-matrix
+// entries of a J^P group share theirs) share one slot of the per-event angular amplitudes.
+struct BatchGroupMap {
+  int slot[MAX_PC];             // order position -> slot within its group
+  int nslot[MAX_GROUPS];        // slots per group
+  int rep[MAX_GROUPS * 8];      // [g * 8 + s] -> order position of the entry representing slot s
+  int max_slots;
+};
+BatchGroupMap batch_group_map(const PointTable& T0);
 
 // Classifies point Tp against the batch centre T0: fills bp (kind, masks; bp->dc and bp->T are left
 // for the caller) and, for BP_PCC, the coupling differences dc_host[nq][24].  Returns false when the
@@ -101,12 +115,13 @@ constexpr int BATCH_MAX_POINTS = 320;
 
 // Partial rows a segment of a batched evaluation writes (its pass, plus the deferred pass when
 // deferred is true); each row holds npts partials.
-int batch_segment_rows(const Segment& s, const PointTable& T0, int npts, int sm_count, bool deferred);
+int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count,
+                       bool deferred);
 
 // Launches the batched passes over one segment: partial rows out[0 .. batch_segment_rows) x npts.
 cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
-                                 const BatchPoint* d_pts, int npts, Partial* out, int32_t* defer, int* defer_count,
-                                 int sm_count, cudaStream_t st);
+                                 const BatchGroupMap& gm, const BatchPoint* d_pts, int npts, Partial* out,
+                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st);
 
 // Reduces rows x npts partials (row-major) into npts results.
 cudaError_t launch_finalize_points(const Partial* parts, int rows, int npts, double sum_w_mc, double sum_w_data,
