@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .model import Model, build_param_block
+from .model import BlockBuilder, Model
 
 
 def default_step(value: float, rel: float = 1e-3, floor: float = 1e-4) -> float:
@@ -33,7 +33,11 @@ def gradient_points(model: Model, vals: dict, names=None, steps: dict | None = N
 
 def gradient_blocks(model: Model, vals: dict, names=None, steps: dict | None = None) -> tuple:
     labels, points = gradient_points(model, vals, names, steps)
-    return labels, [build_param_block(model, v) for v in points]
+    builder = BlockBuilder(model, vals)
+    blocks = [builder.block()]
+    for (name, _), v in zip(labels[1:], points[1:]):
+        blocks.append(builder.block({name: v[name]}))
+    return labels, blocks
 
 
 def numerical_gradient(labels: list, points: list, fvals) -> dict:

@@ -329,64 +329,73 @@ class ParamBlock:
         return self.para_size + self.vamp_size + self.spline_size
 
 
-def build_param_block(model: Model, vals: dict, include: tuple | None = None) -> ParamBlock:
-    """The float parameter block for one parameter point (ConfigureCouplings + cu_init_data).
-    include: optional (Lambda* indices, Pc indices) whose couplings are kept (SetupCoupling);
-    the others are zeroed, as for per-resonance weights."""
-    res = model.resonances
-    table = np.zeros(NSET * len(res), f32)
+def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tuple:
+    """The pieces of the parameter block one resonance contributes: its table row (NSET floats), its
+    helicity couplings (float Re/Im pairs) and its K-matrix inputs (('g', group, g1..g4) for a pole,
+    ('f', group, f) for a non-resonant term, or None)."""
+    r = model.resonances[ir]
+    q = np.zeros(NSET, f32)
+    q[0] = f32(model.value(vals, r.mass))
+    q[1] = f32(model.value(vals, r.width))
+    q[2] = r.spin2
+    q[3] = orbital_l(r)
+    q[4] = r.type
+    q[5] = r.parity
+    lsc = [complex(model.value(vals, r.couplings[2 * i]), model.value(vals, r.couplings[2 * i + 1]))
+           for i in range(len(r.couplings) // 2)]
     vamp: list = []
+    km = None
+    if r.chain == "L":
+        S = f32(r.spin2) / f32(2)
+        sc = complex(model.value(vals, r.extra[0]), model.value(vals, r.extra[1]))
+        for k in range(2):
+            pp = _pow_m1(int(S - 1.5)) * r.parity if k == 0 else 1.0
+            for m in range(6):
+                if r.spin2 == 1 and m >= 4:
+                    continue
+                h2 = HEL2[m]
+                a = part_wave_lstar(lsc, r.spin2, HEL1_TWO[m], h2 * 2) * pp
+                a = a * _pow_m1(1 - h2)
+                a = a * sc
+                vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+        if r.type not in (BREITWIGNER, NONRESONANT):
+            raise NotImplementedError(f"Lambda* lineshape type {r.type}")
+    else:
+        S = r.spin2 / 2.0
+        for k in range(2):
+            for hpsi in (-1, 0, 1):
+                for ihz in range(2):
+                    hz = -0.5 if ihz == 0 else 0.5
+                    for ihp in range(2):
+                        hp = -0.5 if ihp == 0 else 0.5
+                        if abs(hpsi - hp) > S:
+                            continue
+                        a = part_wave_pc(lsc, r.parity, r.spin2, int(hz * 2), hpsi * 2, int(hp * 2))
+                        a = a * _pow_m1(1 - ihp)
+                        vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+        if r.type == KMATRIX:
+            ik = km_group(r)
+            if q[0] > 0:
+                km = ("g", ik, [f32(model.value(vals, g)) for g in r.extra[:4]])
+            else:
+                km = ("f", ik, f32(model.value(vals, r.extra[0])))
+        elif r.type not in (BREITWIGNER, NONRESONANT):
+            raise NotImplementedError(f"Pc lineshape type {r.type}")
+    return q, vamp, km
+
+
+def _assemble_block(model: Model, parts: list) -> ParamBlock:
+    table = np.concatenate([p[0] for p in parts]) if parts else np.zeros(0, f32)
+    vamp = [x for p in parts for x in p[1]]
     galpha = [[] for _ in range(4)]
     fscat = [[] for _ in range(4)]
-    for ir, r in enumerate(res):
-        q = table[ir * NSET:(ir + 1) * NSET]
-        q[0] = f32(model.value(vals, r.mass))
-        q[1] = f32(model.value(vals, r.width))
-        q[2] = r.spin2
-        q[3] = orbital_l(r)
-        q[4] = r.type
-        q[5] = r.parity
-        lsc = [complex(model.value(vals, r.couplings[2 * i]), model.value(vals, r.couplings[2 * i + 1]))
-               for i in range(len(r.couplings) // 2)]
-        keep = True
-        if include is not None:
-            keep = (ir in include[0]) if r.chain == "L" else ((ir - model.NR) in include[1])
-        if r.chain == "L":
-            S = f32(r.spin2) / f32(2)
-            sc = complex(model.value(vals, r.extra[0]), model.value(vals, r.extra[1]))
-            for k in range(2):
-                pp = _pow_m1(int(S - 1.5)) * r.parity if k == 0 else 1.0
-                for m in range(6):
-                    if r.spin2 == 1 and m >= 4:
-                        continue
-                    h2 = HEL2[m]
-                    a = part_wave_lstar(lsc, r.spin2, HEL1_TWO[m], h2 * 2) * pp
-                    a = a * _pow_m1(1 - h2)
-                    a = a * sc
-                    vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+    for _, _, km in parts:
+        if km is None:
+            continue
+        if km[0] == "g":
+            galpha[km[1]] += km[2]
         else:
-            S = r.spin2 / 2.0
-            for k in range(2):
-                for hpsi in (-1, 0, 1):
-                    for ihz in range(2):
-                        hz = -0.5 if ihz == 0 else 0.5
-                        for ihp in range(2):
-                            hp = -0.5 if ihp == 0 else 0.5
-                            if abs(hpsi - hp) > S:
-                                continue
-                            a = part_wave_pc(lsc, r.parity, r.spin2, int(hz * 2), hpsi * 2, int(hp * 2))
-                            a = a * _pow_m1(1 - ihp)
-                            vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
-            if r.type == KMATRIX:
-                ik = km_group(r)
-                if q[0] > 0:
-                    galpha[ik] += [f32(model.value(vals, g)) for g in r.extra[:4]]
-                else:
-                    fscat[ik].append(f32(model.value(vals, r.extra[0])))
-            elif r.type not in (BREITWIGNER, NONRESONANT):
-                raise NotImplementedError(f"Pc lineshape type {r.type}")
-        if r.chain == "L" and r.type not in (BREITWIGNER, NONRESONANT):
-            raise NotImplementedError(f"Lambda* lineshape type {r.type}")
+            fscat[km[1]].append(km[2])
     km = []
     for ik in range(4):
         g = galpha[ik][: NPMAX * NKMC]
@@ -396,8 +405,56 @@ def build_param_block(model: Model, vals: dict, include: tuple | None = None) ->
         for i in range(1, NKMC):
             f[NKMC * i] = f[i]
         km += g + [f32(0)] * (NPMAX * NKMC - len(g)) + f
-    data = np.concatenate([table, np.array(vamp, f32), np.array(km, f32)]).astype(f32)
+    data = np.concatenate([table.astype(f32), np.array(vamp, f32), np.array(km, f32)]).astype(f32)
     return ParamBlock(data, len(table), len(vamp), 0, model.NR, model.NZ, 0, model.ffr, model.ffb)
+
+
+def build_param_block(model: Model, vals: dict, include: tuple | None = None) -> ParamBlock:
+    """The float parameter block for one parameter point (ConfigureCouplings + cu_init_data).
+    include: optional (Lambda* indices, Pc indices) whose couplings are kept (SetupCoupling);
+    the others are zeroed, as for per-resonance weights."""
+    parts = []
+    for ir, r in enumerate(model.resonances):
+        keep = True
+        if include is not None:
+            keep = (ir in include[0]) if r.chain == "L" else ((ir - model.NR) in include[1])
+        parts.append(_resonance_parts(model, vals, ir, keep))
+    return _assemble_block(model, parts)
+
+
+class BlockBuilder:
+    """Parameter blocks of points that differ from a base point in a few parameters (Minuit's
+    gradient and line-search points): only the resonances a changed parameter enters are recomputed,
+    and the result is identical to build_param_block of the same values."""
+
+    def __init__(self, model: Model, vals: dict):
+        self.model = model
+        self.base = dict(vals)
+        self.parts = [_resonance_parts(model, vals, i) for i in range(len(model.resonances))]
+        self.uses: dict = {}
+        everything = list(range(len(model.resonances)))
+        for i, r in enumerate(model.resonances):
+            refs = [x for x in (*r.couplings, *r.extra, r.mass, r.width) if isinstance(x, str)]
+            for x in refs:
+                if x in model.derived:  # derived values may read any parameter
+                    for n in list(vals):
+                        self.uses.setdefault(n, set()).update(everything)
+                else:
+                    self.uses.setdefault(x, set()).add(i)
+
+    def block(self, changes: dict | None = None) -> ParamBlock:
+        changes = changes or {}
+        if not changes:
+            return _assemble_block(self.model, self.parts)
+        vals = dict(self.base)
+        vals.update(changes)
+        parts = list(self.parts)
+        touched = set()
+        for n in changes:
+            touched |= self.uses.get(n, set())
+        for i in touched:
+            parts[i] = _resonance_parts(self.model, vals, i)
+        return _assemble_block(self.model, parts)
 
 
 # ------------------------------------------------------------------ parameter files
