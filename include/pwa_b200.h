@@ -96,6 +96,13 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* ctx, const float* h_paraLists, int npoints, 
  * evaluated one by one). */
 double pwa_ctx_last_batch_ms(pwa_ctx* ctx);
 
+/* Sum over the MC events of w * |A|^2 (unsmeared |A|^2 as host_store_amp2s gives it, w the event weight):
+ * the normalisation integral of one parameter block that the reference's fit and interference
+ * fractions divide (RooDalitzAmplitude::getIFandFF, src/RooDalitzAmplitude.cxx:5250-5435, evaluated
+ * with subset couplings as in storeResonanceWeights :985-1292). */
+int pwa_ctx_mc_integral(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size,
+                        int NR, int NZ, int NX, float FFR, float FFB, double* integral);
+
 /* Per-event unsmeared |A|^2 for toy weights (host_store_amp2s, kernel_calEva.cu:1376-1419). */
 int pwa_ctx_amp2(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR,
                  int NZ, int NX, float FFR, float FFB, double* h_amp2);

@@ -526,6 +526,35 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
   return PWA_OK;
 }
 
+int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                        int NX, float FFR, float FFB, double* integral) {
+  if (!c || !pl || !integral) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  if (spline_size != 0) return PWA_E_UNSUPPORTED;
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  if (rc) return rc;
+  PWA_CUDA(cudaSetDevice(c->device));
+  if (c->fx_cap < c->n) {
+    cudaFree(c->d_fx);
+    c->d_fx = nullptr;
+    PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
+    c->fx_cap = c->n;
+  }
+  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  int launches = 0;
+  if ((rc = upload_point(c, &launches))) return rc;
+  const bool defer = c->h_table->tab.enabled != 0;
+  if (defer) PWA_CUDA(cudaMemsetAsync(c->d_defer_cnt + 7, 0, sizeof(int), c->st));
+  PWA_CUDA(launch_amp2(ev, c->d_table, c->d_fx, defer ? c->d_defer : nullptr, defer ? c->d_defer_cnt + 7 : nullptr,
+                       c->sm_count, c->st));
+  const int nb = std::max(1, std::min(c->total_parts, 2 * c->sm_count));
+  PWA_CUDA(launch_mc_integral(ev, c->d_fx, c->d_parts, nb, c->d_res, c->st));
+  PWA_CUDA(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, c->st));
+  PWA_CUDA(cudaStreamSynchronize(c->st));
+  *integral = c->h_res->sumint;
+  return PWA_OK;
+}
+
 int pwa_host_lineshapes(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                         float FFR, float FFB, double mkp, double mz, double* lstar, double* pc) {
   if (!pl || !lstar || !pc) return PWA_E_ARG;

@@ -578,6 +578,22 @@ cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, d
   return cudaGetLastError();
 }
 
+// Sum over MC events (index >= nda) of w * fx[e], w the event's weight plane; one partial per block.
+__global__ void k_mc_integral(EventSet ev, const double* __restrict__ fx, Partial* parts) {
+  double acc = 0;
+  for (int64_t e = ev.nda + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ev.n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    acc += fx[e] * (double)__ldg(ev.pp + 2 * ev.n_size + e);
+  block_reduce_store<256>(0.0, acc, 0.0, 0.0, parts);
+}
+
+cudaError_t launch_mc_integral(const EventSet& ev, const double* fx, Partial* parts, int nblocks, EvalResult* res,
+                               cudaStream_t st) {
+  k_mc_integral<<<nblocks, 256, 0, st>>>(ev, fx, parts);
+  k_finalize<<<1, 32, 0, st>>>(parts, nblocks, 1, 1.0, 0.0, 0.0, res);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int32_t* defer, int* defer_count,
                         int sm_count, cudaStream_t st) {
   const Segment seg{SMEAR_NONE, 0, ev.n, nullptr};

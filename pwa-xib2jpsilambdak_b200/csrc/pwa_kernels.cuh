@@ -129,6 +129,11 @@ cudaError_t launch_finalize_points(const Partial* parts, int rows, int npts, dou
 
 cudaError_t configure_batch_kernels();
 
+// Sum over the MC events of w * fx (fx: per-event values on the device) into res->sumint, through
+// nblocks partial slots.
+cudaError_t launch_mc_integral(const EventSet& ev, const double* fx, Partial* parts, int nblocks, EvalResult* res,
+                               cudaStream_t st);
+
 // Per-event unsmeared |A|^2 without weights (host_store_amp2s semantics) for n events.
 cudaError_t launch_amp2(const EventSet& ev, const PointTable* d_table, double* out, int32_t* defer, int* defer_count,
                         int sm_count, cudaStream_t st);

@@ -16,7 +16,7 @@ import os
 LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
-            "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
+            "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
@@ -53,6 +53,8 @@ def load() -> C.CDLL:
                                        C.POINTER(PwaResult), _dp]
         L.pwa_ctx_amp2.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_float, C.c_float, _dp]
+        L.pwa_ctx_mc_integral.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_float, C.c_float, _dp]
         L.pwa_ctx_eval_nll_batch.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
                                              C.c_double, C.POINTER(PwaResult), C.POINTER(C.c_int)]
@@ -179,6 +181,15 @@ class Context:
 
     def last_batch_ms(self) -> float:
         return self.L.pwa_ctx_last_batch_ms(self.h)
+
+    def mc_integral(self, block) -> float:
+        """Sum over the MC events of w * unsmeared |A|^2 (pwa_ctx_mc_integral)."""
+        pl = np.ascontiguousarray(block.data, np.float32)
+        out = C.c_double()
+        check(self.L.pwa_ctx_mc_integral(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size,
+                                         block.NR, block.NZ, block.NX, block.ffr, block.ffb, C.byref(out)),
+              "pwa_ctx_mc_integral")
+        return out.value
 
     def amp2(self, block) -> np.ndarray:
         pl = np.ascontiguousarray(block.data, np.float32)
