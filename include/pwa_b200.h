@@ -72,6 +72,18 @@ int pwa_ctx_set_device_events(pwa_ctx* ctx, const float* d_pp, const float* d_pp
                               const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
                               int64_t nda_fine);
 
+/* Data in any order (gen_toys/rearrange_mJpsip/reOrder.C made the reference's inputs legal by sorting
+ * them): the data columns [0, nda) are put into the three m(J/psi p) bands (30-offset, 150-offset,
+ * unsmeared; order kept inside each band) before the upload, and the band counts are derived as
+ * RooDalitzAmplitude does (src/RooDalitzAmplitude.cxx:391-396, passing the band-1 count minus one as
+ * IntegralMethod2 does).  Per-event outputs (h_fx, amp2) come back in the caller's order. */
+int pwa_ctx_upload_events_unsorted(pwa_ctx* ctx, const float* h_pp, const float* h_pp1, const float* h_pp2,
+                                   const float* h_sw, int64_t n, int64_t n_size, int64_t nda);
+
+/* The reOrder.C permutation of nda data masses (float m(J/psi p)): order[i] = index of the i-th
+ * event in band order; band counts of the 30- and 150-offset bands.  Host only. */
+int pwa_band_order(const float* mz, int64_t nda, int32_t* order, int64_t* n_band1, int64_t* n_band2);
+
 /* One likelihood evaluation (host_store_fx, kernel_calEva.cu:1186-1363): parameter block from host
  * memory in, result out; h_fx (optional, n doubles) receives per-event fx like the reference's
  * store_h_fx copy.  Blocks until the result is on the host. */

@@ -71,6 +71,8 @@ struct pwa_ctx {
   std::vector<cudaEvent_t> seg_ev;
   std::vector<double> seg_ms;
   int h_defer_cnt[8] = {};  // deferred events per segment of the last timed evaluation
+  // data uploaded unsorted: device position i < nda holds the caller's data event order[i]
+  std::vector<int32_t> order;
   // batched evaluation (grow-only buffers)
   std::vector<void*> bt_tabs;        // lineshape tables of points that move a Pc lineshape
   PointTable* d_btables = nullptr;   // decoded tables of the points of one launch
@@ -103,7 +105,15 @@ void free_events(pwa_ctx* c) {
   c->segs.clear();
   c->seg_off.clear();
   c->seg_defer_off.clear();
+  c->order.clear();
   c->n = 0;
+}
+
+// Per-event outputs of the device order back into the caller's order (data uploaded unsorted).
+void to_caller_order(const pwa_ctx* c, double* h) {
+  if (c->order.empty()) return;
+  std::vector<double> t(h, h + c->order.size());
+  for (size_t i = 0; i < c->order.size(); ++i) h[c->order[i]] = t[i];
 }
 
 // Splits the events into the reference's kernel ranges (fake_kernel_store_fx,
@@ -255,6 +265,53 @@ int pwa_ctx_upload_events(pwa_ctx* c, const float* pp, const float* pp1, const f
   return build_segments(c, pp + n_size);
 }
 
+int pwa_band_order(const float* mz, int64_t nda, int32_t* order, int64_t* n_band1, int64_t* n_band2) {
+  if ((nda > 0 && (!mz || !order)) || nda < 0 || !n_band1 || !n_band2) return PWA_E_ARG;
+  // reOrder.C: (4.2, 4.43) U (4.47, 4.6), then (4.43, 4.47), then the rest, order kept inside each
+  auto band = [](double m) {
+    if ((m > 4.2 && m < 4.43) || (m > 4.47 && m < 4.6)) return 1;
+    if (m > 4.43 && m < 4.47) return 2;
+    return 3;
+  };
+  int64_t k = 0, n1 = 0, n2 = 0;
+  for (int b = 1; b <= 3; ++b)
+    for (int64_t i = 0; i < nda; ++i)
+      if (band((double)mz[i]) == b) {
+        order[k++] = (int32_t)i;
+        n1 += b == 1;
+        n2 += b == 2;
+      }
+  *n_band1 = n1;
+  *n_band2 = n2;
+  return PWA_OK;
+}
+
+int pwa_ctx_upload_events_unsorted(pwa_ctx* c, const float* pp, const float* pp1, const float* pp2, const float* sw,
+                                   int64_t n, int64_t n_size, int64_t nda) {
+  if (!c || !pp || !pp1 || !pp2 || (nda > 0 && !sw)) return PWA_E_ARG;
+  int rc = check_events(n, n_size, nda);
+  if (rc) return rc;
+  std::vector<int32_t> order((size_t)nda);
+  int64_t n1 = 0, n2 = 0;
+  if ((rc = pwa_band_order(pp + n_size, nda, order.data(), &n1, &n2))) return rc;
+  // host copies with the data columns in band order (MC columns as given)
+  auto permute = [&](const float* src, int planes) {
+    std::vector<float> dst(src, src + (size_t)planes * n_size);
+    for (int p = 0; p < planes; ++p)
+      for (int64_t i = 0; i < nda; ++i) dst[(size_t)p * n_size + i] = src[(size_t)p * n_size + order[i]];
+    return dst;
+  };
+  const std::vector<float> a = permute(pp, 111), b = permute(pp1, 96), d = permute(pp2, 96);
+  std::vector<float> w;
+  if (sw) w = permute(sw, 1);
+  // the reference's caller passes the band-1 count minus one (RooDalitzAmplitude.cxx:1943-1946)
+  if ((rc = pwa_ctx_upload_events(c, a.data(), b.data(), d.data(), sw ? w.data() : nullptr, n, n_size, nda,
+                                  n1 - 1, n2)))
+    return rc;
+  c->order = std::move(order);
+  return PWA_OK;
+}
+
 int pwa_ctx_set_device_events(pwa_ctx* c, const float* d_pp, const float* d_pp1, const float* d_pp2,
                               const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
                               int64_t nda_fine) {
@@ -336,6 +393,7 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
   PWA_CUDA(cudaMemcpyAsync(c->h_res, c->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, c->st));
   if (h_fx && c->n) PWA_CUDA(cudaMemcpyAsync(h_fx, c->d_fx, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   PWA_CUDA(cudaStreamSynchronize(c->st));
+  if (h_fx) to_caller_order(c, h_fx);
   float ms = 0;
   cudaEventElapsedTime(&ms, c->e0, c->e1);
   c->last_ms = ms;
@@ -523,6 +581,7 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
                        c->sm_count, c->st));
   if (c->n) PWA_CUDA(cudaMemcpyAsync(h_amp2, c->d_fx, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   PWA_CUDA(cudaStreamSynchronize(c->st));
+  to_caller_order(c, h_amp2);
   return PWA_OK;
 }
 

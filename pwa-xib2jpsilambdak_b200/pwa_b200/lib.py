@@ -15,7 +15,7 @@ import os
 # The in-tree build; PWA_B200_LIB may name another build of the same library (A/B comparisons).
 LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
-EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_set_device_events",
+EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
@@ -23,6 +23,17 @@ EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_c
 
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
+
+
+def band_order(mz) -> tuple:
+    """(order, band-1 count, band-2 count) of data masses as the library sorts them (pwa_band_order)."""
+    L = load()
+    m = np.ascontiguousarray(mz, np.float32)
+    order = np.zeros(len(m), np.int32)
+    n1, n2 = C.c_int64(), C.c_int64()
+    check(L.pwa_band_order(_f(m), len(m), order.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n1), C.byref(n2)),
+          "pwa_band_order")
+    return order, n1.value, n2.value
 
 
 class PwaResult(C.Structure):
@@ -53,6 +64,9 @@ def load() -> C.CDLL:
                                        C.POINTER(PwaResult), _dp]
         L.pwa_ctx_amp2.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_float, C.c_float, _dp]
+        L.pwa_ctx_upload_events_unsorted.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp] + [C.c_int64] * 3
+        L.pwa_band_order.argtypes = [_fp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64)]
         L.pwa_ctx_mc_integral.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           C.c_float, C.c_float, _dp]
         L.pwa_ctx_eval_nll_batch.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -129,6 +143,18 @@ class Context:
         sw = np.ascontiguousarray(sample.sw, np.float32)
         check(self.L.pwa_ctx_upload_events(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n, sample.n_size,
                                            sample.nda, a, b), "pwa_ctx_upload_events")
+        self.sample = sample
+        self.n = sample.n
+
+    def upload_unsorted(self, sample):
+        """Upload a Sample whose data events are in any order (pwa_ctx_upload_events_unsorted): the
+        library sorts them into the m(J/psi p) bands and derives the band arguments itself."""
+        pp = np.ascontiguousarray(sample.pp, np.float32)
+        pp1 = np.ascontiguousarray(sample.pp1, np.float32)
+        pp2 = np.ascontiguousarray(sample.pp2, np.float32)
+        sw = np.ascontiguousarray(sample.sw, np.float32)
+        check(self.L.pwa_ctx_upload_events_unsorted(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n,
+                                                    sample.n_size, sample.nda), "pwa_ctx_upload_events_unsorted")
         self.sample = sample
         self.n = sample.n
 

@@ -80,3 +80,16 @@ def test_error_codes():
     assert L.pwa_host_lineshapes(None, *args, 0, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
                                  d.ctypes.data_as(dp)) == 2
     assert lib.load().pwa_error_string(5).decode().startswith("lineshape")
+
+
+def test_band_order_matches_reorder_semantics():
+    """pwa_band_order (host, no GPU) against the numpy restatement of reOrder.C."""
+    import numpy as np
+    from pwa_b200 import basis as B, lib
+    rng = np.random.default_rng(3)
+    mz = rng.uniform(4.05, 4.9, 5000).astype(np.float32)
+    order, n1, n2 = lib.band_order(mz)
+    ref = B.order_data_by_band(mz)
+    assert np.array_equal(order, ref)
+    b = B.band_of(mz)
+    assert n1 == int(np.sum(b == 1)) and n2 == int(np.sum(b == 2))

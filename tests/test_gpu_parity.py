@@ -77,3 +77,34 @@ def test_lineshape_tables_match_exact_solves(ctx, oracle_mod):
     assert abs(r1.nll - r0.nll) < 1e-7
     v, s, ofx, _ = oracle_mod.nll(smp, blk)
     assert abs(r1.nll - v) < NLL_TOL
+
+
+def test_unsorted_upload_matches_sorted(ctx):
+    """Data in shuffled order through pwa_ctx_upload_events_unsorted: same NLL as the band-sorted
+    upload, per-event fx returned in the caller's order."""
+    import copy
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    ctx.upload(smp)
+    r0, fx0 = ctx.eval_nll(blk, want_fx=True)
+    rng = np.random.default_rng(4)
+    perm = rng.permutation(smp.nda)
+    # the reference's caller passes the band-1 count minus one, so the last band-1 event by position is
+    # evaluated with 150 offsets and the last band-2 event with 20 (tail window): keep both last in
+    # their bands
+    last1, last2 = smp.nda_smr1 - 1, smp.nda_smr1 + smp.nda_fine - 1
+    perm = np.concatenate([perm[(perm != last1) & (perm != last2)], [last1, last2]])
+    sh = copy.copy(smp)
+    ns = smp.n_size
+    for name, planes in (("pp", 111), ("pp1", 96), ("pp2", 96)):
+        a = np.array(getattr(smp, name), np.float32).reshape(planes, ns).copy()
+        a[:, :smp.nda] = a[:, perm]
+        setattr(sh, name, a.reshape(-1))
+    sw = np.array(smp.sw, np.float32).copy()
+    sw[:smp.nda] = sw[perm]
+    sh.sw = sw
+    ctx.upload_unsorted(sh)
+    r1, fx1 = ctx.eval_nll(blk, want_fx=True)
+    assert abs(r1.nll - r0.nll) < NLL_TOL
+    assert np.array_equal(fx1[:smp.nda], fx0[perm])
+    assert np.array_equal(fx1[smp.nda:], fx0[smp.nda:])
+    ctx.upload(smp)
