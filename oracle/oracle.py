@@ -45,6 +45,13 @@ def lib():
         L.oracle_amp2.restype = C.c_int
         L.oracle_amp2.argtypes = [_fp, _fp, _fp, C.c_long, C.c_long, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_int, C.c_float, C.c_float, _dp, C.c_int]
+        L.oracle_eval_fx_x.restype = C.c_int
+        L.oracle_eval_fx_x.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, C.c_long, C.c_long, _fp,
+                                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                       C.c_int, _dp, _dp, C.c_int]
+        L.oracle_amp2_x.restype = C.c_int
+        L.oracle_amp2_x.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, _fp, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _dp, C.c_int]
         L.oracle_assemble_nll.restype = C.c_double
         L.oracle_assemble_nll.argtypes = [_dp, _dp, _fp, C.c_long, C.c_long, C.c_double, C.c_double, C.c_double, _dp]
         for f in ("oracle_bw_lstar", "oracle_bw_pc"):
@@ -63,17 +70,29 @@ def _f(a):
     return np.ascontiguousarray(a, np.float32).ctypes.data_as(_fp)
 
 
+def _planes_x(sample):
+    """Zcs chain planes of a sample (null pointers when the sample has none)."""
+    p3, p4 = getattr(sample, "pp3", None), getattr(sample, "pp4", None)
+    if p3 is None:
+        return None, None, None
+    a3 = np.ascontiguousarray(p3, np.float32)
+    a4 = np.ascontiguousarray(p4, np.float32)
+    return a3.ctypes.data_as(_fp), a4.ctypes.data_as(_fp), (a3, a4)
+
+
 def eval_fx(sample, block, nda_smr: int, nda_fine: int, swap_coupling_parts: bool = False,
             threads: int | None = None):
     """Per-event |A|^2 (fx) and non-interfering w|A|^2 with the reference's band dispatch."""
     fx = np.zeros(sample.n, np.float64)
     fxn = np.zeros(sample.n, np.float64)
     pl = np.ascontiguousarray(block.data, np.float32)
-    keep = (sample.pp, sample.pp1, sample.pp2, pl)
-    rc = lib().oracle_eval_fx(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), sample.n_size, sample.n, nda_smr,
-                              nda_fine, pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size,
-                              block.NR, block.NZ, block.NX, block.ffr, block.ffb, int(swap_coupling_parts),
-                              fx.ctypes.data_as(_dp), fxn.ctypes.data_as(_dp), threads or os.cpu_count())
+    p3, p4, kx = _planes_x(sample)
+    keep = (sample.pp, sample.pp1, sample.pp2, pl, kx)
+    rc = lib().oracle_eval_fx_x(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), p3, p4, sample.n_size, sample.n,
+                                nda_smr, nda_fine, pl.ctypes.data_as(_fp), block.para_size, block.vamp_size,
+                                block.spline_size, block.NR, block.NZ, block.NX, block.ffr, block.ffb,
+                                int(swap_coupling_parts), fx.ctypes.data_as(_dp), fxn.ctypes.data_as(_dp),
+                                threads or os.cpu_count())
     del keep
     if rc != 0:
         raise RuntimeError(f"oracle_eval_fx failed: {rc}")
@@ -84,9 +103,12 @@ def amp2(sample, block, threads: int | None = None) -> np.ndarray:
     """Unsmeared, unweighted coherent |A|^2 per event (host_store_amp2s semantics)."""
     out = np.zeros(sample.n, np.float64)
     pl = np.ascontiguousarray(block.data, np.float32)
-    rc = lib().oracle_amp2(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), sample.n_size, sample.n,
-                           pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size, block.NR,
-                           block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp), threads or os.cpu_count())
+    p3, p4, kx = _planes_x(sample)
+    rc = lib().oracle_amp2_x(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), p3, p4, sample.n_size, sample.n,
+                             pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size, block.NR,
+                             block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp),
+                             threads or os.cpu_count())
+    del kx
     if rc != 0:
         raise RuntimeError(f"oracle_amp2 failed: {rc}")
     return out
@@ -149,7 +171,9 @@ class RefHost:
         self.pp = np.ascontiguousarray(sample.pp, np.float32)
         self.pp1 = np.ascontiguousarray(sample.pp1, np.float32)
         self.pp2 = np.ascontiguousarray(sample.pp2, np.float32)
-        self.pp3 = np.zeros(16, np.float32)
+        p3, p4 = getattr(sample, "pp3", None), getattr(sample, "pp4", None)
+        self.pp3 = np.ascontiguousarray(p3, np.float32) if p3 is not None else np.zeros(16, np.float32)
+        self.pp4 = np.ascontiguousarray(p4, np.float32) if p4 is not None else np.zeros(16, np.float32)
         self.sw = np.ascontiguousarray(sample.sw, np.float32)
         self.L.ref_reset()
         pl = np.ascontiguousarray(block.data, np.float32)
@@ -161,7 +185,7 @@ class RefHost:
         pl = np.ascontiguousarray(block.data, np.float32)
         out = C.c_double()
         a, b = s.reference_band_args()
-        sumint = self.L.ref_host_store_fx(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp3),
+        sumint = self.L.ref_host_store_fx(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp4),
                                           _f(self.sw), pl.ctypes.data_as(_fp), block.para_size, block.vamp_size,
                                           block.spline_size, self.fx.ctypes.data_as(_dp), s.n, 0, s.nda, a, b,
                                           block.NR, block.NZ, block.NX, C.byref(out), s.sum_w_mc, s.sum_w_data,
@@ -171,7 +195,7 @@ class RefHost:
     def amp2s(self, block) -> np.ndarray:
         out = np.zeros(self.s.n, np.float64)
         pl = np.ascontiguousarray(block.data, np.float32)
-        self.L.ref_host_store_amp2s(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp3),
+        self.L.ref_host_store_amp2s(_f(self.pp), _f(self.pp1), _f(self.pp2), _f(self.pp3), _f(self.pp4),
                                     pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size,
                                     out.ctypes.data_as(_dp), self.s.n, block.NR, block.NZ, block.NX, block.ffr,
                                     block.ffb)

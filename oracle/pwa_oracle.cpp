@@ -172,6 +172,15 @@ double barrier_lb_pc(double J, double mpp, double mr, double ffb) {  // BTermZ
   return barrier_ratio(ffb, LB, pB, pB0) * std::pow(pB / M_LB, LB);
 }
 
+double barrier_lb_x(double J, double mpp, double mr, double ffb) {  // BTermX (cu_DPFPropogator.cu:205-217)
+  const int LB = (int)(J - 0.5);  // C truncation toward zero
+  const double pB = two_body_p(M_LB, M_P, mpp);
+  double pB0 = pB;
+  if (mr < 0) return std::pow(pB / M_LB, LB);
+  if (mr > 1e-10 && mr + M_P < M_LB) pB0 = two_body_p(M_LB, M_P, mr);
+  return barrier_ratio(ffb, LB, pB, pB0) * std::pow(pB / M_LB, LB);
+}
+
 // ---------------------------------------------------------------- Breit-Wigners (cu_DPFPropogator.cu:219-336)
 cd breit_wigner(double m, double gamma, double e2) {
   const double de2 = m * m - e2, gm = gamma * m, d = de2 * de2 + gm * gm;
@@ -217,6 +226,18 @@ cd bw_pc(double m_r, double gamma_r, double mpp, int LR, double ffr) {  // BW_AM
   double pR0 = pR;
   const double thr = F(M_P + M_JPSI);
   if (m_r > thr) pR0 = two_body_p(m_r, M_P, M_JPSI);
+  const double FR = barrier_ratio(ffr, LR, pR, pR0);
+  double gamma = gamma_r;
+  if (m_r > thr) gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp) * FR * FR;
+  const double factor = FR * std::pow(pR / pR0, LR) * bw_norm(m_r, gamma_r);
+  return factor * breit_wigner(m_r, gamma, mpp * mpp);
+}
+
+cd bw_x(double m_r, double gamma_r, double mpp, int LR, double ffr) {  // BW_AMPX (cu_DPFPropogator.cu:226-246)
+  const double pR = two_body_p(mpp, M_K, M_JPSI);
+  double pR0 = pR;
+  const double thr = F(M_K + M_JPSI);
+  if (m_r > thr) pR0 = two_body_p(m_r, M_K, M_JPSI);
   const double FR = barrier_ratio(ffr, LR, pR, pR0);
   double gamma = gamma_r;
   if (m_r > thr) gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp) * FR * FR;
@@ -413,9 +434,12 @@ struct Ev {
   const float *pp, *pp1, *pp2;
   long n;  // plane stride
   long i;  // event index
+  const float *pp3 = nullptr, *pp4 = nullptr;  // Zcs chain planes (NX > 0)
   double p0(int plane) const { return pp[i + plane * n]; }
   double p1(int plane) const { return pp1[i + plane * n]; }
   double p2(int plane) const { return pp2[i + plane * n]; }
+  double p3(int plane) const { return pp3[i + plane * n]; }
+  double p4(int plane) const { return pp4[i + plane * n]; }
 };
 
 inline cd read_coupling(const Model& md, int& cnt) {
@@ -460,6 +484,49 @@ bool amp_lstar(const Model& md, const Ev& e, cd* H) {
       }
   }
   return true;
+}
+
+// Zcs chain contribution to H[8] (GetAmpZcs, kernel_calEva.cu:192-286), reproducing how that kernel
+// walks the couplings: per proton helicity it reads consecutive couplings for (lambda_psi in -1..1,
+// lambda_p in {0, 1}, lambda_Zcs = lambda_p -+ 1/2) with |lambda_psi|, |lambda_Zcs| <= J, and the
+// running index m of those combinations selects the AX / DX planes.  (ConfigureCouplings wrote the
+// couplings for lambda_p = -+1/2 instead; the kernel's reading is what enters the likelihood.)
+void amp_zcs(const Model& md, const Ev& e, cd* H) {
+  const double mjk = e.p3(0);
+  for (int x = 0; x < md.NX; ++x) {
+    const int r = md.NR + md.NZ + x;
+    const float* q = &md.pl[r * NSET];
+    const double m0 = q[P_MASS], g0 = q[P_WIDTH];
+    const int S2 = (int)q[P_SPIN], LR = (int)q[P_LRESON];
+    const double S = 0.5 * S2;
+    const cd bw = barrier_lb_x(S, mjk, m0, md.FFB) * bw_x(m0, g0, mjk, LR, md.FFR);
+    int cnt = md.ampcount[r];
+    const int s = S2 / 2;
+    for (int k = 0; k < 2; ++k) {
+      int m = 0;
+      for (int hpsi = -1; hpsi <= 1; ++hpsi) {
+        if (std::fabs((double)hpsi) > S) continue;
+        for (int hp = 0; hp <= 1; ++hp)
+          for (int iz = 0; iz < 2; ++iz) {
+            const double hz = hp - 0.5 + iz;
+            if (std::fabs(hz) > S) continue;
+            const cd c = read_coupling(md, cnt);
+            if (std::abs(c) < 1e-10) {
+              ++m;
+              continue;
+            }
+            const double dx = e.p4(s * 24 + k * 12 + m);
+            for (int i = 0; i < 2; ++i)
+              for (int j = 0; j < 2; ++j) {
+                const int a = 1 + (i * 24 + j * 12 + m) * 2;
+                const cd A(e.p3(a), e.p3(a + 1));
+                H[4 * i + 2 * j + k] += dx * (A * bw) * c;
+              }
+            ++m;
+          }
+      }
+    }
+  }
 }
 
 // Angular part of one Pc entry times its couplings (no lineshape), added into HZ[8].
@@ -522,14 +589,15 @@ bool pc_lineshapes(const Model& md, double mz, double weight, cd* bw) {
 
 // Unsmeared |A|^2 (GetAmp2s): coherent sum, or the sum of the chains' separate |A|^2.
 double amp2_unsmeared(const Model& md, const Ev& e, bool interference) {
-  cd HL[8] = {}, HZ[8] = {};
+  cd HL[8] = {}, HX[8] = {}, HZ[8] = {};
   if (!amp_lstar(md, e, HL)) return std::nan("");
+  if (md.NX > 0) amp_zcs(md, e, HX);
   std::vector<cd> bw(std::max(md.NZ, 1));
   if (md.NZ > 0 && !pc_lineshapes(md, e.p0(1), 1.0, bw.data())) return std::nan("");
   for (int i = 0; i < md.NZ; ++i) amp_pc_angular(md, e, i, bw[i], HZ);
   double tot = 0;
   for (int h = 0; h < 8; ++h)
-    tot += interference ? std::norm(HL[h] + HZ[h]) : std::norm(HL[h]) + std::norm(HZ[h]);
+    tot += interference ? std::norm(HL[h] + HX[h] + HZ[h]) : std::norm(HL[h]) + std::norm(HX[h]) + std::norm(HZ[h]);
   return tot;
 }
 
@@ -538,8 +606,9 @@ double amp2_unsmeared(const Model& md, const Ev& e, bool interference) {
 // Pc-Pc accumulator is rescaled by its float reciprocal, exactly as the reference does
 // (kernel_calEva.cu:676,771-783), so the effective weights match to the last bit of the constants.
 double amp2_smeared(const Model& md, const Ev& e, int nbins, const float* scheme) {
-  cd HL[8] = {};
+  cd HL[8] = {};  // Lambda* and Zcs (H_L_Zcs of the reference)
   if (!amp_lstar(md, e, HL)) return std::nan("");
+  if (md.NX > 0) amp_zcs(md, e, HL);
   const int NZ = md.NZ;
   std::vector<cd> HZ(NZ * 8, cd(0, 0)), BW1(NZ, cd(0, 0)), BW2(NZ * NZ, cd(0, 0)), bw(std::max(NZ, 1));
   for (int i = 0; i < NZ; ++i) amp_pc_angular(md, e, i, cd(1, 0), &HZ[i * 8]);
@@ -580,11 +649,12 @@ extern "C" {
 //   [nda_smr + nda_fine, n_events)   20-offset smearing inside the MC windows, else unsmeared,
 //                                    times the event weight w unless w <= -1000 (data sentinel).
 // fx_noint receives w*|A|^2 without Pc/Lambda* interference (0 for data).  Returns 0 on success.
-int oracle_eval_fx(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
-                   long nda_smr, long nda_fine, const float* paraList, int para_size, int vamp_size,
-                   int spline_size, int NR, int NZ, int NX, float FFR, float FFB, int swap_coupling_parts,
-                   double* fx, double* fx_noint, int nthreads) {
-  if (NX != 0) return -10;  // the Zcs chain is not part of this oracle
+// pp3 / pp4: the Zcs chain planes (mJ/psi K, AX; DX), required when NX > 0.
+int oracle_eval_fx_x(const float* pp, const float* pp1, const float* pp2, const float* pp3, const float* pp4,
+                     long n_size, long n_events, long nda_smr, long nda_fine, const float* paraList, int para_size,
+                     int vamp_size, int spline_size, int NR, int NZ, int NX, float FFR, float FFB,
+                     int swap_coupling_parts, double* fx, double* fx_noint, int nthreads) {
+  if (NX > 0 && (!pp3 || !pp4)) return -10;
   Model md;
   md.pl = paraList;
   md.para_size = para_size;
@@ -602,7 +672,7 @@ int oracle_eval_fx(const float* pp, const float* pp1, const float* pp2, long n_s
   int err = 0;
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(| : err)
   for (long i = 0; i < n_events; ++i) {
-    Ev e{pp, pp1, pp2, n_size, i};
+    Ev e{pp, pp1, pp2, n_size, i, pp3, pp4};
     double v;
     if (i < b1) {
       v = amp2_smeared(md, e, 30, kSmear30);
@@ -625,12 +695,21 @@ int oracle_eval_fx(const float* pp, const float* pp1, const float* pp2, long n_s
   return err ? -12 : 0;
 }
 
+int oracle_eval_fx(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
+                   long nda_smr, long nda_fine, const float* paraList, int para_size, int vamp_size,
+                   int spline_size, int NR, int NZ, int NX, float FFR, float FFB, int swap_coupling_parts,
+                   double* fx, double* fx_noint, int nthreads) {
+  return oracle_eval_fx_x(pp, pp1, pp2, nullptr, nullptr, n_size, n_events, nda_smr, nda_fine, paraList,
+                          para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, swap_coupling_parts, fx,
+                          fx_noint, nthreads);
+}
+
 // Per-event unsmeared coherent |A|^2 without weights (GetAmp2s_NoSMR as used by
 // kernel_store_amp2s, kernel_calEva.cu:1365-1373).
-int oracle_amp2(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
-                const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
-                float FFR, float FFB, double* out, int nthreads) {
-  if (NX != 0) return -10;
+int oracle_amp2_x(const float* pp, const float* pp1, const float* pp2, const float* pp3, const float* pp4,
+                  long n_size, long n_events, const float* paraList, int para_size, int vamp_size, int spline_size,
+                  int NR, int NZ, int NX, float FFR, float FFB, double* out, int nthreads) {
+  if (NX > 0 && (!pp3 || !pp4)) return -10;
   Model md;
   md.pl = paraList;
   md.para_size = para_size;
@@ -638,17 +717,25 @@ int oracle_amp2(const float* pp, const float* pp1, const float* pp2, long n_size
   md.spline_size = spline_size;
   md.NR = NR;
   md.NZ = NZ;
+  md.NX = NX;
   md.FFR = FFR;
   md.FFB = FFB;
   configure(md);
   int err = 0;
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(| : err)
   for (long i = 0; i < n_events; ++i) {
-    Ev e{pp, pp1, pp2, n_size, i};
+    Ev e{pp, pp1, pp2, n_size, i, pp3, pp4};
     out[i] = amp2_unsmeared(md, e, true);
     if (std::isnan(out[i])) err |= 1;
   }
   return err ? -12 : 0;
+}
+
+int oracle_amp2(const float* pp, const float* pp1, const float* pp2, long n_size, long n_events,
+                const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                float FFR, float FFB, double* out, int nthreads) {
+  return oracle_amp2_x(pp, pp1, pp2, nullptr, nullptr, n_size, n_events, paraList, para_size, vamp_size,
+                       spline_size, NR, NZ, NX, FFR, FFB, out, nthreads);
 }
 
 // NLL assembly of host_store_fx (kernel_calEva.cu:1296-1362) from per-event values, with

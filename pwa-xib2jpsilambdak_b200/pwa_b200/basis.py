@@ -10,6 +10,8 @@ products are formed in double and stored as float.
   pp  (111 planes): 0 mKp, 1 mJ/psi p, 2 weight, 3.. ARe/AIm[i][j][m] interleaved, 51.. DL[s][k][m]
   pp1 (96 planes):  AZRe/AZIm[i][j][m] interleaved
   pp2 (96 planes):  DZ[s][k][m]
+  pp3 (97 planes):  0 mJ/psi K, 1.. AXRe/AXIm[i][j][m] interleaved       (Zcs chain, NX > 0 only)
+  pp4 (96 planes):  DX[s][k][m]
 """
 from __future__ import annotations
 
@@ -17,7 +19,7 @@ import math
 
 import numpy as np
 
-N_PP, N_PP1, N_PP2 = 111, 96, 96
+N_PP, N_PP1, N_PP2, N_PP3, N_PP4 = 111, 96, 96, 97, 96
 HEL1_TWO = (1, 1, -1, -1, 3, -3)  # 2 x helicity of Lambda* (RooDalitzAmplitude.cxx:110)
 HEL2 = (1, 0, 0, -1, 1, -1)  # helicity of J/psi in the Lambda* chain (:111)
 
@@ -181,6 +183,57 @@ def order_data_by_band(mz) -> np.ndarray:
     return np.concatenate([np.nonzero(b == 1)[0], np.nonzero(b == 2)[0], np.nonzero(b == 3)[0]])
 
 
+def fill_basis_x(ang: dict) -> dict:
+    """Zcs-chain basis per event (filldlz, RooDalitzAmplitude.cxx:7239-7303, with MEangXPart :2650-2665):
+    AXRe/AXIm (N,2,2,12) over all (J/psi, proton, Zcs) helicity combinations, DX (N,4,2,12) for
+    Zcs spins 0..3 over the combinations the spin allows (|lambda_psi|, |lambda_Zcs| <= J)."""
+    f32 = np.float32
+    acos32 = lambda x: np.arccos(np.asarray(x, np.float64)).astype(f32).astype(np.float64)
+    thB = acos32(ang["X_cosTheta_Lb"])
+    thX = acos32(ang["X_cosTheta_X"])
+    thPsi = acos32(ang["X_cosTheta_Jpsi"])
+    thp = acos32(ang["X_cosTheta_p"])
+    phiX = np.asarray(ang["X_phiX"]).astype(f32)
+    phiPsi = np.asarray(ang["X_phiJpsi"]).astype(f32)
+    phiMu = np.asarray(ang["X_phiMu"]).astype(f32)
+    alphaMu = np.asarray(ang["X_alpha_Mu"]).astype(f32)
+    n = thB.shape[0]
+    AXRe = np.zeros((n, 2, 2, 12), f32)
+    AXIm = np.zeros((n, 2, 2, 12), f32)
+    for i in range(2):
+        dmu = -1 if i == 0 else 1
+        for j in range(2):
+            hel0 = -0.5 if j == 0 else 0.5
+            m = 0
+            for hpsi in (-1, 0, 1):
+                for hp in (-0.5, 0.5):
+                    for helZ in (hp - 0.5, hp + 0.5):
+                        part = (((f32(hel0) * phiX + f32(hpsi) * phiMu) + f32(helZ - hp) * phiPsi)
+                                + f32(dmu) * alphaMu).astype(np.float64)
+                        d1 = dfun_one(thPsi, hpsi, dmu)
+                        dh = dfun_half(thB, int(hel0 * 2), int((helZ - hp) * 2))
+                        AXRe[:, i, j, m] = ((np.cos(part) * d1) * dh).astype(f32)
+                        AXIm[:, i, j, m] = ((np.sin(part) * d1) * dh).astype(f32)
+                        m += 1
+    DX = np.zeros((n, 4, 2, 12), f32)
+    for s in range(4):
+        S = float(s)
+        for k in range(2):
+            hel3 = -0.5 if k == 0 else 0.5
+            m = 0
+            for hpsi in (-1, 0, 1):
+                if abs(hpsi) > S:
+                    continue
+                for hp in (-0.5, 0.5):
+                    for helZ in (hp - 0.5, hp + 0.5):
+                        if abs(helZ) > S:
+                            continue
+                        DX[:, s, k, m] = (dfun_half(thp, int(hp * 2), int(hel3 * 2))
+                                          * dfun(thX, S, helZ, -hpsi)).astype(f32)
+                        m += 1
+    return {"AXRe": AXRe, "AXIm": AXIm, "DX": DX}
+
+
 def pack_soa(mkp, mz, w, basis: dict, n_size: int | None = None) -> dict:
     """Pack events into the reference device planes; returns dict pp, pp1, pp2 (float32, flat)."""
     n = len(mkp)
@@ -211,4 +264,21 @@ def pack_soa(mkp, mz, w, basis: dict, n_size: int | None = None) -> dict:
         for k in range(2):
             for m in range(12):
                 pp2[s * 24 + k * 12 + m, :n] = basis["DZ"][:, s, k, m]
-    return {"pp": pp.reshape(-1), "pp1": pp1.reshape(-1), "pp2": pp2.reshape(-1), "n_size": ns, "n": n}
+    out = {"pp": pp.reshape(-1), "pp1": pp1.reshape(-1), "pp2": pp2.reshape(-1), "n_size": ns, "n": n}
+    if "AXRe" in basis:
+        pp3 = np.zeros((N_PP3, ns), np.float32)
+        pp4 = np.zeros((N_PP4, ns), np.float32)
+        pp3[0, :n] = basis["mjpsik"]
+        for i in range(2):
+            for j in range(2):
+                for m in range(12):
+                    a = 1 + (i * 24 + j * 12 + m) * 2
+                    pp3[a, :n] = basis["AXRe"][:, i, j, m]
+                    pp3[a + 1, :n] = basis["AXIm"][:, i, j, m]
+        for s in range(4):
+            for k in range(2):
+                for m in range(12):
+                    pp4[s * 24 + k * 12 + m, :n] = basis["DX"][:, s, k, m]
+        out["pp3"] = pp3.reshape(-1)
+        out["pp4"] = pp4.reshape(-1)
+    return out

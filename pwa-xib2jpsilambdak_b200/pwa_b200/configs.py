@@ -66,6 +66,12 @@ def pc_km_nr(name: str, shared: str, s2: int, par: int) -> Resonance:
     return Resonance("Z", name, s2, par, KMATRIX, -0.5, 0.0, coup, (f"fsc_{name}",))
 
 
+def zcs_bw(name: str, s2: int, par: int) -> Resonance:
+    # RooTDalitz/ResX.h: four Lambda_b -> Zcs p couplings (L0..L3), then the Zcs -> J/psi K one (Bp)
+    coup = tuple(f"{ap}_{t}_{name}" for t in ("L0", "L1", "L2", "L3", "Bp") for ap in ("a", "p"))
+    return Resonance("X", name, s2, par, BREITWIGNER, f"m0_{name}", f"width_{name}", coup)
+
+
 def _seed_couplings(model: Model, vals: dict, rng, scale=1.0):
     for r in model.resonances:
         for i in range(0, len(r.couplings), 2):
@@ -163,6 +169,20 @@ def small_kmatrix(seed: int = 4) -> tuple:
     return m, vals
 
 
+def small_zcs(seed: int = 6) -> tuple:
+    """Two Lambda*, a Breit-Wigner Pc and the two Zcs -> J/psi K states of RooTDalitz/ResX.h (1+, 1-)."""
+    names = ["1520", "1800"]
+    m = Model([lstar_resonance(n) for n in names], [pc_bw("Pc4312", 1, -1)],
+              zcs=[zcs_bw("Xplus", 2, +1), zcs_bw("Xminus", 2, -1)])
+    vals = {}
+    _lstar_vals(names, vals)
+    vals["m0_Pc4312"], vals["width_Pc4312"] = 4.312, 0.010
+    vals["m0_Xplus"], vals["width_Xplus"] = 4.003, 0.131
+    vals["m0_Xminus"], vals["width_Xminus"] = 4.216, 0.091
+    _seed_couplings(m, vals, np.random.default_rng(seed))
+    return m, vals
+
+
 def small_bw(seed: int = 5) -> tuple:
     """Two Lambda* and two Breit-Wigner Pc (test size)."""
     names = ["1520", "1800"]
@@ -177,7 +197,7 @@ def small_bw(seed: int = 5) -> tuple:
 
 
 MODELS = {"lstar_only": lstar_only, "full_bw": full_bw, "kmatrix": kmatrix, "small_kmatrix": small_kmatrix,
-          "small_bw": small_bw}
+          "small_bw": small_bw, "small_zcs": small_zcs}
 
 # Workloads: model, data events, MC events, MC weight range.
 WORKLOADS = {

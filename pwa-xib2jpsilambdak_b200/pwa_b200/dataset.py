@@ -31,6 +31,8 @@ class Sample:
     sum_w_mc: float
     sum_w_data: float
     sum_w2_data: float
+    pp3: np.ndarray | None = None  # Zcs chain planes (models with NX > 0)
+    pp4: np.ndarray | None = None
 
     @property
     def nmc(self):
@@ -44,6 +46,9 @@ class Sample:
 
 def events_from_angles(ang: dict) -> tuple:
     bas = B.fill_basis(ang)
+    if "X_cosTheta_Lb" in ang:
+        bas.update(B.fill_basis_x(ang))
+        bas["mjpsik"] = np.asarray(ang["mjpsik"], np.float32)
     return np.asarray(ang["mLk"], np.float32), np.asarray(ang["mjpsiL"], np.float32), bas
 
 
@@ -70,7 +75,7 @@ def build_sample(data_ang: dict, mc_ang: dict, mc_w: np.ndarray, data_sw: np.nda
     mcw = np.asarray(mc_w, np.float32)
     return Sample(soa["pp"], soa["pp1"], soa["pp2"], sw, nd + nm, soa["n_size"], nd, int((band == 1).sum()),
                   int((band == 2).sum()), float(mcw.astype(np.float64).sum()), float(sw_d.astype(np.float64).sum()),
-                  float((sw_d.astype(np.float64) ** 2).sum()))
+                  float((sw_d.astype(np.float64) ** 2).sum()), soa.get("pp3"), soa.get("pp4"))
 
 
 def hit_or_miss(amp2: np.ndarray, rng, amp2_max: float | None = None) -> np.ndarray:
@@ -79,21 +84,21 @@ def hit_or_miss(amp2: np.ndarray, rng, amp2_max: float | None = None) -> np.ndar
     return rng.uniform(0, mx, amp2.shape[0]) < amp2
 
 
-def make_sample(n_data: int, n_mc: int, w_range: tuple, seed: int, amp2_of_angles) -> Sample:
+def make_sample(n_data: int, n_mc: int, w_range: tuple, seed: int, amp2_of_angles, zcs: bool = False) -> Sample:
     """Data by hit-or-miss from the model (amp2_of_angles: angle dict -> |A|^2 per event), MC flat
     with weights uniform in w_range."""
     rng = np.random.default_rng(seed + 7919)
     chunks, have = [], 0
     s = seed * 1000 + 1
     while have < n_data:
-        cand = K.flat_events(max(4 * (n_data - have), 2048), s)
+        cand = K.flat_events(max(4 * (n_data - have), 2048), s, zcs)
         s += 1
         a2 = amp2_of_angles(cand)
         ok = hit_or_miss(a2, rng, 1.05 * a2.max())
         chunks.append({k: v[ok] for k, v in cand.items()})
         have += int(ok.sum())
     data = {k: np.concatenate([c[k] for c in chunks])[:n_data] for k in chunks[0]}
-    mc = K.flat_events(n_mc, seed * 1000 + 999)
+    mc = K.flat_events(n_mc, seed * 1000 + 999, zcs)
     lo, hi = w_range
     mcw = rng.uniform(lo, hi, n_mc) if hi > lo else np.full(n_mc, lo)
     return build_sample(data, mc, mcw)

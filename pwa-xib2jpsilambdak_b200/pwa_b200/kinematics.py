@@ -190,6 +190,30 @@ def helicity_angles(ev: dict) -> dict:
     return out
 
 
-def flat_events(n: int, seed: int) -> dict:
-    """n flat phase-space events as the angle dictionary consumed by the basis builder."""
-    return helicity_angles(generate_phase_space(n, seed))
+def flat_events(n: int, seed: int, zcs: bool = False) -> dict:
+    """n flat phase-space events as the angle dictionary consumed by the basis builder.  zcs: also
+    the inputs of the Zcs -> J/psi K chain (zcs_angles)."""
+    ang = helicity_angles(generate_phase_space(n, seed))
+    if zcs:
+        ang.update(zcs_angles(ang, seed))
+    return ang
+
+
+def zcs_angles(ang: dict, seed: int) -> dict:
+    """Inputs of the Zcs -> J/psi K chain: m(J/psi K) from the Dalitz relation
+    m^2(J/psi K) = M^2(Lb) + m^2(p) + m^2(K) + m^2(J/psi) - m^2(Kp) - m^2(J/psi p), and the eight
+    Zcs-chain angles.  The reference reads those angles from its ntuples (X_cosTheta_Lb ...
+    X_alpha_Mu, RooDalitzAmplitude.cxx:278-295, 346-353) and its generator does not compute them
+    (gen_toys/phsp_toys/tree.C covers the Lambda* and Pc chains only), so they are drawn here,
+    seeded, flat in cos(theta) and phi; the amplitude path from them on is the reference's."""
+    rng = np.random.default_rng(seed * 7 + 424243)
+    n = len(ang["mLk"])
+    mkp = np.asarray(ang["mLk"], np.float64)
+    mjp = np.asarray(ang["mjpsiL"], np.float64)
+    m2 = M_LB ** 2 + M_P ** 2 + M_K ** 2 + M_JPSI ** 2 - mkp ** 2 - mjp ** 2
+    out = {"mjpsik": np.sqrt(np.maximum(m2, (M_JPSI + M_K) ** 2))}
+    for name in ("X_cosTheta_Lb", "X_cosTheta_X", "X_cosTheta_Jpsi", "X_cosTheta_p"):
+        out[name] = rng.uniform(-1.0, 1.0, n)
+    for name in ("X_phiX", "X_phiJpsi", "X_phiMu", "X_alpha_Mu"):
+        out[name] = rng.uniform(-np.pi, np.pi, n)
+    return out

@@ -165,8 +165,9 @@ def cg_evtgen(j1: int, j2: int, J: int, M: int, m1: int, m2: int) -> float:
 # ------------------------------------------------------------------ model description
 @dataclasses.dataclass
 class Resonance:
-    """One entry of a resonance list.  chain: 'L' (Lambda* -> pK), 'Z' (Pc -> J/psi p).
-    couplings: names of the LS coupling parameters as (Re, Im) pairs (12 for 'L', 8 for 'Z').
+    """One entry of a resonance list.  chain: 'L' (Lambda* -> pK), 'Z' (Pc -> J/psi p), 'X' (Zcs -> J/psi K).
+    couplings: names of the LS coupling parameters as (Re, Im) pairs (12 for 'L', 8 for 'Z'; for 'X'
+    four Lambda_b -> Zcs p couplings, then the Zcs -> J/psi K ones after the first).
     extra: 'L': (scRe, scIm) names; 'Z' K-matrix pole: g1..g4 names; 'Z' K-matrix NR: (fsc,).
     mass / width: parameter names or constants (for a K-matrix pole the width slot holds the
     channel index used for the near-threshold mass shift)."""
@@ -188,6 +189,7 @@ class Model:
     ffr: float = 3.0
     ffb: float = 3.0
     derived: dict = dataclasses.field(default_factory=dict)  # name -> callable(values) -> float
+    zcs: list = dataclasses.field(default_factory=list)
 
     @property
     def NR(self):
@@ -199,11 +201,11 @@ class Model:
 
     @property
     def NX(self):
-        return 0
+        return len(self.zcs)
 
     @property
     def resonances(self):
-        return list(self.lstar) + list(self.pc)
+        return list(self.lstar) + list(self.pc) + list(self.zcs)
 
     def value(self, vals: dict, ref) -> float:
         if isinstance(ref, (int, float)):
@@ -222,8 +224,13 @@ class Model:
 
 
 def orbital_l(r: Resonance) -> int:
-    """Decay orbital angular momentum stored in the table (setup_paraList :3079-3112)."""
+    """Decay orbital angular momentum stored in the table (setup_paraList :3079-3137)."""
     S = r.spin2 / 2.0
+    if r.chain == "X":
+        LR = max(abs(int(S - 1)), 0)  # C truncation: int(-1.0) = -1 for a spin-0 Zcs
+        if ((-1) ** LR) * r.parity < 0:
+            LR += 1
+        return LR
     if r.chain == "L":
         LR = int(S - 0.5)
     else:
@@ -308,6 +315,51 @@ def part_wave_pc(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: i
     return c * HB
 
 
+def part_wave_x(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: int) -> complex:
+    """Lambda_b -> Zcs p and Zcs -> J/psi K helicity coupling from LS couplings (PartWaveCoffX,
+    src/RooDalitzAmplitude.cxx:5724-5830; doubled quantum numbers, double arithmetic, EvtGen
+    Clebsch-Gordan coefficients).  As there, the first Zcs -> J/psi K wave has coupling 1 and a
+    decay coupling is only moved past when it is zero, so a non-zero one serves every later wave."""
+    HZ = 0j
+    ib = 4
+    SZ = 2
+    first = True
+    for LZ in range(J - SZ, SZ + J + 1, 2):
+        if J == 0 and LZ != SZ:
+            continue
+        if parity * (-1) ** (LZ // 2) < 0:
+            continue
+        tmp1 = (LZ + 1.0) / (J + 1.0)
+        cg2 = cg_evtgen(LZ, SZ, J, lamPsi, 0, lamPsi)
+        if first:
+            first = False
+            HZ += math.sqrt(tmp1) * cg2
+        else:
+            M = lsc[ib] if ib < len(lsc) else 0j
+            if abs(M) ** 2 < 1e-10:
+                ib += 1
+                continue
+            HZ += M * math.sqrt(tmp1) * cg2
+    ib = 0
+    c = 0j
+    m1 = lamZ - lamp
+    for S in (J - 1, J + 1):
+        if S < 0:
+            continue
+        for L in (S - 1, S + 1):
+            ccg1 = C2[(S - 1) // 2][(L - S + 1) // 2]
+            if m1 < 0 and L > S:
+                ccg1 = -ccg1
+            M = lsc[ib]
+            if abs(M) ** 2 < 1e-10:
+                ib += 1
+                continue
+            ccg = cg_evtgen(J, 1, S, m1, lamZ, -lamp)
+            c += math.sqrt((L + 1.0) / 2.0) * ccg * ccg1 * M
+            ib += 1
+    return c * HZ
+
+
 def _pow_m1(e) -> float:
     return 1.0 if int(round(e)) % 2 == 0 else -1.0
 
@@ -345,6 +397,21 @@ def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tu
            for i in range(len(r.couplings) // 2)]
     vamp: list = []
     km = None
+    if r.chain == "X":
+        S = r.spin2 / 2.0
+        for k in range(2):
+            for hpsi in (-1, 0, 1):
+                if abs(hpsi) > S:
+                    continue
+                for hp in (-0.5, 0.5):
+                    for helZ in (hp - 0.5, hp + 0.5):
+                        if abs(helZ) > S:
+                            continue
+                        a = part_wave_x(lsc, r.parity, r.spin2, int(helZ * 2), hpsi * 2, int(hp * 2))
+                        vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
+        if r.type != BREITWIGNER:
+            raise NotImplementedError(f"Zcs lineshape type {r.type}")
+        return q, vamp, km
     if r.chain == "L":
         S = f32(r.spin2) / f32(2)
         sc = complex(model.value(vals, r.extra[0]), model.value(vals, r.extra[1]))
@@ -406,18 +473,23 @@ def _assemble_block(model: Model, parts: list) -> ParamBlock:
             f[NKMC * i] = f[i]
         km += g + [f32(0)] * (NPMAX * NKMC - len(g)) + f
     data = np.concatenate([table.astype(f32), np.array(vamp, f32), np.array(km, f32)]).astype(f32)
-    return ParamBlock(data, len(table), len(vamp), 0, model.NR, model.NZ, 0, model.ffr, model.ffb)
+    return ParamBlock(data, len(table), len(vamp), 0, model.NR, model.NZ, model.NX, model.ffr, model.ffb)
 
 
 def build_param_block(model: Model, vals: dict, include: tuple | None = None) -> ParamBlock:
     """The float parameter block for one parameter point (ConfigureCouplings + cu_init_data).
-    include: optional (Lambda* indices, Pc indices) whose couplings are kept (SetupCoupling);
-    the others are zeroed, as for per-resonance weights."""
+    include: optional (Lambda* indices, Pc indices[, Zcs indices]) whose couplings are kept
+    (SetupCoupling); the others are zeroed, as for per-resonance weights."""
     parts = []
     for ir, r in enumerate(model.resonances):
         keep = True
         if include is not None:
-            keep = (ir in include[0]) if r.chain == "L" else ((ir - model.NR) in include[1])
+            if r.chain == "L":
+                keep = ir in include[0]
+            elif r.chain == "Z":
+                keep = (ir - model.NR) in include[1]
+            else:
+                keep = (ir - model.NR - model.NZ) in (include[2] if len(include) > 2 else ())
         parts.append(_resonance_parts(model, vals, ir, keep))
     return _assemble_block(model, parts)
 

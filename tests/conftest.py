@@ -41,7 +41,7 @@ def make_test_sample(model_name: str, n_data: int, n_mc: int, seed: int = 11, w_
         fx, _ = O.eval_fx(s, blk, -1, 0)
         return fx
 
-    smp = D.make_sample(n_data, n_mc, w_range, seed, amp2)
+    smp = D.make_sample(n_data, n_mc, w_range, seed, amp2, zcs=mdl.NX > 0)
     _samples[key] = (mdl, vals, blk, smp)
     return _samples[key]
 

@@ -11,11 +11,15 @@ from pwa_b200 import configs, model as M
 def test_block_layout(name):
     mdl, vals = configs.MODELS[name]()
     b = M.build_param_block(mdl, vals)
-    assert b.para_size == 6 * (mdl.NR + mdl.NZ)
+    assert b.para_size == 6 * (mdl.NR + mdl.NZ + mdl.NX)
     exp = sum(16 if r.spin2 == 1 else 24 for r in mdl.lstar)
     for r in mdl.pc:
         S = r.spin2 / 2
         exp += 2 * 2 * sum(1 for hpsi in (-1, 0, 1) for _ in range(2) for hp in (-0.5, 0.5) if abs(hpsi - hp) <= S)
+    for r in mdl.zcs:
+        S = r.spin2 / 2
+        exp += 2 * 2 * sum(1 for hpsi in (-1, 0, 1) if abs(hpsi) <= S for hp in (-0.5, 0.5)
+                           for hz in (hp - 0.5, hp + 0.5) if abs(hz) <= S)
     assert b.vamp_size == exp
     assert len(b.data) == b.para_size + b.vamp_size + M.KM_SIZE
     assert b.data.dtype == np.float32

@@ -23,9 +23,10 @@ def test_oracle_reproduces_golden(row, oracle_mod):
     assert abs(row["sumint_reference_fp32"] / s - 1) < 5e-5
 
 
-@pytest.mark.parametrize("name", ["small_kmatrix", "small_bw"])
+@pytest.mark.parametrize("name", ["small_kmatrix", "small_bw", "small_zcs"])
 def test_oracle_vs_reference_live(name, oracle_mod):
-    L = oracle_mod.ref_lib(*{"small_kmatrix": (3, 4), "small_bw": (2, 2)}[name], build_if_missing=True)
+    L = oracle_mod.ref_lib(*{"small_kmatrix": (3, 4, 0), "small_bw": (2, 2, 0), "small_zcs": (2, 1, 2)}[name],
+                           build_if_missing=True)
     if L is None:
         pytest.skip("reference host build unavailable")
     mdl, vals, blk, smp = make_test_sample(name, 600, 6000, seed=31)
