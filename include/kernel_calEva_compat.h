@@ -20,7 +20,8 @@ void cu_Free_pp(std::vector<float*> d_float_pp, std::vector<float*> d_float_pp1,
 
 /* One likelihood evaluation (kernel_calEva.cu:1186-1363).  Returns the MC normalisation sum and
  * writes the NLL to mynll.  NUMLz/NUMPc/NUMZcs are the model sizes (compile-time constants in the
- * reference, run-time here).  h_fx receives all per-event values when store_h_fx is true. */
+ * reference, run-time here); the Zcs planes d_float_pp3 / d_float_pp4 are read when NUMZcs > 0.
+ * h_fx receives all per-event values when store_h_fx is true. */
 double host_store_fx(std::vector<float*> d_float_pp, std::vector<float*> d_float_pp1,
                      std::vector<float*> d_float_pp2, std::vector<float*> d_float_pp3,
                      std::vector<float*> d_float_pp4, std::vector<float*> d_float_sw, float* h_paraList,

@@ -15,6 +15,9 @@
  *   pp1 :  96 planes  Pc angular factors (Re/Im interleaved)
  *   pp2 :  96 planes  Pc d-functions
  *   sw  :  n_size floats, data sWeights for events [0, nda)
+ *   pp3 :  97 planes  (models with Zcs entries) 0 m(J/psi K), 1..96 Zcs angular factors AX
+ *         (Re/Im interleaved, plane 1 + 2 (i*24 + j*12 + m))
+ *   pp4 :  96 planes  Zcs d-functions DX (plane s*24 + k*12 + m)
  * Events [0, nda) are data, sorted into m(J/psi p) bands; [nda, n) are MC.
  *
  * Parameter block ("h_paraList"): the reference's float layout (cu_init_data,
@@ -39,9 +42,9 @@ enum {
   PWA_E_ARG = 2,         /* null pointer or negative size */
   PWA_E_LAYOUT = 3,      /* parameter block sizes inconsistent with the resonance table */
   PWA_E_SIZE = 4,        /* a model size exceeds the compiled maximum */
-  PWA_E_UNSUPPORTED = 5, /* lineshape type or chain not built (spline, revised K-matrix, Zcs) */
+  PWA_E_UNSUPPORTED = 5, /* lineshape type not built (spline, revised K-matrix) */
   PWA_E_PARAM = 6,       /* invalid resonance parameters (spin, K-matrix channel) */
-  PWA_E_STATE = 7,       /* no events uploaded */
+  PWA_E_STATE = 7,       /* no events uploaded (or no Zcs planes for a model with Zcs entries) */
   PWA_E_NOMEM = 8        /* device allocation failed */
 };
 
@@ -71,6 +74,17 @@ int pwa_ctx_upload_events(pwa_ctx* ctx, const float* pp, const float* pp1, const
 int pwa_ctx_set_device_events(pwa_ctx* ctx, const float* d_pp, const float* d_pp1, const float* d_pp2,
                               const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
                               int64_t nda_fine);
+
+/* Zcs chain planes of the uploaded events (the reference's d_float_pp3 / d_float_pp4, filled from
+ * cu_Jpsihh_dlz's mjpsik, AXRe/AXIm and DX members, src/RooDalitzAmplitude.cxx:564-717), needed by
+ * models with Zcs entries (NX > 0).  Call after the event upload; the same n_size and event order
+ * (including the band order of an unsorted upload, applied here too).  A new event upload drops
+ * them. */
+#define PWA_PP3_PLANES 97
+#define PWA_PP4_PLANES 96
+int pwa_ctx_upload_zcs_events(pwa_ctx* ctx, const float* h_pp3, const float* h_pp4);
+/* Caller-owned device planes instead (not freed by the context); in the context's event order. */
+int pwa_ctx_set_device_zcs_events(pwa_ctx* ctx, const float* d_pp3, const float* d_pp4);
 
 /* Data in any order (gen_toys/rearrange_mJpsip/reOrder.C made the reference's inputs legal by sorting
  * them): the data columns [0, nda) are put into the three m(J/psi p) bands (30-offset, 150-offset,

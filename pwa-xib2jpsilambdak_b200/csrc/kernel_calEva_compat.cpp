@@ -20,6 +20,7 @@ namespace {
 struct Bound {
   pwa_ctx* ctx = nullptr;
   const float *pp = nullptr, *pp1 = nullptr, *pp2 = nullptr, *sw = nullptr;
+  const float *pp3 = nullptr, *pp4 = nullptr;
   long n = -1, nda = -1, smr = -1, fine = -1;
 };
 std::mutex g_mu;
@@ -53,6 +54,7 @@ Bound* bind(const float* pp, const float* pp1, const float* pp2, const float* sw
       b.pp = nullptr;
       return nullptr;
     }
+    b.pp3 = b.pp4 = nullptr;
     b.pp = pp;
     b.pp1 = pp1;
     b.pp2 = pp2;
@@ -64,6 +66,18 @@ Bound* bind(const float* pp, const float* pp1, const float* pp2, const float* sw
   }
   *rc = 0;
   return &b;
+}
+
+// Zcs planes (the reference's d_float_pp3 / d_float_pp4), attached when the model has Zcs entries.
+int bind_zcs(Bound* b, const std::vector<float*>& pp3, const std::vector<float*>& pp4, int NUMZcs) {
+  if (NUMZcs <= 0) return 0;
+  if (pp3.size() != 1 || pp4.size() != 1 || !pp3[0] || !pp4[0]) return PWA_E_ARG;
+  if (b->pp3 == pp3[0] && b->pp4 == pp4[0]) return 0;
+  const int rc = pwa_ctx_set_device_zcs_events(b->ctx, pp3[0], pp4[0]);
+  if (rc) return rc;
+  b->pp3 = pp3[0];
+  b->pp4 = pp4[0];
+  return 0;
 }
 
 }  // namespace
@@ -90,8 +104,8 @@ void cu_Free_pp(std::vector<float*> a, std::vector<float*> b, std::vector<float*
 }
 
 double host_store_fx(std::vector<float*> d_float_pp, std::vector<float*> d_float_pp1,
-                     std::vector<float*> d_float_pp2, std::vector<float*>, std::vector<float*>,
-                     std::vector<float*> d_float_sw, float* h_paraList, int para_size, int vamp_size,
+                     std::vector<float*> d_float_pp2, std::vector<float*> d_float_pp3,
+                     std::vector<float*> d_float_pp4, std::vector<float*> d_float_sw, float* h_paraList, int para_size, int vamp_size,
                      int paraSpline_size, double* h_fx, int end, int begin, int Nda, int Nda_SMR,
                      int Nda_SMR_finebinning, int NUMLz, int NUMPc, int NUMZcs, double& mynll, double SumW,
                      double sumW_data, float _FFR, float _FFB, bool store_h_fx) {
@@ -106,7 +120,8 @@ double host_store_fx(std::vector<float*> d_float_pp, std::vector<float*> d_float
   int rc = 0;
   Bound* b = bind(d_float_pp[0], d_float_pp1[0], d_float_pp2[0], d_float_sw[0], end, Nda, Nda_SMR,
                   Nda_SMR_finebinning, &rc);
-  if (!b) {
+  if (b) rc = bind_zcs(b, d_float_pp3, d_float_pp4, NUMZcs);
+  if (!b || rc) {
     report("host_store_fx", rc);
     mynll = nan;
     return nan;
@@ -129,7 +144,8 @@ void cuda_configure_ampcount(const float*, const int) {}
 void cuda_configure_smear() {}
 
 void host_store_amp2s(std::vector<float*> d_float_pp, std::vector<float*> d_float_pp1,
-                      std::vector<float*> d_float_pp2, std::vector<float*>, std::vector<float*>, float* h_paraList,
+                      std::vector<float*> d_float_pp2, std::vector<float*> d_float_pp3,
+                      std::vector<float*> d_float_pp4, float* h_paraList,
                       int para_size, int vamp_size, int paraSpline_size, double* h_amp2s, int end, int begin,
                       int NUMLz, int NUMPc, int NUMZcs, float _FFR, float _FFB) {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -143,6 +159,12 @@ void host_store_amp2s(std::vector<float*> d_float_pp, std::vector<float*> d_floa
     const long n_size = (end / 32 + 1) * 32;
     rc = pwa_ctx_set_device_events(ctx, d_float_pp[0], d_float_pp1[0], d_float_pp2[0], nullptr, end, n_size, 0, -1,
                                    0);
+  }
+  if (!rc && NUMZcs > 0) {
+    if (d_float_pp3.size() != 1 || d_float_pp4.size() != 1)
+      rc = PWA_E_ARG;
+    else
+      rc = pwa_ctx_set_device_zcs_events(ctx, d_float_pp3[0], d_float_pp4[0]);
   }
   if (!rc)
     rc = pwa_ctx_amp2(ctx, h_paraList, para_size, vamp_size, paraSpline_size, NUMLz, NUMPc, NUMZcs, _FFR, _FFB,

@@ -44,6 +44,8 @@ struct pwa_ctx {
   // events
   const float *pp = nullptr, *pp1 = nullptr, *pp2 = nullptr, *sw = nullptr;
   float *own_pp = nullptr, *own_pp1 = nullptr, *own_pp2 = nullptr, *own_sw = nullptr;
+  const float *pp3 = nullptr, *pp4 = nullptr;  // Zcs chain planes (models with Zcs entries)
+  float *own_pp3 = nullptr, *own_pp4 = nullptr;
   int64_t n = 0, n_size = 0, nda = 0, nda_smr = 0, nda_fine = 0;
   int32_t* d_lists = nullptr;
   std::vector<Segment> segs;
@@ -92,6 +94,10 @@ void free_events(pwa_ctx* c) {
   cudaFree(c->own_pp1);
   cudaFree(c->own_pp2);
   cudaFree(c->own_sw);
+  cudaFree(c->own_pp3);
+  cudaFree(c->own_pp4);
+  c->own_pp3 = c->own_pp4 = nullptr;
+  c->pp3 = c->pp4 = nullptr;
   cudaFree(c->d_lists);
   cudaFree(c->d_parts);
   cudaFree(c->d_defer);
@@ -177,7 +183,7 @@ const char* pwa_error_string(int code) {
     case PWA_E_SIZE: return "model size exceeds the compiled maximum";
     case PWA_E_UNSUPPORTED: return "lineshape type or decay chain not supported";
     case PWA_E_PARAM: return "invalid resonance parameters";
-    case PWA_E_STATE: return "no events uploaded";
+    case PWA_E_STATE: return "no events uploaded (or no Zcs planes for a model with Zcs entries)";
     case PWA_E_NOMEM: return "device allocation failed";
   }
   return "unknown error";
@@ -334,6 +340,60 @@ int pwa_ctx_set_device_events(pwa_ctx* c, const float* d_pp, const float* d_pp1,
   return build_segments(c, mz.data());
 }
 
+int pwa_ctx_upload_zcs_events(pwa_ctx* c, const float* pp3, const float* pp4) {
+  if (!c || !pp3 || !pp4) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  PWA_CUDA(cudaSetDevice(c->device));
+  cudaFree(c->own_pp3);
+  cudaFree(c->own_pp4);
+  c->own_pp3 = c->own_pp4 = nullptr;
+  c->pp3 = c->pp4 = nullptr;
+  const size_t ns = (size_t)c->n_size;
+  std::vector<float> a, b;
+  if (!c->order.empty()) {  // data uploaded unsorted: the same band order for the Zcs planes
+    auto permute = [&](const float* src, int planes, std::vector<float>& dst) {
+      dst.assign(src, src + (size_t)planes * ns);
+      for (int p = 0; p < planes; ++p)
+        for (size_t i = 0; i < c->order.size(); ++i) dst[(size_t)p * ns + i] = src[(size_t)p * ns + c->order[i]];
+    };
+    permute(pp3, PWA_PP3_PLANES, a);
+    permute(pp4, PWA_PP4_PLANES, b);
+    pp3 = a.data();
+    pp4 = b.data();
+  }
+  PWA_CUDA(cudaMalloc(&c->own_pp3, PWA_PP3_PLANES * ns * sizeof(float)));
+  PWA_CUDA(cudaMalloc(&c->own_pp4, PWA_PP4_PLANES * ns * sizeof(float)));
+  PWA_CUDA(cudaMemcpy(c->own_pp3, pp3, PWA_PP3_PLANES * ns * sizeof(float), cudaMemcpyHostToDevice));
+  PWA_CUDA(cudaMemcpy(c->own_pp4, pp4, PWA_PP4_PLANES * ns * sizeof(float), cudaMemcpyHostToDevice));
+  c->pp3 = c->own_pp3;
+  c->pp4 = c->own_pp4;
+  return PWA_OK;
+}
+
+int pwa_ctx_set_device_zcs_events(pwa_ctx* c, const float* d_pp3, const float* d_pp4) {
+  if (!c || !d_pp3 || !d_pp4) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  PWA_CUDA(cudaSetDevice(c->device));
+  cudaFree(c->own_pp3);
+  cudaFree(c->own_pp4);
+  c->own_pp3 = c->own_pp4 = nullptr;
+  c->pp3 = d_pp3;
+  c->pp4 = d_pp4;
+  return PWA_OK;
+}
+
+// The event set of an evaluation: the Zcs planes go with it only for a model with Zcs entries
+// (they select the kernels with the Zcs terms).
+static int event_set(const pwa_ctx* c, int NX, EventSet* ev) {
+  *ev = EventSet{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  if (NX > 0) {
+    if (!c->pp3 || !c->pp4) return PWA_E_STATE;
+    ev->pp3 = c->pp3;
+    ev->pp4 = c->pp4;
+  }
+  return PWA_OK;
+}
+
 // Copies the decoded point table to the device and, with tables on, builds the lineshape tables
 // for it on the context's stream.
 static int upload_point(pwa_ctx* c, int* launches) {
@@ -364,7 +424,8 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
     PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
     c->fx_cap = c->n;
   }
-  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  EventSet ev;
+  if ((rc = event_set(c, NX, &ev))) return rc;
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
@@ -443,7 +504,8 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   std::vector<int> sidx, fidx;
   int ntab = 0;
   for (int p = 0; p < npoints; ++p) {
-    bool ok = classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
+    // the structured kernels carry no Zcs terms: models with Zcs entries take the single-point path
+    bool ok = NX == 0 && classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
     if (ok && bp[p].kind == BP_PCG && c->use_tables) ok = ntab++ < BATCH_MAX_TABLES;
     (ok ? sidx : fidx).push_back(p);
   }
@@ -471,11 +533,12 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     PWA_CUDA(cudaMalloc(&t, TAB_BYTES));
     c->bt_tabs.push_back(t);
   }
-  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  int launches = 0, rc = 0;
+  EventSet ev;
+  if ((rc = event_set(c, NX, &ev))) return rc;
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   // centre: the context's table and lineshape tables
   *c->h_table = H[0];
-  int launches = 0, rc = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const PointTable& T0 = *c->h_table;
   const BatchGroupMap gm = batch_group_map(T0);
@@ -572,7 +635,8 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
     PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
     c->fx_cap = c->n;
   }
-  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  EventSet ev;
+  if ((rc = event_set(c, NX, &ev))) return rc;
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const bool defer = c->h_table->tab.enabled != 0;
@@ -599,7 +663,8 @@ int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_siz
     PWA_CUDA(cudaMalloc(&c->d_fx, std::max<int64_t>(c->n, 1) * sizeof(double)));
     c->fx_cap = c->n;
   }
-  EventSet ev{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  EventSet ev;
+  if ((rc = event_set(c, NX, &ev))) return rc;
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const bool defer = c->h_table->tab.enabled != 0;

@@ -115,6 +115,39 @@ __host__ __device__ inline cplx pc_bw(const PcEntry& Z, const PcKin& k) {
   return mk(de2 * f, gm * f);
 }
 
+// Zcs -> J/psi K lineshapes at m(J/psi K): Breit-Wigner (BW_AMPX, cu_DPFPropogator.cu:226-246) times
+// the Lambda_b -> Zcs p barrier (BTermX, :205-217).
+struct XKin {
+  double inv_m, s, pR, pBm;
+  double rsR[6], rsB[6];
+};
+
+__host__ __device__ inline XKin x_kin(const PointTable& T, double mjk) {
+  XKin k;
+  k.inv_m = 1.0 / mjk;
+  k.s = mjk * mjk;
+  k.pR = two_body_p(mjk, M_K, M_JPSI);
+  const double pB = two_body_p(M_LB, M_P, mjk);
+  k.pBm = pB / M_LB;
+  fill_rs(k.rsR, T.lmask_x_R, T.ffr, k.pR);
+  fill_rs(k.rsB, T.lmask_x_B, T.ffb, pB);
+  return k;
+}
+
+__host__ __device__ inline cplx x_lineshape(const XEntry& X, const XKin& k) {
+  double FR = 1.0, gamma = X.g_r, ratio = 1.0;
+  if (X.bw_above) {
+    FR = X.sqrt_polyR0 * k.rsR[X.LR];
+    ratio = k.pR * X.inv_pR0;
+    gamma = X.g_r * ipow(ratio, 2 * X.LR + 1) * (X.m_r * k.inv_m) * FR * FR;
+  }
+  const double factor = FR * ipow(ratio, X.LR) * X.norm;
+  const double de2 = X.m_r * X.m_r - k.s, gm = gamma * X.m_r;
+  const double f = factor / (de2 * de2 + gm * gm);
+  const double FB = (X.lb_mode != 0 || X.LB == 0) ? 1.0 : X.sqrt_polyB0 * k.rsB[X.LB];
+  return mk(de2 * f, gm * f) * (FB * ipow(k.pBm, X.LB));
+}
+
 // One J^P group of the coupled-channel K-matrix at mass mz (Default_KMatrix,
 // cu_DPFPropogator.cu:588-813): P-vector outputs, npole poles first then 4 production terms.
 __host__ __device__ inline void km_solve(const KmGroup& G, double mz, double ffb, cplx* out) {
@@ -298,6 +331,41 @@ struct Ev {
 };
 
 __device__ __forceinline__ bool nonzero(cplx c) { return c.re != 0.0 || c.im != 0.0; }
+
+// Zcs planes of one event: pp3 plane 0 m(J/psi K), planes 1 + 2 (i*24 + j*12 + m) (+1) the angular
+// factors AX; pp4 plane s*24 + k*12 + m the d-functions DX (GetAmpZcs, kernel_calEva.cu:192-286).
+struct EvX {
+  const float *pp3, *pp4;
+  int64_t ns, e;
+  __device__ __forceinline__ double mjk() const { return ldf(pp3, e); }
+  __device__ __forceinline__ cplx AX(int i, int j, int m) const {
+    const int a = 1 + (i * 24 + j * 12 + m) * 2;
+    return mk(ldf(pp3, e + a * ns), ldf(pp3, e + (a + 1) * ns));
+  }
+  __device__ __forceinline__ double DX(int s, int k, int m) const { return ldf(pp4, e + (s * 24 + k * 12 + m) * ns); }
+};
+
+// Zcs chain amplitudes of proton helicity k for the helicities (i, j) in ij_lo .. ij_hi - 1
+// (ij = 2 i + j), added to H[ij - ij_lo]: sum_x lineshape_x sum_m c_{x,k,m} DX AX.
+template <int NIJ>
+__device__ __forceinline__ void zcs_amplitudes(const PointTable& T, const EvX& X, int k, int ij_lo, cplx* H) {
+  const XKin xk = x_kin(T, X.mjk());
+  for (int x = 0; x < T.NX; ++x) {
+    const XEntry& Xe = T.X[x];
+    const cplx bw = x_lineshape(Xe, xk);
+#pragma unroll 1
+    for (int m = 0; m < 12; ++m) {
+      const cplx c = Xe.c[k * 12 + m];
+      if (!nonzero(c)) continue;
+      const cplx D = (bw * c) * X.DX(Xe.sidx, k, m);
+#pragma unroll
+      for (int q = 0; q < NIJ; ++q) {
+        const int ij = ij_lo + q;
+        cmac(H[q], X.AX(ij >> 1, ij & 1, m), D);
+      }
+    }
+  }
+}
 
 __device__ __forceinline__ cplx shfl_xor(cplx v, int o) {
   return mk(__shfl_xor_sync(0xffffffffu, v.re, o), __shfl_xor_sync(0xffffffffu, v.im, o));

@@ -35,7 +35,7 @@ namespace pwa {
 // masses exactly (out of line); it runs over the deferred list (events [0, *n_list) of list) or,
 // without tables, over the whole segment.  Keeping the exact path out of the main kernel keeps its
 // register allocation free of the call's save/restore.
-template <bool FIX>
+template <bool FIX, bool ZCS>
 __global__ void __launch_bounds__(EV_THREADS, 2)
     k_unsmeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
                 const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int mode, int32_t* defer,
@@ -87,6 +87,19 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
 #pragma unroll
       for (int ij = 0; ij < 4; ++ij) cmac(H[ij], E.A(ij >> 1, ij & 1, m), F[m]);
     }
+    // Zcs (GetAmpZcs): joins the Lambda* amplitudes; separate in the non-interference sum
+    double vn = 0;
+    if (ZCS) {
+      cplx HX[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) HX[q] = mk(0, 0);
+      zcs_amplitudes<4>(T, EvX{ev.pp3, ev.pp4, ev.n_size, E.e}, k, 0, HX);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        vn += norm2(H[q]) + norm2(HX[q]);
+        H[q] += HX[q];
+      }
+    }
     // Pc
     bool deferred = false;
     if (T.NZ > 0) {
@@ -120,11 +133,11 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
         }
       }
     }
-    double v = 0, vn = 0;
+    double v = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       v += norm2(H[q] + HZ[q]);
-      vn += norm2(H[q]) + norm2(HZ[q]);
+      vn += ZCS ? norm2(HZ[q]) : norm2(H[q]) + norm2(HZ[q]);
     }
     v += __shfl_xor_sync(0xffffffffu, v, 16);
     vn += __shfl_xor_sync(0xffffffffu, vn, 16);
@@ -172,7 +185,7 @@ constexpr size_t SMEARED_SMEM = align16(sizeof(PointTable)) + EV_WARPS * sizeof(
 //
 // FIX as for k_unsmeared: the main launch defers every event with a resolution offset the table
 // cannot serve.
-template <int NB, bool FIX>
+template <int NB, bool FIX, bool ZCS>
 __global__ void __launch_bounds__(EV_THREADS, 2)
     k_smeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
               const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band, int32_t* defer,
@@ -215,6 +228,14 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
       }
       cmac(hl, W.q[ei][r], f);
     }
+    // Zcs joins H_L (H_L_Zcs of TemplateGetAmp2s); |A|^2 without interference keeps it separate
+    double vlx = norm2(hl);
+    if (ZCS) {
+      cplx hx = mk(0, 0);
+      zcs_amplitudes<1>(T, EvX{ev.pp3, ev.pp4, ev.n_size, E.e}, hk, 2 * hi + hj, &hx);
+      vlx += norm2(hx);
+      hl += hx;
+    }
     cplx hz[MAX_PC];
 #pragma unroll
     for (int q = 0; q < MAX_PC; ++q) hz[q] = mk(0, 0);
@@ -256,7 +277,7 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
           cmac(s, r[q], hz[q]);
         }
         if (l0 + bb < shift) {
-          vn = norm2(hl) + norm2(s);
+          vn = vlx + norm2(s);
         } else {
           a1 += s;
           a2 += norm2(s);
@@ -493,28 +514,42 @@ int segment_parts(const Segment& s, int sm_count, bool deferred) {
   return segment_blocks(s, sm_count) + (deferred ? fix_blocks(s, sm_count) : 0);
 }
 
+template <bool FIX, bool ZCS>
+static void launch_kind_t(const EventSet& ev, int kind, int64_t begin, int64_t end, const int32_t* list,
+                          const int* n_list, const PointTable* d_table, Partial* out, double* fx_out, int mode,
+                          int32_t* defer, int* defer_count, int nb, cudaStream_t st) {
+  switch (kind) {
+    case SMEAR_NONE:
+      k_unsmeared<FIX, ZCS><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
+                                                                     fx_out, mode, defer, defer_count);
+      break;
+    case SMEAR_20:
+      k_smeared<20, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
+                                                                     fx_out, 0, defer, defer_count);
+      break;
+    case SMEAR_30:
+      k_smeared<30, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
+                                                                     fx_out, 1, defer, defer_count);
+      break;
+    case SMEAR_150:
+      k_smeared<150, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
+                                                                      fx_out, 1, defer, defer_count);
+      break;
+  }
+}
+
+// The Zcs variants run when the event set carries the Zcs planes (the caller passes them only for a
+// model with Zcs entries).
 template <bool FIX>
 static void launch_kind(const EventSet& ev, int kind, int64_t begin, int64_t end, const int32_t* list,
                         const int* n_list, const PointTable* d_table, Partial* out, double* fx_out, int mode,
                         int32_t* defer, int* defer_count, int nb, cudaStream_t st) {
-  switch (kind) {
-    case SMEAR_NONE:
-      k_unsmeared<FIX><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out,
-                                                                mode, defer, defer_count);
-      break;
-    case SMEAR_20:
-      k_smeared<20, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 0,
-                                                                defer, defer_count);
-      break;
-    case SMEAR_30:
-      k_smeared<30, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 1,
-                                                                defer, defer_count);
-      break;
-    case SMEAR_150:
-      k_smeared<150, FIX><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out, fx_out, 1,
-                                                                 defer, defer_count);
-      break;
-  }
+  if (ev.pp3)
+    launch_kind_t<FIX, true>(ev, kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count, nb,
+                             st);
+  else
+    launch_kind_t<FIX, false>(ev, kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count, nb,
+                              st);
 }
 
 // One segment: with a deferral buffer (tables on), the table-only pass over the segment and then the
@@ -552,17 +587,25 @@ static cudaError_t configure_one(K kernel, size_t smem, int* occ) {
   return cudaSuccess;
 }
 
-cudaError_t configure_kernels() {
+template <bool ZCS>
+static cudaError_t configure_variant(int* occ) {
   cudaError_t e;
   int unused = 0;
-  if ((e = configure_one(k_unsmeared<false>, UNSMEARED_SMEM, &g_occ[SMEAR_NONE]))) return e;
-  if ((e = configure_one(k_unsmeared<true>, UNSMEARED_SMEM, &unused))) return e;
-  if ((e = configure_one(k_smeared<20, false>, SMEARED_SMEM, &g_occ[SMEAR_20]))) return e;
-  if ((e = configure_one(k_smeared<30, false>, SMEARED_SMEM, &g_occ[SMEAR_30]))) return e;
-  if ((e = configure_one(k_smeared<150, false>, SMEARED_SMEM, &g_occ[SMEAR_150]))) return e;
-  if ((e = configure_one(k_smeared<20, true>, SMEARED_SMEM, &unused))) return e;
-  if ((e = configure_one(k_smeared<30, true>, SMEARED_SMEM, &unused))) return e;
-  if ((e = configure_one(k_smeared<150, true>, SMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_unsmeared<false, ZCS>, UNSMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_NONE]))) return e;
+  if ((e = configure_one(k_unsmeared<true, ZCS>, UNSMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<20, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_20]))) return e;
+  if ((e = configure_one(k_smeared<30, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_30]))) return e;
+  if ((e = configure_one(k_smeared<150, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_150]))) return e;
+  if ((e = configure_one(k_smeared<20, true, ZCS>, SMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<30, true, ZCS>, SMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_smeared<150, true, ZCS>, SMEARED_SMEM, &unused))) return e;
+  return cudaSuccess;
+}
+
+cudaError_t configure_kernels() {
+  cudaError_t e;
+  if ((e = configure_variant<false>(g_occ))) return e;
+  if ((e = configure_variant<true>(g_occ))) return e;
   return configure_batch_kernels();
 }
 
@@ -642,17 +685,19 @@ static const std::vector<double>& complex_branch_masses() {
   return out;
 }
 
+static bool nonzero_host(cplx c) { return c.re != 0.0 || c.im != 0.0; }
+
 // Decodes the float parameter block (layout of cu_init_data, RooDalitzAmplitude.cxx:3141-3210;
 // coupling offsets of cuda_configure_ampcount, kernel_calEva.cu:1014-1098; K-matrix output slots
 // of cuda_configure_Pc_KMatrix, :978-1010) and hoists every parameter-only constant.
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                       float ffr, float ffb, PointTable* T) {
   std::memset(T, 0, sizeof(PointTable));
-  if (NX != 0) return 5;                       // PWA_E_UNSUPPORTED: Zcs chain
-  if (NR > MAX_LSTAR || NZ > MAX_PC || NR < 0 || NZ < 0) return 4;  // PWA_E_SIZE
-  if (para_size != NSET * (NR + NZ + NX)) return 3;                 // PWA_E_LAYOUT
+  if (NR > MAX_LSTAR || NZ > MAX_PC || NX > MAX_ZCS || NR < 0 || NZ < 0 || NX < 0) return 4;  // PWA_E_SIZE
+  if (para_size != NSET * (NR + NZ + NX)) return 3;                                           // PWA_E_LAYOUT
   T->NR = NR;
   T->NZ = NZ;
+  T->NX = NX;
   T->ffr = ffr;
   T->ffb = ffb;
   const double mmin = M_K + M_P, mmax = M_LB - M_JPSI;
@@ -786,6 +831,69 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
             ++m;
           }
     }
+  }
+  // Zcs entries (GetAmpZcs, kernel_calEva.cu:192-286; BTermX / BW_AMPX, cu_DPFPropogator.cu:205-246).
+  // The kernel uses a Breit-Wigner whatever the type field says.
+  const double thr_xk = (double)(float)(M_K + M_JPSI);
+  for (int x = 0; x < NX; ++x) {
+    const float* q = pl + (NR + NZ + x) * NSET;
+    XEntry& X = T->X[x];
+    const int S2 = (int)q[2];
+    if (S2 < 0 || S2 > 6 || (S2 % 2) != 0) return 6;
+    X.m_r = q[0];
+    X.g_r = q[1];
+    X.LR = (int)q[3];
+    if (X.LR < 0 || X.LR > 5) return 5;
+    X.sidx = S2 / 2;
+    const double S = 0.5 * S2;
+    X.bw_above = X.m_r > thr_xk;
+    const double pR0 = X.bw_above ? two_body_p(X.m_r, M_K, M_JPSI) : 0.0;
+    X.norm = bw_norm(X.m_r, X.g_r);
+    X.inv_pR0 = (pR0 != 0) ? 1.0 / pR0 : 0.0;
+    X.sqrt_polyR0 = std::sqrt(bw_poly(X.LR, sq(T->ffr * pR0)));
+    if (X.bw_above && X.LR >= 1) T->lmask_x_R |= 1 << X.LR;
+    X.LB = (int)(S - 0.5);  // C truncation toward zero
+    if (X.LB > 5) return 5;
+    if (X.m_r < 0) {
+      X.lb_mode = 2;
+    } else if (X.m_r > 1e-10 && X.m_r + M_P < M_LB) {
+      X.lb_mode = 0;
+      X.sqrt_polyB0 = std::sqrt(bw_poly(X.LB, sq(T->ffb * two_body_p(M_LB, M_P, X.m_r))));
+      if (X.LB >= 1) T->lmask_x_B |= 1 << X.LB;
+    } else {
+      X.lb_mode = 1;
+    }
+    // the kernel reads N(J) consecutive couplings per proton helicity from the resonance's offset
+    // (lambda_p in {0, 1}, lambda_Zcs = lambda_p -+ 1/2); the block holds ConfigureCouplings' count
+    // (lambda_p = -+1/2)
+    const int base = cnt;
+    int rd = base;
+    for (int k = 0; k < 2; ++k) {
+      int m = 0;
+      for (int hpsi = -1; hpsi <= 1; ++hpsi) {
+        if (std::abs(hpsi) > S) continue;
+        for (int hp = 0; hp <= 1; ++hp)
+          for (int iz = 0; iz < 2; ++iz) {
+            if (std::fabs(hp - 0.5 + iz) > S) continue;
+            X.c[k * 12 + m] = coupling(rd);
+            rd += 2;
+            ++m;
+          }
+      }
+    }
+    for (int k = 0; k < 2; ++k)
+      for (int hpsi = -1; hpsi <= 1; ++hpsi) {
+        if (std::abs(hpsi) > S) continue;
+        for (int ihp = 0; ihp < 2; ++ihp)
+          for (int ihz = 0; ihz < 2; ++ihz) {
+            const double hz = (ihp ? 0.5 : -0.5) + (ihz ? 0.5 : -0.5);
+            if (!(std::fabs(hz) > S)) cnt += 2;
+          }
+      }
+    if (rd > cnt) return 3;
+    for (int k = 0; k < 2; ++k)
+      for (int m = 0; m < 12; ++m)
+        if (nonzero_host(X.c[k * 12 + m])) T->x_mmask[k] |= 1 << m;
   }
   if (cnt != para_size + vamp_size) return 3;
   // K-matrix groups (Default_KMatrix pole scan and near-threshold mass shift, :674-746)

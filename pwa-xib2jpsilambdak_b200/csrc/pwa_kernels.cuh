@@ -35,6 +35,10 @@ struct EventSet {
   int64_t n_size;   // plane stride
   int64_t n;        // events
   int64_t nda;      // events [0, nda) are data (NLL term), the rest MC (normalisation)
+  // Zcs chain planes (needed when the model has Zcs entries): pp3 97 planes (m(J/psi K), AX Re/Im),
+  // pp4 96 planes (DX)
+  const float* pp3 = nullptr;
+  const float* pp4 = nullptr;
 };
 
 enum Smear : int { SMEAR_NONE = 0, SMEAR_20 = 1, SMEAR_30 = 2, SMEAR_150 = 3 };

@@ -128,6 +128,7 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
   if (n < 0 || nda < 0 || nda > n || n_size < n) return PWA_E_ARG;
   if (n > kMaxEvents) return PWA_E_SIZE;  // PWA_NOALLOC_MAX_EVENTS
   if (spline_size != 0) return PWA_E_UNSUPPORTED;
+  if (NX != 0) return PWA_E_UNSUPPORTED;  // no Zcs planes among this entry point's arguments
   std::lock_guard<std::mutex> lock(g_mu);
   thread_local PointTable table;
   int rc = build_point_table(h_paraList, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, &table);

@@ -11,6 +11,7 @@ namespace pwa {
 
 constexpr int MAX_LSTAR = 24;
 constexpr int MAX_PC = 16;
+constexpr int MAX_ZCS = 4;
 constexpr int MAX_GROUPS = MAX_PC + 4;  // K-matrix J^P groups + one group per non-K-matrix Pc entry
 constexpr int NSET = 6;
 
@@ -42,6 +43,20 @@ struct PcEntry {
   double pB0, polyB0;
   double inv_pR0, sqrt_polyR0, sqrt_polyB0;
   cplx c[24];  // c[k*12+m], 12 helicity slots per proton helicity (disallowed slots are 0)
+};
+
+// Zcs -> J/psi K entry (Breit-Wigner BW_AMPX with production barrier BTermX,
+// cu_DPFPropogator.cu:205-246).  Couplings in the order GetAmpZcs (kernel_calEva.cu:192-286) reads
+// them: per proton helicity k, N(J) consecutive (Re, Im) pairs from the resonance's coupling offset
+// (N = 0, 9, 12, 12 for 2J = 0, 2, 4, 6), slot m of c[k*12+m] selecting the AX / DX planes.
+struct XEntry {
+  int sidx;      // DX spin index 2J / 2
+  int LR, LB;
+  int bw_above;  // Breit-Wigner mass above the J/psi K threshold
+  int lb_mode;   // production barrier: 0 F ratio with pB0(m_r), 1 ratio 1 (pB0 = event's), 2 no ratio
+  int pad;
+  double m_r, g_r, norm, inv_pR0, sqrt_polyR0, sqrt_polyB0;
+  cplx c[24];
 };
 
 struct KmGroup {
@@ -107,6 +122,9 @@ constexpr size_t TAB_BYTES =
 struct alignas(16) PointTable {
   int NR, NZ, ngroups;
   int status;  // 0 ok, else a PWA_E_* code
+  int NX;      // Zcs entries
+  int lmask_x_R, lmask_x_B;  // Blatt-Weisskopf orders of the Zcs decay and production barriers
+  int x_mmask[2];            // Zcs helicity slots with a non-zero coupling, per proton helicity
   // Blatt-Weisskopf orders L in use (bit L set): decay barriers of the Lambda* Breit-Wigners, their
   // production barriers, production barriers of the Pc entries, decay barriers of Pc Breit-Wigners;
   // needs_sigma_pi: a Lambda* below the pK threshold uses the Sigma pi channel momentum.
@@ -116,6 +134,7 @@ struct alignas(16) PointTable {
   double ffr, ffb;
   LstarEntry L[MAX_LSTAR];
   PcEntry Z[MAX_PC];
+  XEntry X[MAX_ZCS];
   KmGroup G[4];
   PcGroup grp[MAX_GROUPS];
   int order[MAX_PC];  // Pc entries in group order

@@ -16,6 +16,7 @@ import os
 LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
+            "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
@@ -65,6 +66,8 @@ def load() -> C.CDLL:
         L.pwa_ctx_amp2.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_float, C.c_float, _dp]
         L.pwa_ctx_upload_events_unsorted.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp] + [C.c_int64] * 3
+        L.pwa_ctx_upload_zcs_events.argtypes = [C.c_void_p, _fp, _fp]
+        L.pwa_ctx_set_device_zcs_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.pwa_band_order.argtypes = [_fp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int64)]
         L.pwa_ctx_mc_integral.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -143,8 +146,17 @@ class Context:
         sw = np.ascontiguousarray(sample.sw, np.float32)
         check(self.L.pwa_ctx_upload_events(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n, sample.n_size,
                                            sample.nda, a, b), "pwa_ctx_upload_events")
+        self._upload_zcs(sample)
         self.sample = sample
         self.n = sample.n
+
+    def _upload_zcs(self, sample):
+        """Zcs chain planes of a sample that has them (pwa_ctx_upload_zcs_events)."""
+        if getattr(sample, "pp3", None) is None:
+            return
+        pp3 = np.ascontiguousarray(sample.pp3, np.float32)
+        pp4 = np.ascontiguousarray(sample.pp4, np.float32)
+        check(self.L.pwa_ctx_upload_zcs_events(self.h, _f(pp3), _f(pp4)), "pwa_ctx_upload_zcs_events")
 
     def upload_unsorted(self, sample):
         """Upload a Sample whose data events are in any order (pwa_ctx_upload_events_unsorted): the
@@ -155,6 +167,7 @@ class Context:
         sw = np.ascontiguousarray(sample.sw, np.float32)
         check(self.L.pwa_ctx_upload_events_unsorted(self.h, _f(pp), _f(pp1), _f(pp2), _f(sw), sample.n,
                                                     sample.n_size, sample.nda), "pwa_ctx_upload_events_unsorted")
+        self._upload_zcs(sample)
         self.sample = sample
         self.n = sample.n
 

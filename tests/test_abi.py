@@ -71,8 +71,17 @@ def test_error_codes():
     pl = np.ascontiguousarray(b.data)
     args = (b.para_size, b.vamp_size, 0, b.NR, b.NZ)
     f = lib._f(pl)
+    bad = pl.copy()
+    bad[4] = 360  # revised K-matrix Lambda* lineshape: not built
+    assert L.pwa_host_lineshapes(lib._f(bad), *args, 0, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
+                                 d.ctypes.data_as(dp)) == 5
     assert L.pwa_host_lineshapes(f, *args, 1, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
-                                 d.ctypes.data_as(dp)) == 5  # Zcs chain not built
+                                 d.ctypes.data_as(dp)) == 3  # a Zcs entry without its table row
+    mz_, vz = configs.small_zcs()
+    bz = M.build_param_block(mz_, vz)
+    pz = np.ascontiguousarray(bz.data)
+    assert L.pwa_host_lineshapes(lib._f(pz), bz.para_size, bz.vamp_size, 0, bz.NR, bz.NZ, bz.NX, bz.ffr, bz.ffb,
+                                 1.5, 4.4, d.ctypes.data_as(dp), d.ctypes.data_as(dp)) == 0
     assert L.pwa_host_lineshapes(f, b.para_size + 6, b.vamp_size, 0, b.NR, b.NZ, 0, b.ffr, b.ffb, 1.5, 4.4,
                                  d.ctypes.data_as(dp), d.ctypes.data_as(dp)) == 3  # layout
     assert L.pwa_host_lineshapes(f, b.para_size, b.vamp_size - 2, 0, b.NR, b.NZ, 0, b.ffr, b.ffb, 1.5, 4.4,

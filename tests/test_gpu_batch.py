@@ -92,3 +92,10 @@ def test_batch_repeated_and_chunked(ctx):
     assert [a.nll for a in r1] == [b.nll for b in r2]
     for i in (0, 1, 200, 399, 400):
         assert abs(r1[i].nll - ctx.eval_nll(blocks[i]).nll) < NLL_TOL
+
+
+def test_gradient_batch_with_zcs_entries(ctx):
+    """A model with Zcs entries: the batch call evaluates every point through the single-point path
+    (the structured kernels carry no Zcs terms) and matches one-by-one calls."""
+    labels, blocks, res, nstruct, smp = _check_batch(ctx, "small_zcs", 1500, 15000)
+    assert nstruct == 0

@@ -11,7 +11,7 @@ NLL_TOL = 1e-6
 FX_RTOL = 1e-9
 
 CASES = [("small_kmatrix", 1500, 15000), ("small_bw", 1500, 15000), ("lstar_only", 1000, 10000),
-         ("kmatrix", 1200, 12000), ("full_bw", 800, 8000)]
+         ("kmatrix", 1200, 12000), ("full_bw", 800, 8000), ("small_zcs", 1500, 15000)]
 
 
 @pytest.fixture(scope="module")
@@ -35,8 +35,9 @@ def test_nll_and_fx_match_oracle(ctx, oracle_mod, name, nd, nm):
     assert r.n_nonpos == 0
 
 
-def test_amp2_matches_oracle(ctx, oracle_mod):
-    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+@pytest.mark.parametrize("name", ["small_kmatrix", "small_zcs"])
+def test_amp2_matches_oracle(ctx, oracle_mod, name):
+    mdl, vals, blk, smp = make_test_sample(name, 1500, 15000)
     ctx.upload(smp)
     a = ctx.amp2(blk)
     o = oracle_mod.amp2(smp, blk)
@@ -79,11 +80,12 @@ def test_lineshape_tables_match_exact_solves(ctx, oracle_mod):
     assert abs(r1.nll - v) < NLL_TOL
 
 
-def test_unsorted_upload_matches_sorted(ctx):
+@pytest.mark.parametrize("name", ["small_kmatrix", "small_zcs"])
+def test_unsorted_upload_matches_sorted(ctx, name):
     """Data in shuffled order through pwa_ctx_upload_events_unsorted: same NLL as the band-sorted
-    upload, per-event fx returned in the caller's order."""
+    upload, per-event fx returned in the caller's order (Zcs planes permuted alike)."""
     import copy
-    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    mdl, vals, blk, smp = make_test_sample(name, 1500, 15000)
     ctx.upload(smp)
     r0, fx0 = ctx.eval_nll(blk, want_fx=True)
     rng = np.random.default_rng(4)
@@ -95,10 +97,12 @@ def test_unsorted_upload_matches_sorted(ctx):
     perm = np.concatenate([perm[(perm != last1) & (perm != last2)], [last1, last2]])
     sh = copy.copy(smp)
     ns = smp.n_size
-    for name, planes in (("pp", 111), ("pp1", 96), ("pp2", 96)):
-        a = np.array(getattr(smp, name), np.float32).reshape(planes, ns).copy()
+    for plane, planes in (("pp", 111), ("pp1", 96), ("pp2", 96), ("pp3", 97), ("pp4", 96)):
+        if getattr(smp, plane, None) is None:
+            continue
+        a = np.array(getattr(smp, plane), np.float32).reshape(planes, ns).copy()
         a[:, :smp.nda] = a[:, perm]
-        setattr(sh, name, a.reshape(-1))
+        setattr(sh, plane, a.reshape(-1))
     sw = np.array(smp.sw, np.float32).copy()
     sw[:smp.nda] = sw[perm]
     sh.sw = sw
@@ -107,4 +111,29 @@ def test_unsorted_upload_matches_sorted(ctx):
     assert abs(r1.nll - r0.nll) < NLL_TOL
     assert np.array_equal(fx1[:smp.nda], fx0[perm])
     assert np.array_equal(fx1[smp.nda:], fx0[smp.nda:])
+    ctx.upload(smp)
+
+
+def test_zcs_terms_enter_and_need_their_planes(ctx, oracle_mod):
+    """The Zcs chain changes the likelihood (same events, couplings of the Zcs entries zeroed), and a
+    model with Zcs entries is refused when the events carry no Zcs planes."""
+    import copy
+    from pwa_b200 import lib, model as M
+    mdl, vals, blk, smp = make_test_sample("small_zcs", 1500, 15000)
+    ctx.upload(smp)
+    r_on = ctx.eval_nll(blk)
+    z = dict(vals)
+    for res in mdl.zcs:
+        for c in res.couplings:
+            z[c] = 0.0
+    blk0 = M.build_param_block(mdl, z)
+    r_off = ctx.eval_nll(blk0)
+    v_off, _, _, _ = oracle_mod.nll(smp, blk0)
+    assert abs(r_off.nll - v_off) < NLL_TOL
+    assert abs(r_on.nll - r_off.nll) > 1.0
+    bare = copy.copy(smp)
+    bare.pp3 = bare.pp4 = None
+    ctx.upload(bare)
+    with pytest.raises(lib.PwaError, match="no events"):
+        ctx.eval_nll(blk)
     ctx.upload(smp)
