@@ -86,6 +86,17 @@ int pwa_ctx_upload_zcs_events(pwa_ctx* ctx, const float* h_pp3, const float* h_p
 /* Caller-owned device planes instead (not freed by the context); in the context's event order. */
 int pwa_ctx_set_device_zcs_events(pwa_ctx* ctx, const float* d_pp3, const float* d_pp4);
 
+/* Resolution model of m(J/psi p).  PWA_SMEAR_REFERENCE (default): the reference's event classes
+ * (kernel_calEva.cu:819-961): the two data bands smeared with 30 / 150 quantile offsets times
+ * mres(m), MC in the two windows with 20, the rest unsmeared.  PWA_SMEAR_GAUSS: every event smeared
+ * with a Gaussian of width sigma (GeV) sampled on offsets (b - half_bins) * step, b = 0 .. 2 half_bins
+ * (at most 127 offsets), weights exp(-offset^2 / 2 sigma^2) normalised to 1: |A|^2 =
+ * sum_b w_b |A(m + offset_b)|^2; the band arguments are then unused.  Applies to the uploaded
+ * events and later uploads; the batch call evaluates point by point in PWA_SMEAR_GAUSS mode. */
+#define PWA_SMEAR_REFERENCE 0
+#define PWA_SMEAR_GAUSS 1
+int pwa_ctx_set_smearing(pwa_ctx* ctx, int mode, double sigma, double step, int half_bins);
+
 /* Data in any order (gen_toys/rearrange_mJpsip/reOrder.C made the reference's inputs legal by sorting
  * them): the data columns [0, nda) are put into the three m(J/psi p) bands (30-offset, 150-offset,
  * unsmeared; order kept inside each band) before the upload, and the band counts are derived as

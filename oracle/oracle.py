@@ -49,6 +49,10 @@ def lib():
         L.oracle_eval_fx_x.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, C.c_long, C.c_long, _fp,
                                        C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                        C.c_int, _dp, _dp, C.c_int]
+        L.oracle_eval_fx_grid.restype = C.c_int
+        L.oracle_eval_fx_grid.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, C.c_int, _dp, _dp, _fp,
+                                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                          C.c_float, _dp, _dp, C.c_int]
         L.oracle_amp2_x.restype = C.c_int
         L.oracle_amp2_x.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, _fp, C.c_int, C.c_int, C.c_int,
                                     C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _dp, C.c_int]
@@ -96,6 +100,33 @@ def eval_fx(sample, block, nda_smr: int, nda_fine: int, swap_coupling_parts: boo
     del keep
     if rc != 0:
         raise RuntimeError(f"oracle_eval_fx failed: {rc}")
+    return fx, fxn
+
+
+def gauss_grid(sigma: float, step: float, half_bins: int) -> tuple:
+    """Offsets (GeV) and weights of the fixed-width Gaussian resolution on a mass grid:
+    offset_b = (b - half_bins) * step, w_b proportional to exp(-offset_b^2 / (2 sigma^2)), sum w_b = 1."""
+    off = (np.arange(2 * half_bins + 1) - half_bins) * float(step)
+    w = np.exp(-0.5 * (off / float(sigma)) ** 2)
+    return off, w / w.sum()
+
+
+def eval_fx_grid(sample, block, sigma: float, step: float, half_bins: int, threads: int | None = None):
+    """Per-event fx and non-interfering w|A|^2 with every event smeared by the Gaussian grid."""
+    off, wt = gauss_grid(sigma, step, half_bins)
+    fx = np.zeros(sample.n, np.float64)
+    fxn = np.zeros(sample.n, np.float64)
+    pl = np.ascontiguousarray(block.data, np.float32)
+    p3, p4, kx = _planes_x(sample)
+    keep = (sample.pp, sample.pp1, sample.pp2, pl, kx, off, wt)
+    rc = lib().oracle_eval_fx_grid(_f(sample.pp), _f(sample.pp1), _f(sample.pp2), p3, p4, sample.n_size, sample.n,
+                                   len(off), off.ctypes.data_as(_dp), wt.ctypes.data_as(_dp), pl.ctypes.data_as(_fp),
+                                   block.para_size, block.vamp_size, block.spline_size, block.NR, block.NZ, block.NX,
+                                   block.ffr, block.ffb, fx.ctypes.data_as(_dp), fxn.ctypes.data_as(_dp),
+                                   threads or os.cpu_count())
+    del keep
+    if rc != 0:
+        raise RuntimeError(f"oracle_eval_fx_grid failed: {rc}")
     return fx, fxn
 
 

@@ -636,6 +636,31 @@ double amp2_smeared(const Model& md, const Ev& e, int nbins, const float* scheme
   return tot;
 }
 
+// Weighted grid smearing (fixed-width Gaussian on a mass grid; no counterpart in the reference):
+// sum_b w_b |A(m + off_b)|^2 evaluated as that sum, helicity by helicity (independent of the
+// expanded BW1/BW2-like form the kernels use).
+double amp2_smeared_grid(const Model& md, const Ev& e, int nb, const double* off, const double* wt) {
+  cd HL[8] = {};
+  if (!amp_lstar(md, e, HL)) return std::nan("");
+  if (md.NX > 0) amp_zcs(md, e, HL);
+  const int NZ = md.NZ;
+  std::vector<cd> HZ(NZ * 8, cd(0, 0)), bw(std::max(NZ, 1));
+  for (int i = 0; i < NZ; ++i) amp_pc_angular(md, e, i, cd(1, 0), &HZ[i * 8]);
+  const double mz = e.p0(1);
+  double tot = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (NZ > 0 && !pc_lineshapes(md, mz + off[b], 1.0, bw.data())) return std::nan("");
+    double s = 0;
+    for (int h = 0; h < 8; ++h) {
+      cd a = HL[h];
+      for (int i = 0; i < NZ; ++i) a += bw[i] * HZ[i * 8 + h];
+      s += std::norm(a);
+    }
+    tot += wt[b] * s;
+  }
+  return tot;
+}
+
 // In the reference the 3/2-band and 20-bin windows are tested on the float mass.
 bool in_mc_smear_window(float mz) { return (mz > 4.4 && mz < 4.48) || (mz > 4.27 && mz < 4.34); }
 
@@ -690,6 +715,39 @@ int oracle_eval_fx_x(const float* pp, const float* pp1, const float* pp2, const 
       fx[i] = data ? v : v * w;
       if (fx_noint) fx_noint[i] = data ? 0.0 : amp2_unsmeared(md, e, false) * w;
     }
+    if (std::isnan(v)) err |= 1;
+  }
+  return err ? -12 : 0;
+}
+
+// Every event smeared with the weighted grid (off[b] GeV, weight wt[b]); fx weighted by w for MC,
+// fx_noint the unsmeared non-interfering w|A|^2 of MC events (0 for data).
+int oracle_eval_fx_grid(const float* pp, const float* pp1, const float* pp2, const float* pp3, const float* pp4,
+                        long n_size, long n_events, int nb, const double* off, const double* wt,
+                        const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                        int NX, float FFR, float FFB, double* fx, double* fx_noint, int nthreads) {
+  if (NX > 0 && (!pp3 || !pp4)) return -10;
+  if (nb < 1 || !off || !wt) return -11;
+  Model md;
+  md.pl = paraList;
+  md.para_size = para_size;
+  md.vamp_size = vamp_size;
+  md.spline_size = spline_size;
+  md.NR = NR;
+  md.NZ = NZ;
+  md.NX = NX;
+  md.FFR = FFR;
+  md.FFB = FFB;
+  configure(md);
+  int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(| : err)
+  for (long i = 0; i < n_events; ++i) {
+    Ev e{pp, pp1, pp2, n_size, i, pp3, pp4};
+    const double v = amp2_smeared_grid(md, e, nb, off, wt);
+    const double w = pp[i + 2 * n_size];
+    const bool data = pp[i + 2 * n_size] <= -1000.f;
+    fx[i] = data ? v : v * w;
+    if (fx_noint) fx_noint[i] = data ? 0.0 : amp2_unsmeared(md, e, false) * w;
     if (std::isnan(v)) err |= 1;
   }
   return err ? -12 : 0;

@@ -47,6 +47,10 @@ struct pwa_ctx {
   const float *pp3 = nullptr, *pp4 = nullptr;  // Zcs chain planes (models with Zcs entries)
   float *own_pp3 = nullptr, *own_pp4 = nullptr;
   int64_t n = 0, n_size = 0, nda = 0, nda_smr = 0, nda_fine = 0;
+  // resolution model: PWA_SMEAR_REFERENCE, or PWA_SMEAR_GAUSS with (offset, weight) pairs on the device
+  int smear_mode = PWA_SMEAR_REFERENCE;
+  double* d_grid = nullptr;
+  int grid_nb = 0;
   int32_t* d_lists = nullptr;
   std::vector<Segment> segs;
   std::vector<int> seg_off;
@@ -89,6 +93,21 @@ struct pwa_ctx {
 
 namespace {
 
+// Segment lists and the buffers sized by the segments.
+void free_segments(pwa_ctx* c) {
+  cudaFree(c->d_lists);
+  cudaFree(c->d_parts);
+  cudaFree(c->d_defer);
+  cudaFree(c->d_defer_cnt);
+  c->d_lists = nullptr;
+  c->d_parts = nullptr;
+  c->d_defer = nullptr;
+  c->d_defer_cnt = nullptr;
+  c->segs.clear();
+  c->seg_off.clear();
+  c->seg_defer_off.clear();
+}
+
 void free_events(pwa_ctx* c) {
   cudaFree(c->own_pp);
   cudaFree(c->own_pp1);
@@ -98,19 +117,9 @@ void free_events(pwa_ctx* c) {
   cudaFree(c->own_pp4);
   c->own_pp3 = c->own_pp4 = nullptr;
   c->pp3 = c->pp4 = nullptr;
-  cudaFree(c->d_lists);
-  cudaFree(c->d_parts);
-  cudaFree(c->d_defer);
-  cudaFree(c->d_defer_cnt);
+  free_segments(c);
   c->own_pp = c->own_pp1 = c->own_pp2 = c->own_sw = nullptr;
-  c->d_lists = nullptr;
-  c->d_parts = nullptr;
-  c->d_defer = nullptr;
-  c->d_defer_cnt = nullptr;
   c->pp = c->pp1 = c->pp2 = c->sw = nullptr;
-  c->segs.clear();
-  c->seg_off.clear();
-  c->seg_defer_off.clear();
   c->order.clear();
   c->n = 0;
 }
@@ -122,9 +131,44 @@ void to_caller_order(const pwa_ctx* c, double* h) {
   for (size_t i = 0; i < c->order.size(); ++i) h[c->order[i]] = t[i];
 }
 
+int build_reference_segments(pwa_ctx* c, const float* h_mz);
+
 // Splits the events into the reference's kernel ranges (fake_kernel_store_fx,
-// kernel_calEva.cu:920-961, begin = 0) and classifies the tail by the 20-offset window.
+// kernel_calEva.cu:920-961, begin = 0) and classifies the tail by the 20-offset window; with the
+// Gaussian resolution model, one segment of all events on the weighted grid.
 int build_segments(pwa_ctx* c, const float* h_mz) {
+  const int64_t n = c->n;
+  if (c->smear_mode == PWA_SMEAR_GAUSS) {
+    c->segs.clear();
+    if (n > 0) {
+      Segment g{SMEAR_GRID, 0, n, nullptr};
+      g.grid = c->d_grid;
+      g.grid_nb = c->grid_nb;
+      c->segs.push_back(g);
+    }
+  } else {
+    const int rc = build_reference_segments(c, h_mz);
+    if (rc) return rc;
+  }
+  c->seg_off.clear();
+  c->seg_defer_off.clear();
+  int tot = 0;
+  int64_t doff = 0;
+  for (auto& s : c->segs) {
+    c->seg_off.push_back(tot);
+    tot += segment_parts(s, c->sm_count, true);
+    c->seg_defer_off.push_back(doff);
+    doff += s.end - s.begin;
+  }
+  c->total_parts = std::max(tot, 1);
+  PWA_CUDA(cudaMalloc(&c->d_parts, c->total_parts * sizeof(Partial)));
+  PWA_CUDA(cudaMemset(c->d_parts, 0, c->total_parts * sizeof(Partial)));
+  PWA_CUDA(cudaMalloc(&c->d_defer, std::max<int64_t>(n, 1) * sizeof(int32_t)));
+  PWA_CUDA(cudaMalloc(&c->d_defer_cnt, 8 * sizeof(int)));
+  return PWA_OK;
+}
+
+int build_reference_segments(pwa_ctx* c, const float* h_mz) {
   const int64_t n = c->n;
   const int64_t b1e = std::max<int64_t>(0, std::min(n, c->nda_smr));
   const int64_t b2s = std::max<int64_t>(0, c->nda_smr);
@@ -147,21 +191,6 @@ int build_segments(pwa_ctx* c, const float* h_mz) {
   if (b1e > 0) c->segs.push_back({SMEAR_30, 0, b1e, nullptr});
   if (!lw.empty()) c->segs.push_back({SMEAR_20, 0, (int64_t)lw.size(), c->d_lists});
   if (!lu.empty()) c->segs.push_back({SMEAR_NONE, 0, (int64_t)lu.size(), c->d_lists + lw.size()});
-  c->seg_off.clear();
-  c->seg_defer_off.clear();
-  int tot = 0;
-  int64_t doff = 0;
-  for (auto& s : c->segs) {
-    c->seg_off.push_back(tot);
-    tot += segment_parts(s, c->sm_count, true);
-    c->seg_defer_off.push_back(doff);
-    doff += s.end - s.begin;
-  }
-  c->total_parts = std::max(tot, 1);
-  PWA_CUDA(cudaMalloc(&c->d_parts, c->total_parts * sizeof(Partial)));
-  PWA_CUDA(cudaMemset(c->d_parts, 0, c->total_parts * sizeof(Partial)));
-  PWA_CUDA(cudaMalloc(&c->d_defer, std::max<int64_t>(n, 1) * sizeof(int32_t)));
-  PWA_CUDA(cudaMalloc(&c->d_defer_cnt, 8 * sizeof(int)));
   return PWA_OK;
 }
 
@@ -226,6 +255,7 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   cudaFree(c->d_bparts);
   cudaFreeHost(c->h_bres);
   free_events(c);
+  cudaFree(c->d_grid);
   cudaFree(c->d_table);
   cudaFreeHost(c->h_table);
   cudaFree(c->d_res);
@@ -337,6 +367,35 @@ int pwa_ctx_set_device_events(pwa_ctx* c, const float* d_pp, const float* d_pp1,
   c->nda_fine = nda_fine;
   std::vector<float> mz((size_t)std::max<int64_t>(n, 1));
   if (n) PWA_CUDA(cudaMemcpy(mz.data(), d_pp + n_size, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return build_segments(c, mz.data());
+}
+
+int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int half_bins) {
+  if (!c) return PWA_E_ARG;
+  if (mode != PWA_SMEAR_REFERENCE && mode != PWA_SMEAR_GAUSS) return PWA_E_ARG;
+  PWA_CUDA(cudaSetDevice(c->device));
+  if (mode == PWA_SMEAR_GAUSS) {
+    if (!(sigma > 0) || !(step > 0) || half_bins < 0 || 2 * half_bins + 1 > GRID_MAX_NB) return PWA_E_ARG;
+    const int nb = 2 * half_bins + 1;
+    std::vector<double> g(2 * nb);
+    double sum = 0;
+    for (int b = 0; b < nb; ++b) {
+      const double off = (b - half_bins) * step;
+      g[2 * b] = off;
+      g[2 * b + 1] = std::exp(-0.5 * (off / sigma) * (off / sigma));
+      sum += g[2 * b + 1];
+    }
+    for (int b = 0; b < nb; ++b) g[2 * b + 1] /= sum;
+    if (!c->d_grid) PWA_CUDA(cudaMalloc(&c->d_grid, 2 * GRID_MAX_NB * sizeof(double)));
+    PWA_CUDA(cudaMemcpy(c->d_grid, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->grid_nb = nb;
+  }
+  c->smear_mode = mode;
+  if (!c->pp) return PWA_OK;
+  // re-split the uploaded events for the new model
+  free_segments(c);
+  std::vector<float> mz((size_t)std::max<int64_t>(c->n, 1));
+  if (c->n) PWA_CUDA(cudaMemcpy(mz.data(), c->pp + c->n_size, c->n * sizeof(float), cudaMemcpyDeviceToHost));
   return build_segments(c, mz.data());
 }
 
@@ -505,7 +564,8 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   int ntab = 0;
   for (int p = 0; p < npoints; ++p) {
     // the structured kernels carry no Zcs terms: models with Zcs entries take the single-point path
-    bool ok = NX == 0 && classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
+    bool ok = NX == 0 && c->smear_mode == PWA_SMEAR_REFERENCE &&
+              classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
     if (ok && bp[p].kind == BP_PCG && c->use_tables) ok = ntab++ < BATCH_MAX_TABLES;
     (ok ? sidx : fidx).push_back(p);
   }

@@ -462,5 +462,7 @@ template <>
 __device__ __forceinline__ const float* smear_table<30>() { return kSmear30; }
 template <>
 __device__ __forceinline__ const float* smear_table<150>() { return kSmear150; }
+template <>
+__device__ __forceinline__ const float* smear_table<0>() { return nullptr; }  // weighted grid scheme
 
 }  // namespace pwa

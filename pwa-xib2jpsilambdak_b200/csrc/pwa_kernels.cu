@@ -183,13 +183,17 @@ constexpr size_t SMEARED_SMEM = align16(sizeof(PointTable)) + EV_WARPS * sizeof(
 // and rescale u = float(1/w).  band = 1 for the two data bands (fx unweighted, no non-interference
 // term), 0 for the tail-region window events.
 //
+// NB = 0: the weighted grid scheme (grid[2b] absolute offset in GeV, grid[2b+1] weight w_b, grid_nb
+// offsets, sum of weights 1): |A|^2 = sum_b w_b |A(m + offset_b)|^2
+//   = sum_h |H_L|^2 + 2 Re(conj(H_L) sum_b w_b S_b) + sum_b w_b |S_b|^2.
+//
 // FIX as for k_unsmeared: the main launch defers every event with a resolution offset the table
 // cannot serve.
 template <int NB, bool FIX, bool ZCS>
 __global__ void __launch_bounds__(EV_THREADS, 2)
     k_smeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
               const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band, int32_t* defer,
-              int* defer_count) {
+              int* defer_count, const double* __restrict__ grid, int grid_nb) {
   extern __shared__ __align__(16) unsigned char sm[];
   PointTable& T = *reinterpret_cast<PointTable*>(sm);
   load_table<EV_THREADS>(gtab, &T);
@@ -197,15 +201,15 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
   const int lane = threadIdx.x & 31, ei = lane >> 3, h = lane & 7;
   const int hi = h >> 2, hj = (h >> 1) & 1, hk = h & 1;
   const float* qoff = smear_table<NB>();
-  const float wf = (float)(1.0 / NB);
-  const double wgt = wf;
-  const double c2 = wgt * wgt * (double)(1.0f / wf);
+  const float wf = (float)(1.0 / (NB ? NB : 1));
+  const double wgt = NB ? (double)wf : 1.0;
+  const double c2 = NB ? wgt * wgt * (double)(1.0f / wf) : 1.0;
   if (n_list) end = begin + *n_list;
   const Chunk ch = block_chunk(end - begin, EV_WARPS * SMEARED_PER_WARP, n_list != nullptr);
   cplx* R = W.raw + ei * RAW_EVENT;
   // band 0: lookup 0 is at the event's own mass (|A|^2 without interference for the MC check sum)
   const int shift = band ? 0 : 1;
-  const int nlook = NB + shift;
+  const int nlook = (NB ? NB : grid_nb) + shift;
   Acc acc;
   for (int64_t base = ch.c0 + ch.warp0 * SMEARED_PER_WARP; base < ch.c1; base += ch.wstep * SMEARED_PER_WARP) {
     const int64_t p = base + ei;
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
       const int l = l0 + h;
       if (l < nlook) {
         const int b = l - shift;
-        const double m = b < 0 ? mz : mz + (double)qoff[b] * mres;
+        const double m = b < 0 ? mz : NB ? mz + (double)qoff[b] * mres : mz + __ldg(grid + 2 * b);
         if (FIX)
           lookup_entries(T, m, R + h * RAW_ROW);
         else
@@ -278,9 +282,13 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
         }
         if (l0 + bb < shift) {
           vn = vlx + norm2(s);
-        } else {
+        } else if (NB) {
           a1 += s;
           a2 += norm2(s);
+        } else {
+          const double wb = __ldg(grid + 2 * (l0 + bb - shift) + 1);
+          a1 += wb * s;
+          a2 += wb * norm2(s);
         }
       }
       __syncwarp();
@@ -492,7 +500,7 @@ __global__ void k_finalize(const Partial* parts, int n, int stride, double sum_w
 // ------------------------------------------------------------------------------- host side
 // Resident blocks per SM of the event kernels by segment kind (from the occupancy calculator, set by
 // configure_kernels); a segment launches at most sm_count times that many blocks.
-static int g_occ[4] = {1, 1, 1, 1};
+static int g_occ[SMEAR_KINDS] = {1, 1, 1, 1, 1};
 
 static int events_per_block(int kind) {
   return kind == SMEAR_NONE ? EV_WARPS * UNSMEARED_PER_WARP : EV_WARPS * SMEARED_PER_WARP;
@@ -517,7 +525,8 @@ int segment_parts(const Segment& s, int sm_count, bool deferred) {
 template <bool FIX, bool ZCS>
 static void launch_kind_t(const EventSet& ev, int kind, int64_t begin, int64_t end, const int32_t* list,
                           const int* n_list, const PointTable* d_table, Partial* out, double* fx_out, int mode,
-                          int32_t* defer, int* defer_count, int nb, cudaStream_t st) {
+                          int32_t* defer, int* defer_count, int nb, const double* grid, int grid_nb,
+                          cudaStream_t st) {
   switch (kind) {
     case SMEAR_NONE:
       k_unsmeared<FIX, ZCS><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
@@ -525,15 +534,19 @@ static void launch_kind_t(const EventSet& ev, int kind, int64_t begin, int64_t e
       break;
     case SMEAR_20:
       k_smeared<20, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
-                                                                     fx_out, 0, defer, defer_count);
+                                                                     fx_out, 0, defer, defer_count, nullptr, 0);
       break;
     case SMEAR_30:
       k_smeared<30, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
-                                                                     fx_out, 1, defer, defer_count);
+                                                                     fx_out, 1, defer, defer_count, nullptr, 0);
       break;
     case SMEAR_150:
       k_smeared<150, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
-                                                                      fx_out, 1, defer, defer_count);
+                                                                      fx_out, 1, defer, defer_count, nullptr, 0);
+      break;
+    case SMEAR_GRID:
+      k_smeared<0, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
+                                                                    fx_out, 0, defer, defer_count, grid, grid_nb);
       break;
   }
 }
@@ -541,15 +554,15 @@ static void launch_kind_t(const EventSet& ev, int kind, int64_t begin, int64_t e
 // The Zcs variants run when the event set carries the Zcs planes (the caller passes them only for a
 // model with Zcs entries).
 template <bool FIX>
-static void launch_kind(const EventSet& ev, int kind, int64_t begin, int64_t end, const int32_t* list,
+static void launch_kind(const EventSet& ev, const Segment& seg, int64_t begin, int64_t end, const int32_t* list,
                         const int* n_list, const PointTable* d_table, Partial* out, double* fx_out, int mode,
                         int32_t* defer, int* defer_count, int nb, cudaStream_t st) {
   if (ev.pp3)
-    launch_kind_t<FIX, true>(ev, kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count, nb,
-                             st);
+    launch_kind_t<FIX, true>(ev, seg.kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count,
+                             nb, seg.grid, seg.grid_nb, st);
   else
-    launch_kind_t<FIX, false>(ev, kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count, nb,
-                              st);
+    launch_kind_t<FIX, false>(ev, seg.kind, begin, end, list, n_list, d_table, out, fx_out, mode, defer, defer_count,
+                              nb, seg.grid, seg.grid_nb, st);
 }
 
 // One segment: with a deferral buffer (tables on), the table-only pass over the segment and then the
@@ -558,16 +571,18 @@ static cudaError_t launch_passes(const EventSet& ev, const Segment& seg, const P
                                  double* fx_out, int mode, int32_t* defer, int* defer_count, int sm_count,
                                  cudaStream_t st) {
   if (seg.end <= seg.begin) return cudaSuccess;
-  if (seg.kind < SMEAR_NONE || seg.kind > SMEAR_150) return cudaErrorInvalidValue;
+  if (seg.kind < SMEAR_NONE || seg.kind >= SMEAR_KINDS) return cudaErrorInvalidValue;
+  if (seg.kind == SMEAR_GRID && (!seg.grid || seg.grid_nb < 1 || seg.grid_nb > GRID_MAX_NB))
+    return cudaErrorInvalidValue;
   const int nb = segment_blocks(seg, sm_count);
   if (defer) {
-    launch_kind<false>(ev, seg.kind, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, defer,
+    launch_kind<false>(ev, seg, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, defer,
                        defer_count, nb, st);
-    launch_kind<true>(ev, seg.kind, 0, 0, defer, defer_count, d_table, out ? out + nb : nullptr, fx_out, mode,
-                      nullptr, nullptr, fix_blocks(seg, sm_count), st);
+    launch_kind<true>(ev, seg, 0, 0, defer, defer_count, d_table, out ? out + nb : nullptr, fx_out, mode, nullptr,
+                      nullptr, fix_blocks(seg, sm_count), st);
   } else {
-    launch_kind<true>(ev, seg.kind, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, nullptr,
-                      nullptr, nb, st);
+    launch_kind<true>(ev, seg, seg.begin, seg.end, seg.list, nullptr, d_table, out, fx_out, mode, nullptr, nullptr,
+                      nb, st);
   }
   return cudaGetLastError();
 }
@@ -596,6 +611,8 @@ static cudaError_t configure_variant(int* occ) {
   if ((e = configure_one(k_smeared<20, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_20]))) return e;
   if ((e = configure_one(k_smeared<30, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_30]))) return e;
   if ((e = configure_one(k_smeared<150, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_150]))) return e;
+  if ((e = configure_one(k_smeared<0, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_GRID]))) return e;
+  if ((e = configure_one(k_smeared<0, true, ZCS>, SMEARED_SMEM, &unused))) return e;
   if ((e = configure_one(k_smeared<20, true, ZCS>, SMEARED_SMEM, &unused))) return e;
   if ((e = configure_one(k_smeared<30, true, ZCS>, SMEARED_SMEM, &unused))) return e;
   if ((e = configure_one(k_smeared<150, true, ZCS>, SMEARED_SMEM, &unused))) return e;

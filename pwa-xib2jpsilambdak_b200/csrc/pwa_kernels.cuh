@@ -41,12 +41,18 @@ struct EventSet {
   const float* pp4 = nullptr;
 };
 
-enum Smear : int { SMEAR_NONE = 0, SMEAR_20 = 1, SMEAR_30 = 2, SMEAR_150 = 3 };
+// Event classes: unsmeared, the reference's three quantile schemes (offsets in units of the mass
+// resolution, equal weights), and a weighted grid of absolute offsets (fixed-width Gaussian).
+enum Smear : int { SMEAR_NONE = 0, SMEAR_20 = 1, SMEAR_30 = 2, SMEAR_150 = 3, SMEAR_GRID = 4 };
+constexpr int SMEAR_KINDS = 5;
+constexpr int GRID_MAX_NB = 127;
 
 struct Segment {
   int kind;             // Smear
   int64_t begin, end;   // contiguous event range when list == nullptr
   const int32_t* list;  // event indices, [begin, end) positions in the list otherwise
+  const double* grid = nullptr;  // SMEAR_GRID: (offset in GeV, weight) pairs on the device
+  int grid_nb = 0;               // SMEAR_GRID: number of offsets
 };
 
 // Blocks of the pass over a segment (and partial slots of that pass).

@@ -39,3 +39,16 @@ def test_oracle_vs_reference_live(name, oracle_mod):
     # swapping the coupling read order breaks agreement by orders of magnitude
     v2, _, _, _ = oracle_mod.nll(smp, blk, swap_coupling_parts=True)
     assert abs(rv - v2) > 100 * abs(rv - v)
+
+
+def test_oracle_grid_smearing_limits(oracle_mod):
+    """The oracle's Gaussian-grid smearing: one offset at zero is the unsmeared |A|^2 (times w for MC),
+    and the weights sum to one."""
+    from conftest import make_test_sample
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 300, 3000)
+    off, w = oracle_mod.gauss_grid(0.0027, 0.0005, 17)
+    assert len(off) == 35 and abs(w.sum() - 1) < 1e-15 and off[17] == 0.0
+    fx, fxn = oracle_mod.eval_fx_grid(smp, blk, 0.0027, 0.0005, 0)
+    a2 = oracle_mod.amp2(smp, blk)
+    wt = np.where(np.arange(smp.n) < smp.nda, 1.0, np.asarray(smp.pp[2 * smp.n_size:2 * smp.n_size + smp.n], np.float64))
+    assert np.max(np.abs(fx - a2 * wt) / (a2 * wt)) < 1e-13
