@@ -345,10 +345,61 @@ struct EvX {
   __device__ __forceinline__ double DX(int s, int k, int m) const { return ldf(pp4, e + (s * 24 + k * 12 + m) * ns); }
 };
 
+// One event's planes staged in shared memory as doubles (slots SLOT_*), with the accessors of Ev / EvX.
+struct EvS {
+  const double* p;
+  __device__ __forceinline__ double mkp() const { return p[0]; }
+  __device__ __forceinline__ double mz() const { return p[1]; }
+  __device__ __forceinline__ cplx A(int i, int j, int m) const {
+    const int a = 3 + (i * 12 + j * 6 + m) * 2;
+    return mk(p[a], p[a + 1]);
+  }
+  __device__ __forceinline__ double DL(int s, int k, int m) const { return p[51 + s * 12 + k * 6 + m]; }
+  __device__ __forceinline__ cplx AZ(int i, int j, int m) const {
+    const int a = SLOT_PP1 + (i * 24 + j * 12 + m) * 2;
+    return mk(p[a], p[a + 1]);
+  }
+  __device__ __forceinline__ double DZ(int s, int k, int m) const { return p[SLOT_PP2 + s * 24 + k * 12 + m]; }
+  __device__ __forceinline__ double mjk() const { return p[SLOT_PP3]; }
+  __device__ __forceinline__ cplx AX(int i, int j, int m) const {
+    const int a = SLOT_PP3 + 1 + (i * 24 + j * 12 + m) * 2;
+    return mk(p[a], p[a + 1]);
+  }
+  __device__ __forceinline__ double DX(int s, int k, int m) const { return p[SLOT_PP4 + s * 24 + k * 12 + m]; }
+};
+
+// Copies the plane slots point T reads of event e into dst (warp-cooperative, lane = 0 .. 31),
+// converting to double; the caller synchronises the warp before reading.
+__device__ __forceinline__ void stage_event(const PointTable& T, const EventSet& ev, int64_t e, double* dst,
+                                            int lane) {
+  for (int i = lane; i < T.nstage; i += 32) {
+    const int s = T.stage[i];
+    const float* src;
+    int plane;
+    if (s < SLOT_PP1) {
+      src = ev.pp;
+      plane = s;
+    } else if (s < SLOT_PP2) {
+      src = ev.pp1;
+      plane = s - SLOT_PP1;
+    } else if (s < SLOT_PP3) {
+      src = ev.pp2;
+      plane = s - SLOT_PP2;
+    } else if (s < SLOT_PP4) {
+      src = ev.pp3;
+      plane = s - SLOT_PP3;
+    } else {
+      src = ev.pp4;
+      plane = s - SLOT_PP4;
+    }
+    dst[s] = ldf(src, e + (int64_t)plane * ev.n_size);
+  }
+}
+
 // Zcs chain amplitudes of proton helicity k for the helicities (i, j) in ij_lo .. ij_hi - 1
 // (ij = 2 i + j), added to H[ij - ij_lo]: sum_x lineshape_x sum_m c_{x,k,m} DX AX.
-template <int NIJ>
-__device__ __forceinline__ void zcs_amplitudes(const PointTable& T, const EvX& X, int k, int ij_lo, cplx* H) {
+template <int NIJ, class XA>
+__device__ __forceinline__ void zcs_amplitudes(const PointTable& T, const XA& X, int k, int ij_lo, cplx* H) {
   const XKin xk = x_kin(T, X.mjk());
   for (int x = 0; x < T.NX; ++x) {
     const XEntry& Xe = T.X[x];
@@ -369,6 +420,10 @@ __device__ __forceinline__ void zcs_amplitudes(const PointTable& T, const EvX& X
 
 __device__ __forceinline__ cplx shfl_xor(cplx v, int o) {
   return mk(__shfl_xor_sync(0xffffffffu, v.re, o), __shfl_xor_sync(0xffffffffu, v.im, o));
+}
+
+__device__ __forceinline__ cplx shfl(cplx v, int src) {
+  return mk(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
 }
 
 // ------------------------------------------------------------------------------- reductions
@@ -433,7 +488,6 @@ struct Acc {
 constexpr int EV_THREADS = 256;
 constexpr int EV_WARPS = EV_THREADS / 32;
 constexpr int UNSMEARED_PER_WARP = 16;  // events per warp: lane = 16 * k + event
-constexpr int SMEARED_PER_WARP = 4;     // events per warp: lane = 8 * event + helicity
 
 __device__ __forceinline__ int64_t event_index(const int32_t* list, int64_t begin, int64_t p) {
   return list ? (int64_t)list[begin + p] : begin + p;

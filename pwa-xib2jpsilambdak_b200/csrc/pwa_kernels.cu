@@ -158,39 +158,51 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
   if (mode != 1) block_reduce_store<EV_THREADS>(acc.data, acc.mc, acc.mcn, acc.bad, parts);
 }
 
-// Per-warp scratch of the smeared kernels: Lambda* lineshapes of the warp's 4 events and, per event,
-// the Pc entry lineshapes at 8 resolution offsets.  Row and event strides are 4 words modulo 32
-// banks, so the 8 lanes of an event write their rows without bank conflicts.
+// Per-warp scratch of the smeared kernels: the event's plane slots (as doubles) and, in the
+// exact-capable pass, the Pc entry lineshapes of the 8 offset rows of a round that the table cannot
+// serve.
 constexpr int RAW_ROW = MAX_PC + 1;
-constexpr int RAW_EVENT = 8 * RAW_ROW + 1;
 struct SmearWarp {
-  cplx q[SMEARED_PER_WARP][MAX_LSTAR];
-  cplx raw[SMEARED_PER_WARP * RAW_EVENT];
+  double pl[SLOT_ALL];
+  cplx raw[8 * RAW_ROW];
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 constexpr size_t UNSMEARED_SMEM = align16(sizeof(PointTable));
 constexpr size_t SMEARED_SMEM = align16(sizeof(PointTable)) + EV_WARPS * sizeof(SmearWarp);
 
+// D += A B for one 8x8x4 FP64 tile (warp-wide; A row-major, B column-major): lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + i], i = 0, 1.
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // Events smeared over NB resolution offsets (kernel_store_fx_SMR / _finebinning, kernel_calEva.cu:
-// 819-900; TemplateGetAmp2s :583-784).  Lanes 8e .. 8e+7 of a warp hold event e; lane h holds the
-// helicity (dmu, lb, k) = (h/4, h/2 % 2, h % 2), its Lambda* amplitude H_L and, in registers, the Pc
-// angular amplitude HZ_q of every entry q (couplings included, lineshape excluded).  The offsets go
-// in rounds of 8: each lane evaluates all Pc entry lineshapes at one offset into the warp's scratch,
-// then every lane contracts S_b = sum_q lineshape_q(m_b) HZ_q for all 8 offsets.  Finally
+// 819-900; TemplateGetAmp2s :583-784).  One warp per event: the warp first copies the plane slots
+// the point reads into shared memory (one batch of independent loads), then for the 8 helicities h = (dmu, lb, k)
+// the kernel forms the Lambda* amplitude H_L[h] and, per Pc entry q, the angular amplitude
+// HZ_q[h] (couplings included, lineshape excluded); the offsets go in rounds of 8 rows b with
+// lineshapes R_q(m_b), and the contraction S_b[h] = sum_q R_q(m_b) HZ_q[h] runs on the FP64 tensor
+// path as two real products, [Re S | Im S] = [Re R | Im R] x [[Re HZ, Im HZ], [-Im HZ, Re HZ]].
+// Lane (row g = l/4, column t = l%4) evaluates exactly its own operand elements: the lineshapes of
+// entries q = t, t+4, t+8, t+12 at the offset of row g (A[g][k]) and HZ_q of helicity g (B[k][g]); it
+// receives S_b[h] for row g and helicities 2t, 2t+1.  Finally
 //   |A|^2 = sum_h |H_L|^2 + 2 w Re(conj(H_L) sum_b S_b) + w^2 u sum_b |S_b|^2,
-// the reference's BW1/BW2 form (kernel_calEva.cu:676-810) with its float weight w = float(1/NB)
-// and rescale u = float(1/w).  band = 1 for the two data bands (fx unweighted, no non-interference
-// term), 0 for the tail-region window events.
+// the reference's BW1/BW2 form (kernel_calEva.cu:676-810) with its float weight w = float(1/NB) and
+// rescale u = float(1/w).  band = 1 for the two data bands (fx unweighted, no non-interference
+// term), 0 for the tail-region window events (row 0 of the first round is then the event's own
+// mass, for |A|^2 without interference).
 //
 // NB = 0: the weighted grid scheme (grid[2b] absolute offset in GeV, grid[2b+1] weight w_b, grid_nb
 // offsets, sum of weights 1): |A|^2 = sum_b w_b |A(m + offset_b)|^2
 //   = sum_h |H_L|^2 + 2 Re(conj(H_L) sum_b w_b S_b) + sum_b w_b |S_b|^2.
 //
 // FIX as for k_unsmeared: the main launch defers every event with a resolution offset the table
-// cannot serve.
+// cannot serve; the exact-capable launch evaluates such rows exactly (one lane per row).
 template <int NB, bool FIX, bool ZCS>
-__global__ void __launch_bounds__(EV_THREADS, 2)
+__global__ void __launch_bounds__(EV_THREADS, 3)
     k_smeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
               const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int band, int32_t* defer,
               int* defer_count, const double* __restrict__ grid, int grid_nb) {
@@ -198,120 +210,148 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
   PointTable& T = *reinterpret_cast<PointTable*>(sm);
   load_table<EV_THREADS>(gtab, &T);
   SmearWarp& W = reinterpret_cast<SmearWarp*>(sm + align16(sizeof(PointTable)))[threadIdx.x / 32];
-  const int lane = threadIdx.x & 31, ei = lane >> 3, h = lane & 7;
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;   // fragment row (offset row, B-operand helicity) and column
+  const int h = lane & 7, part = lane >> 3;  // helicity and resonance share of the Lambda* sums
   const int hi = h >> 2, hj = (h >> 1) & 1, hk = h & 1;
+  const int bi = g >> 2, bj = (g >> 1) & 1, bk = g & 1;
   const float* qoff = smear_table<NB>();
   const float wf = (float)(1.0 / (NB ? NB : 1));
   const double wgt = NB ? (double)wf : 1.0;
   const double c2 = NB ? wgt * wgt * (double)(1.0f / wf) : 1.0;
   if (n_list) end = begin + *n_list;
-  const Chunk ch = block_chunk(end - begin, EV_WARPS * SMEARED_PER_WARP, n_list != nullptr);
-  cplx* R = W.raw + ei * RAW_EVENT;
-  // band 0: lookup 0 is at the event's own mass (|A|^2 without interference for the MC check sum)
+  const Chunk ch = block_chunk(end - begin, EV_WARPS, n_list != nullptr);
   const int shift = band ? 0 : 1;
   const int nlook = (NB ? NB : grid_nb) + shift;
+  const int NZ = T.NZ;
+  const int nq = (NZ + 3) >> 2;  // k-steps per real product (entries q = t + 4j, j < nq)
+  const int pmask = T.pc_mmask[bk];
+  const int lmask = T.lstar_mmask[hk];
   Acc acc;
-  for (int64_t base = ch.c0 + ch.warp0 * SMEARED_PER_WARP; base < ch.c1; base += ch.wstep * SMEARED_PER_WARP) {
-    const int64_t p = base + ei;
-    const bool valid = p < ch.c1;
-    const Ev E{ev.pp, ev.pp1, ev.pp2, ev.n_size, event_index(list, begin, valid ? p : 0)};
-    const double mkp = E.mkp(), mz = E.mz();
-    {
-      const LstarKin lk = lstar_kin(T, mkp);
-      for (int r = h; r < T.NR; r += 8) W.q[ei][r] = lstar_lineshape(T.L[r], lk);
-    }
+  for (int64_t p = ch.c0 + ch.warp0; p < ch.c1; p += ch.wstep) {
+    const int64_t e = event_index(list, begin, p);
+    stage_event(T, ev, e, W.pl, lane);
     __syncwarp();
+    const EvS E{W.pl};
+    const double mkp = E.mkp(), mz = E.mz();
+    // Lambda*: lane r evaluates lineshape r; lane (h, part) sums the resonances r = part mod 4
+    cplx qmine = mk(0, 0);
+    if (lane < T.NR) qmine = lstar_lineshape(T.L[lane], lstar_kin(T, mkp));
     cplx hl = mk(0, 0);
-    for (int r = 0; r < T.NR; ++r) {
-      const LstarEntry& L = T.L[r];
-      cplx f = mk(0, 0);
+    for (int r0 = 0; r0 < T.NR; r0 += 4) {
+      const int r = r0 + part;
+      const cplx q = shfl(qmine, r & 31);
+      if (r < T.NR) {
+        const LstarEntry& L = T.L[r];
+        const cplx* cl = L.c + hk * 6;
+        const double* dl = E.p + 51 + L.sidx * 12 + hk * 6;
+        cplx f = mk(0, 0);
 #pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        const cplx c = L.c[hk * 6 + m];
-        if (nonzero(c)) cmac(f, c, E.A(hi, hj, m) * E.DL(L.sidx, hk, m));
+        for (int m = 0; m < 6; ++m) {
+          if (!(lmask >> m & 1)) continue;
+          const cplx c = cl[m];
+          if (nonzero(c)) cmac(f, c, E.A(hi, hj, m) * dl[m]);
+        }
+        cmac(hl, q, f);
       }
-      cmac(hl, W.q[ei][r], f);
     }
+    hl += shfl_xor(hl, 8);
+    hl += shfl_xor(hl, 16);
     // Zcs joins H_L (H_L_Zcs of TemplateGetAmp2s); |A|^2 without interference keeps it separate
     double vlx = norm2(hl);
     if (ZCS) {
       cplx hx = mk(0, 0);
-      zcs_amplitudes<1>(T, EvX{ev.pp3, ev.pp4, ev.n_size, E.e}, hk, 2 * hi + hj, &hx);
+      zcs_amplitudes<1>(T, E, hk, 2 * hi + hj, &hx);
       vlx += norm2(hx);
       hl += hx;
     }
-    cplx hz[MAX_PC];
+    const double hl2 = part == 0 ? norm2(hl) : 0.0;  // sum over lanes: sum_h |H_L[h]|^2
+    vlx = part == 0 ? vlx : 0.0;
+    const cplx hA = shfl(hl, 2 * t), hB = shfl(hl, 2 * t + 1);  // H_L of this lane's output columns
+    // B operand: HZ_q[g] for q = t + 4j
+    cplx hz[MAX_PC / 4];
 #pragma unroll
-    for (int q = 0; q < MAX_PC; ++q) hz[q] = mk(0, 0);
-    const int pmask = T.pc_mmask[hk];
+    for (int j = 0; j < MAX_PC / 4; ++j) hz[j] = mk(0, 0);
 #pragma unroll
     for (int m = 0; m < 12; ++m) {
       if (!(pmask >> m & 1)) continue;
-      const cplx az = E.AZ(hi, hj, m);
+      const cplx az = E.AZ(bi, bj, m);
 #pragma unroll
-      for (int q = 0; q < MAX_PC; ++q) {
-        if (q >= T.NZ) break;
+      for (int j = 0; j < MAX_PC / 4; ++j) {
+        const int q = t + 4 * j;
+        if (q >= NZ) break;
         const PcEntry& Z = T.Z[T.order[q]];
-        const cplx c = Z.c[hk * 12 + m];
-        if (nonzero(c)) cmac(hz[q], c, az * E.DZ(Z.sidx, hk, m));
+        const cplx c = Z.c[bk * 12 + m];
+        if (nonzero(c)) cmac(hz[j], c, az * E.DZ(Z.sidx, bk, m));
       }
     }
     const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
-    double vn = 0, a2 = 0;
-    cplx a1 = mk(0, 0);
+    double a1 = 0, a2 = 0, vn = 0;
     bool fail = false;
-    for (int l0 = 0; l0 < nlook; l0 += 8) {
-      const int l = l0 + h;
-      if (l < nlook) {
+    for (int l0 = 0; NZ > 0 && l0 < nlook; l0 += 8) {
+      const int l = l0 + g;
+      const bool row = l < nlook;
+      double m = mz, wb = 1.0;
+      if (row && l >= shift) {
         const int b = l - shift;
-        const double m = b < 0 ? mz : NB ? mz + (double)qoff[b] * mres : mz + __ldg(grid + 2 * b);
-        if (FIX)
-          lookup_entries(T, m, R + h * RAW_ROW);
-        else
-          fail |= !lookup_table(T, m, R + h * RAW_ROW);
+        m = NB ? mz + (double)qoff[b] * mres : mz + __ldg(grid + 2 * b);
+        if (!NB) wb = __ldg(grid + 2 * b + 1);
       }
-      __syncwarp();
-      const int nl = min(8, nlook - l0);
-      for (int bb = 0; bb < nl; ++bb) {
-        const cplx* r = R + bb * RAW_ROW;
-        cplx s = mk(0, 0);
+      TabAt ta;
+      const bool ok = row && tab_at(T.tab, m, ta);
+      if (FIX) {
+        if (row && !ok && t == 0) pc_entries_exact(T, m, W.raw + g * RAW_ROW);
+        __syncwarp();
+      } else {
+        fail |= row && !ok;
+      }
+      double are[MAX_PC / 4], aim[MAX_PC / 4];
 #pragma unroll
-        for (int q = 0; q < MAX_PC; ++q) {
-          if (q >= T.NZ) break;
-          cmac(s, r[q], hz[q]);
-        }
-        if (l0 + bb < shift) {
-          vn = vlx + norm2(s);
-        } else if (NB) {
-          a1 += s;
-          a2 += norm2(s);
+      for (int j = 0; j < MAX_PC / 4; ++j) {
+        const int q = t + 4 * j;
+        cplx r = mk(0, 0);
+        if (row && q < NZ) r = ok ? tab_get(ta, T.tab.stride, q) : (FIX ? W.raw[g * RAW_ROW + q] : mk(0, 0));
+        are[j] = r.re;
+        aim[j] = r.im;
+      }
+      if (FIX) __syncwarp();
+      double sr0 = 0, sr1 = 0, si0 = 0, si1 = 0;
+#pragma unroll
+      for (int j = 0; j < MAX_PC / 4; ++j) {
+        if (j >= nq) break;
+        dmma(sr0, sr1, are[j], hz[j].re);
+        dmma(si0, si1, are[j], hz[j].im);
+        dmma(sr0, sr1, aim[j], -hz[j].im);
+        dmma(si0, si1, aim[j], hz[j].re);
+      }
+      if (row) {
+        const double n2 = sr0 * sr0 + si0 * si0 + sr1 * sr1 + si1 * si1;
+        if (l < shift) {
+          vn += n2;
         } else {
-          const double wb = __ldg(grid + 2 * (l0 + bb - shift) + 1);
-          a1 += wb * s;
-          a2 += wb * norm2(s);
+          a1 += wb * (hA.re * sr0 + hA.im * si0 + hB.re * sr1 + hB.im * si1);
+          a2 += wb * n2;
         }
       }
-      __syncwarp();
     }
-    double v = norm2(hl) + 2.0 * wgt * (hl.re * a1.re + hl.im * a1.im) + c2 * a2;
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-      v += __shfl_xor_sync(0xffffffffu, v, o);
-      vn += __shfl_xor_sync(0xffffffffu, vn, o);
-    }
-    const bool deferred = !FIX && ((__ballot_sync(0xffffffffu, fail) >> (ei * 8)) & 0xFFu);
-    if (h == 0 && valid && deferred) defer[atomicAdd(defer_count, 1)] = (int32_t)E.e;
-    if (h == 0 && valid && !deferred) {
-      double fxe = v, vnw = 0;
-      if (!band) {
-        const float wfe = E.w();
-        if (!(wfe <= -1000.f)) {
-          fxe = v * (double)wfe;
-          vnw = vn * (double)wfe;
+    const double v = warp_sum(hl2) + 2.0 * wgt * warp_sum(a1) + c2 * warp_sum(a2);
+    const double vnt = warp_sum(vlx) + warp_sum(vn);
+    const bool deferred = !FIX && __any_sync(0xffffffffu, fail);
+    if (lane == 0) {
+      if (deferred) {
+        defer[atomicAdd(defer_count, 1)] = (int32_t)e;
+      } else {
+        double fxe = v, vnw = 0;
+        if (!band) {
+          const float wfe = (float)E.p[2];
+          if (!(wfe <= -1000.f)) {
+            fxe = v * (double)wfe;
+            vnw = vnt * (double)wfe;
+          }
         }
+        if (fx_out) fx_out[e] = fxe;
+        acc.add(e, ev.nda, ev.sw, fxe, vnw, band != 0);
       }
-      if (fx_out) fx_out[E.e] = fxe;
-      acc.add(E.e, ev.nda, ev.sw, fxe, vnw, band != 0);
     }
     __syncwarp();
   }
@@ -502,9 +542,7 @@ __global__ void k_finalize(const Partial* parts, int n, int stride, double sum_w
 // configure_kernels); a segment launches at most sm_count times that many blocks.
 static int g_occ[SMEAR_KINDS] = {1, 1, 1, 1, 1};
 
-static int events_per_block(int kind) {
-  return kind == SMEAR_NONE ? EV_WARPS * UNSMEARED_PER_WARP : EV_WARPS * SMEARED_PER_WARP;
-}
+static int events_per_block(int kind) { return kind == SMEAR_NONE ? EV_WARPS * UNSMEARED_PER_WARP : EV_WARPS; }
 
 int segment_blocks(const Segment& s, int sm_count) {
   const int per = events_per_block(s.kind);
@@ -1002,6 +1040,43 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
         }
     T->pc_mmask[0] |= gr.mmask[0];
     T->pc_mmask[1] |= gr.mmask[1];
+  }
+  // plane slots the amplitude reads: masses and weight, the Lambda* angular factors and the
+  // d-functions of the spins in use for the helicity slots in use, likewise for Pc and Zcs
+  {
+    bool use[SLOT_ALL] = {};
+    use[0] = use[1] = use[2] = true;
+    const int lm = T->lstar_mmask[0] | T->lstar_mmask[1];
+    for (int r = 0; r < NR; ++r)
+      for (int k = 0; k < 2; ++k)
+        for (int m = 0; m < 6; ++m)
+          if (lm >> m & 1) {
+            for (int ij = 0; ij < 4; ++ij) use[3 + ((ij >> 1) * 12 + (ij & 1) * 6 + m) * 2] =
+                use[4 + ((ij >> 1) * 12 + (ij & 1) * 6 + m) * 2] = true;
+            use[51 + T->L[r].sidx * 12 + k * 6 + m] = true;
+          }
+    const int pm = T->pc_mmask[0] | T->pc_mmask[1];
+    for (int i = 0; i < NZ; ++i)
+      for (int k = 0; k < 2; ++k)
+        for (int m = 0; m < 12; ++m)
+          if (pm >> m & 1) {
+            for (int ij = 0; ij < 4; ++ij) use[SLOT_PP1 + ((ij >> 1) * 24 + (ij & 1) * 12 + m) * 2] =
+                use[SLOT_PP1 + 1 + ((ij >> 1) * 24 + (ij & 1) * 12 + m) * 2] = true;
+            use[SLOT_PP2 + T->Z[i].sidx * 24 + k * 12 + m] = true;
+          }
+    if (NX > 0) use[SLOT_PP3] = true;
+    const int xm = T->x_mmask[0] | T->x_mmask[1];
+    for (int x = 0; x < NX; ++x)
+      for (int k = 0; k < 2; ++k)
+        for (int m = 0; m < 12; ++m)
+          if (xm >> m & 1) {
+            for (int ij = 0; ij < 4; ++ij) use[SLOT_PP3 + 1 + ((ij >> 1) * 24 + (ij & 1) * 12 + m) * 2] =
+                use[SLOT_PP3 + 2 + ((ij >> 1) * 24 + (ij & 1) * 12 + m) * 2] = true;
+            use[SLOT_PP4 + T->X[x].sidx * 24 + k * 12 + m] = true;
+          }
+    T->nstage = 0;
+    for (int i = 0; i < SLOT_ALL; ++i)
+      if (use[i]) T->stage[T->nstage++] = (short)i;
   }
   // table grid and guard intervals (tables stay disabled until the caller attaches table memory)
   LineTables& tb = T->tab;

@@ -119,6 +119,9 @@ constexpr size_t TAB_BYTES_BLOCKS = tab_align((size_t)(TAB_MAX_BLOCKS + 1) * 4);
 constexpr size_t TAB_BYTES =
     TAB_BYTES_DATA + TAB_BYTES_CELL + TAB_BYTES_SUB + TAB_BYTES_SUB_BAD + TAB_BYTES_BLOCKS;
 
+// Plane slots of one event staged in shared memory (as doubles): pp 111, pp1 96, pp2 96, pp3 97, pp4 96.
+constexpr int SLOT_PP = 0, SLOT_PP1 = 111, SLOT_PP2 = 207, SLOT_PP3 = 303, SLOT_PP4 = 400, SLOT_ALL = 496;
+
 struct alignas(16) PointTable {
   int NR, NZ, ngroups;
   int status;  // 0 ok, else a PWA_E_* code
@@ -139,6 +142,9 @@ struct alignas(16) PointTable {
   PcGroup grp[MAX_GROUPS];
   int order[MAX_PC];  // Pc entries in group order
   LineTables tab;
+  // the plane slots this point's amplitude reads (kernels that stage an event copy only these)
+  int nstage;
+  short stage[SLOT_ALL];
 };
 
 }  // namespace pwa
