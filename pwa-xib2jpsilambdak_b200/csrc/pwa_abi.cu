@@ -541,7 +541,7 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
 
 // Lineshape tables for at most this many points of a batch that move a Pc lineshape; further such
 // points are evaluated one by one.
-constexpr int BATCH_MAX_TABLES = 48;
+constexpr int BATCH_MAX_TABLES = 128;
 
 int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_stride, int para_size,
                            int vamp_size, int spline_size, int NR, int NZ, int NX, float FFR, float FFB,

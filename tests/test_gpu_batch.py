@@ -40,9 +40,9 @@ def _check_batch(ctx, name, nd, nm, tables=True, seed=0):
                                         ("full_bw", 800, 8000)])
 def test_gradient_batch_matches_single_points(ctx, name, nd, nm):
     labels, blocks, res, nstruct, smp = _check_batch(ctx, name, nd, nm)
-    # every point of these models moves one part of the amplitude; beyond 48 points that move a Pc
-    # lineshape (each needs its own table) the rest go through the single-point path
-    assert nstruct >= min(len(blocks), len(blocks) - 2 * 28 + 48), (nstruct, len(blocks))
+    # every point of these models moves one part of the amplitude, and the points that move a Pc
+    # lineshape (each with its own table, at most 128 per batch) are fewer than the table limit
+    assert nstruct == len(blocks), (nstruct, len(blocks))
 
 
 def test_gradient_batch_exact_lineshapes(ctx):
