@@ -45,7 +45,7 @@ __host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
   L.rs = L.nzp + 1;
   size_t o = 0;
   L.bs = o;
-  o = bal16(o + N_PLANES * sizeof(float));
+  o = bal16(o + N_PLANES * sizeof(double));
   L.q0 = o;
   o = bal16(o + (size_t)(NR > 0 ? NR : 1) * sizeof(cplx));
   L.f0 = o;
@@ -72,20 +72,20 @@ __host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
 
 // Event accessors on the staged planes.
 struct StagedEv {
-  const float* s;
-  __device__ __forceinline__ double mkp() const { return (double)s[0]; }
-  __device__ __forceinline__ double mz() const { return (double)s[1]; }
+  const double* s;
+  __device__ __forceinline__ double mkp() const { return s[0]; }
+  __device__ __forceinline__ double mz() const { return s[1]; }
   __device__ __forceinline__ float w() const { return s[2]; }
   __device__ __forceinline__ cplx A(int i, int j, int m) const {
     const int a = 3 + (i * 12 + j * 6 + m) * 2;
-    return mk((double)s[a], (double)s[a + 1]);
+    return mk(s[a], s[a + 1]);
   }
-  __device__ __forceinline__ double DL(int sx, int k, int m) const { return (double)s[51 + sx * 12 + k * 6 + m]; }
+  __device__ __forceinline__ double DL(int sx, int k, int m) const { return s[51 + sx * 12 + k * 6 + m]; }
   __device__ __forceinline__ cplx AZ(int i, int j, int m) const {
     const int a = 111 + (i * 24 + j * 12 + m) * 2;
-    return mk((double)s[a], (double)s[a + 1]);
+    return mk(s[a], s[a + 1]);
   }
-  __device__ __forceinline__ double DZ(int sx, int k, int m) const { return (double)s[207 + sx * 24 + k * 12 + m]; }
+  __device__ __forceinline__ double DZ(int sx, int k, int m) const { return s[207 + sx * 24 + k * 12 + m]; }
 };
 
 // f_r[h] = sum_m c_rkm A_ijm DL_{s_r,k,m} for helicity h = (i, j, k).
@@ -121,14 +121,20 @@ __device__ __forceinline__ bool group_lineshapes(const PointTable& T, int g, dou
   TabAt ta;
   if (tab_at(T.tab, m, ta)) {
 #pragma unroll
-    for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) out[q] = q < cnt ? tab_get(ta, T.tab.stride, first + q) : mk(0, 0);
+    for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) {
+      if (q >= cnt) break;
+      out[q] = tab_get(ta, T.tab.stride, first + q);
+    }
     return true;
   }
   if (!FIX) return false;
   cplx ex[MAX_GROUP_ENTRIES];
   pc_group_exact(T, g, pc_kin(T, m), ex);
 #pragma unroll
-  for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) out[q] = q < cnt ? ex[q] : mk(0, 0);
+  for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) {
+    if (q >= cnt) break;
+    out[q] = ex[q];
+  }
   return true;
 }
 
@@ -169,7 +175,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   const BatchLayout Ly = batch_layout(NR, NZ, npts);
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   unsigned char* wb = sm + warp * Ly.warp_bytes;
-  float* bs = reinterpret_cast<float*>(wb + Ly.bs);
+  double* bs = reinterpret_cast<double*>(wb + Ly.bs);
   cplx* q0 = reinterpret_cast<cplx*>(wb + Ly.q0);
   cplx* f0 = reinterpret_cast<cplx*>(wb + Ly.f0);  // [r][h]
   cplx* hl0 = reinterpret_cast<cplx*>(wb + Ly.hl0);
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
       const float* src = i < 111 ? ev.pp + (int64_t)i * ev.n_size
                                  : (i < 207 ? ev.pp1 + (int64_t)(i - 111) * ev.n_size
                                             : ev.pp2 + (int64_t)(i - 207) * ev.n_size);
-      bs[i] = __ldg(src + e);
+      bs[i] = (double)__ldg(src + e);
     }
     __syncwarp();
     const double mkp = E.mkp(), mz = E.mz();
@@ -313,14 +319,17 @@ __global__ void __launch_bounds__(BATCH_THREADS)
               int pos[BATCH_MAXQ];
 #pragma unroll
               for (int u = 0; u < BATCH_MAXQ; ++u) {
-                pos[u] = u < nq ? bp.qpos[u] : 0;
-                d[u] = u < nq ? pc_angular(bp.dc + u * 24, bp.qsidx[u], E, h) : mk(0, 0);
+                if (u >= nq) break;
+                pos[u] = bp.qpos[u];
+                d[u] = pc_angular(bp.dc + u * 24, bp.qsidx[u], E, h);
               }
               for (int b = 0; b < rows; ++b) {
                 cplx sv = S0[b * 9 + h];
 #pragma unroll
-                for (int u = 0; u < BATCH_MAXQ; ++u)
-                  if (u < nq) cmac(sv, R[b * rs + pos[u]], d[u]);
+                for (int u = 0; u < BATCH_MAXQ; ++u) {
+                  if (u >= nq) break;
+                  cmac(sv, R[b * rs + pos[u]], d[u]);
+                }
                 if (NB == 0) {
                   a1[h] = sv;
                 } else if (l0 + b < shift) {
@@ -348,12 +357,14 @@ __global__ void __launch_bounds__(BATCH_THREADS)
 #pragma unroll
               for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
                 if (q < cnt) dr[q] -= R[b * rs + first + q];
+                else break;
 #pragma unroll
               for (int h = 0; h < 8; ++h) {
                 cplx sv = S0[b * 9 + h];
 #pragma unroll
                 for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
                   if (q < cnt) cmac(sv, dr[q], hz[(first + q) * 8 + h]);
+                  else break;
                 if (NB == 0) {
                   a1[h] = sv;
                 } else if (l < shift) {
