@@ -571,10 +571,13 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   }
   if (n_structured) *n_structured = (int)sidx.size();
   // lanes of a warp take consecutive points: order them by kind (and group / entry count) so that a
-  // warp's 32 points follow one code path
+  // warp's 32 points follow one code path; the costliest kind (lineshape points, a pass over the
+  // offset rows each) first, so that its points fill whole warps and the partly filled last warp
+  // holds cheap points
+  auto rank = [](int kind) { return kind == BP_PCG ? 0 : kind == BP_PCC ? 1 : kind == BP_LSTAR ? 2 : 3; };
   std::stable_sort(sidx.begin(), sidx.end(), [&](int a, int b) {
     const BatchPoint &x = bp[a], &y = bp[b];
-    if (x.kind != y.kind) return x.kind < y.kind;
+    if (x.kind != y.kind) return rank(x.kind) < rank(y.kind);
     if (x.kind == BP_PCG) return x.group < y.group;
     if (x.kind == BP_PCC) return x.nq < y.nq;
     return false;
