@@ -36,7 +36,7 @@ constexpr int N_PLANES = 303;  // pp 111 + pp1 96 + pp2 96
 // Per-warp shared-memory layout of the batched kernel for a model with NR Lambda* and NZ Pc entries.
 struct BatchLayout {
   int nzp, rs;  // Pc entries rounded up to 4; row stride of R (odd, conflict-free row writes)
-  size_t bs, q0, f0, hl0, a10, a20, hz, R, S0, vbuf, warp_bytes, acc, total;
+  size_t bs, lk, q0, f0, hl0, a10, a20, hz, R, S0, vbuf, warp_bytes, acc, total;
 };
 __host__ __device__ inline size_t bal16(size_t x) { return (x + 15) & ~size_t(15); }
 __host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
@@ -46,6 +46,8 @@ __host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
   size_t o = 0;
   L.bs = o;
   o = bal16(o + N_PLANES * sizeof(double));
+  L.lk = o;
+  o = bal16(o + sizeof(LstarKin));
   L.q0 = o;
   o = bal16(o + (size_t)(NR > 0 ? NR : 1) * sizeof(cplx));
   L.f0 = o;
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   unsigned char* wb = sm + warp * Ly.warp_bytes;
   double* bs = reinterpret_cast<double*>(wb + Ly.bs);
+  LstarKin* lks = reinterpret_cast<LstarKin*>(wb + Ly.lk);  // the event's Lambda* kinematics
   cplx* q0 = reinterpret_cast<cplx*>(wb + Ly.q0);
   cplx* f0 = reinterpret_cast<cplx*>(wb + Ly.f0);  // [r][h]
   cplx* hl0 = reinterpret_cast<cplx*>(wb + Ly.hl0);
@@ -228,7 +231,11 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     const double mkp = E.mkp(), mz = E.mz();
     const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
     // centre: Lambda* lineshapes, f_r[h], H_L[h]; Pc angular amplitudes HZ_q[h]
-    if (lane < NR) q0[lane] = lstar_lineshape(T0.L[lane], lstar_kin(T0, mkp));
+    if (lane < NR || lane == 0) {
+      const LstarKin lk = lstar_kin(T0, mkp);
+      if (lane < NR) q0[lane] = lstar_lineshape(T0.L[lane], lk);
+      if (lane == 0) *lks = lk;
+    }
     __syncwarp();
     {
       cplx hl = mk(0, 0);
@@ -385,7 +392,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
           if (kind == BP_LSTAR) {
             // the kinematic inputs of the lineshapes (barrier orders, radii) equal the centre's
             const PointTable& Tp = *bp.T;
-            const LstarKin lk = lstar_kin(T0, mkp);
+            const LstarKin& lk = *lks;
             const unsigned lm = bp.lmask, lsm = bp.lsmask, lcm = bp.lcmask;
             int u = 0;
             for (int r = 0; r < NR; ++r) {
