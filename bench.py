@@ -31,8 +31,10 @@ METRIC = "NLL evals/s, 5M-event K-matrix model: batched vs plain on B200, |dNLL|
 WORKLOAD = {"name": "kmatrix", "n_data": 500_000, "n_mc": 5_000_000, "w_range": (0.2, 1.0)}
 CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
 # DRAM bytes read + written per event of a segment (table-only and exact passes together), from one
-# ncu capture of the 50k data + 500k MC case; the traffic of a launch scales with its events.
-DRAM_BYTES_PER_EVENT = {1: 1304.0}
+# ncu captures of the 50k data + 500k MC case (DRAM read + write of the table-only and the
+# exact-capable pass of the window segment); the traffic of a launch scales with its events.
+DRAM_BYTES_PER_EVENT = {1: 3120.0}
+BATCH_DRAM_BYTES_PER_EVENT = {1: 210900.0}
 
 
 def parse():
@@ -288,9 +290,13 @@ def main():
         b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         b0.record(stream)
         blaunch = 0
+        bseg = {}
         for _ in range(args.steps):
             bres, nstruct = bstep()
             blaunch += ctx.last_launches()
+            for (kind, n, _), ms in zip(ctx.segments(), ctx.batch_segment_ms()):
+                t, _ = bseg.get(kind, (0.0, n))
+                bseg[kind] = (t + ms, n)
         b1.record(stream)
         torch.cuda.synchronize(dev)
         bdev_ms = b0.elapsed_time(b1)
@@ -304,7 +310,7 @@ def main():
         idx = [0] + [labels.index((n, +1)) for n in probe if (n, +1) in labels]
         dmax = max(abs(bres[i].nll - ctx.eval_nll(gblocks[i]).nll) for i in idx)
         bat = dict(npts=npts, nstruct=nstruct, dev_ms=bdev_ms, e2e_ms=be2e_ms, launches=blaunch, dnll=dmax,
-                   nprobe=len(idx))
+                   nprobe=len(idx), seg=bseg)
     clocks = clk.stop()
     if world > 1:
         t = torch.tensor([dev_ms, e2e_ms, bat["dev_ms"] if bat else 0.0, bat["e2e_ms"] if bat else 0.0],
@@ -394,8 +400,14 @@ def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, h
     value = world * npts * args.steps / (bat["dev_ms"] / 1e3)
     e2e = world * npts * args.steps / (bat["e2e_ms"] / 1e3)
     ms_step = bat["dev_ms"] / args.steps
-    events = sample.n
-    achieved = events * req_b / (ms_step / 1e3) / 1e9
+    # dominant kernel: the batched passes of the costliest event class (CUDA events around its launches)
+    bnames = {0: "k_batch_un", 1: "k_batch<20>", 2: "k_batch<30>", 3: "k_batch<150>"}
+    seg = bat["seg"]
+    dom = max(seg, key=lambda k: seg[k][0])
+    dom_ms = seg[dom][0] / args.steps
+    dom_ev = seg[dom][1]
+    achieved = dom_ev * (req_b + 4) / (dom_ms / 1e3) / 1e9
+    tot = sum(t for t, _ in seg.values())
     keep = ("value", "ms_per_step", "gpu_launches", "kernel_shares", "segments", "roofline", "e2e")
     out = {k: v for k, v in plain.items() if k not in keep}
     out["plain"] = {k: plain[k] for k in keep if k in plain}
@@ -409,10 +421,16 @@ def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, h
                   "max_abs_dnll_vs_single_point": bat["dnll"], "probed_points": bat["nprobe"],
                   "step": "the 2N+1 parameter points of Minuit's numerical gradient (centre, +-h per parameter) "
                           "in one pwa_ctx_eval_nll_batch call; every point's NLL is computed in FP64"},
-        "roofline": {"bound": "hbm", "kernel": "k_batch (all launches of one gradient batch)",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                     "note": f"algorithmic bytes = {req_b} B per event read once per batch; FP64-issue bound, "
-                             f"peak {peak_kind}"},
+        "kernel_shares": {bnames[k]: round(t / tot, 4) for k, (t, n) in seg.items()},
+        "segments": {bnames[k]: {"events": int(n), "ms_per_step": round(t / args.steps, 3)}
+                     for k, (t, n) in seg.items()},
+        "roofline": {"bound": "hbm", "kernel": bnames[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm,
+                     "traffic": (BATCH_DRAM_BYTES_PER_EVENT[dom] * dom_ev if dom in BATCH_DRAM_BYTES_PER_EVENT
+                                 else None),
+                     "traffic_unit": "bytes per step of this segment (ncu, scaled by events)",
+                     "note": f"algorithmic bytes = {req_b} B of planes + 4 B index per event, read once per "
+                             f"batch of {npts} points; the kernel is FP64-issue bound, peak {peak_kind}"},
         "e2e": {"value": e2e, "unit": "evals/s",
                 "h2d_bytes_per_step": (npts + 1) * pt_bytes + npts * (8 * 24 * 16 + 96),
                 "d2h_bytes_per_step": npts * 48},

@@ -133,6 +133,11 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* ctx, const float* h_paraLists, int npoints, 
  * evaluated one by one). */
 double pwa_ctx_last_batch_ms(pwa_ctx* ctx);
 
+/* Device time (ms, CUDA events) of segment i's batched passes in the last pwa_ctx_eval_nll_batch with
+ * timing on (pwa_ctx_set_timing); segments as pwa_ctx_segment_info numbers them.  Diagnostic, no
+ * counterpart in the reference. */
+int pwa_ctx_batch_segment_ms(pwa_ctx* ctx, int i, double* ms);
+
 /* Sum over the MC events of w * |A|^2 (unsmeared |A|^2 as host_store_amp2s gives it, w the event weight):
  * the normalisation integral of one parameter block that the reference's fit and interference
  * fractions divide (RooDalitzAmplitude::getIFandFF, src/RooDalitzAmplitude.cxx:5250-5435, evaluated

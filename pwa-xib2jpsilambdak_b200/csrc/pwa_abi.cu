@@ -89,6 +89,8 @@ struct pwa_ctx {
   Partial* d_bparts = nullptr;
   size_t bparts_cap = 0;
   double last_batch_ms = 0;
+  std::vector<cudaEvent_t> bseg_ev;  // batched evaluation timing: start and end event per segment
+  std::vector<double> bseg_ms;       // device time per segment of the last batch call (timing on)
 };
 
 namespace {
@@ -263,6 +265,7 @@ int pwa_ctx_destroy(pwa_ctx* c) {
   cudaFree(c->d_fx);
   cudaFree(c->d_tab);
   for (auto e : c->seg_ev) cudaEventDestroy(e);
+  for (auto e : c->bseg_ev) cudaEventDestroy(e);
   if (c->e0) cudaEventDestroy(c->e0);
   if (c->e1) cudaEventDestroy(c->e1);
   if (c->st) cudaStreamDestroy(c->st);
@@ -606,6 +609,14 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   const PointTable& T0 = *c->h_table;
   const BatchGroupMap gm = batch_group_map(T0);
   int tab_slot = 0;
+  if (c->timing) {
+    while (c->bseg_ev.size() < 2 * c->segs.size()) {
+      cudaEvent_t e;
+      PWA_CUDA(cudaEventCreate(&e));
+      c->bseg_ev.push_back(e);
+    }
+  }
+  c->bseg_ms.assign(c->segs.size(), 0.0);
   for (size_t c0 = 0; c0 < sidx.size(); c0 += chunk_cap) {
     const int nc = (int)std::min<size_t>(chunk_cap, sidx.size() - c0);
     std::vector<PointTable> dt(nc);
@@ -647,8 +658,10 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     for (size_t i = 0; i < c->segs.size(); ++i) {
       int32_t* dq = tables ? c->d_defer + c->seg_defer_off[i] : nullptr;
       int* dcnt = tables ? c->d_defer_cnt + i : nullptr;
+      if (c->timing) PWA_CUDA(cudaEventRecord(c->bseg_ev[2 * i], c->st));
       PWA_CUDA(launch_batch_segment(ev, c->segs[i], c->d_table, T0, gm, c->d_bpts, nc,
                                     c->d_bparts + row_off[i] * nc, dq, dcnt, c->sm_count, c->st));
+      if (c->timing) PWA_CUDA(cudaEventRecord(c->bseg_ev[2 * i + 1], c->st));
       launches += tables ? 2 : 1;
     }
     PWA_CUDA(launch_finalize_points(c->d_bparts, (int)std::max<size_t>(rows, 1), nc, sum_w_mc, sum_w_data, nll_shift,
@@ -656,6 +669,12 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     ++launches;
     PWA_CUDA(cudaMemcpyAsync(c->h_bres, c->d_bres, nc * sizeof(EvalResult), cudaMemcpyDeviceToHost, c->st));
     PWA_CUDA(cudaStreamSynchronize(c->st));
+    if (c->timing)
+      for (size_t i = 0; i < c->segs.size(); ++i) {
+        float m = 0;
+        cudaEventElapsedTime(&m, c->bseg_ev[2 * i], c->bseg_ev[2 * i + 1]);
+        c->bseg_ms[i] += m;
+      }
     for (int j = 0; j < nc; ++j) {
       const EvalResult& r = c->h_bres[j];
       pwa_result& o = out[sidx[c0 + j]];
@@ -683,6 +702,12 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
 }
 
 double pwa_ctx_last_batch_ms(pwa_ctx* c) { return c ? c->last_batch_ms : 0.0; }
+
+int pwa_ctx_batch_segment_ms(pwa_ctx* c, int i, double* ms) {
+  if (!c || !ms || i < 0 || i >= (int)c->segs.size()) return PWA_E_ARG;
+  *ms = i < (int)c->bseg_ms.size() ? c->bseg_ms[i] : 0.0;
+  return PWA_OK;
+}
 
 int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                  float FFR, float FFB, double* h_amp2) {

@@ -297,7 +297,9 @@ __global__ void __launch_bounds__(BATCH_THREADS)
         __syncwarp();
       }
     };
-    if (nrounds == 1) centre_round(0, true);
+    // the centre's sums over all offset rows first; with several rounds the rows are recomputed
+    // below only in passes whose points read them
+    for (int rd = 0; rd < nrounds; ++rd) centre_round(rd * 32, true);
     const bool centre_fail = !FIX && __any_sync(0xffffffffu, fail);
     if (!centre_fail) {
       for (int pass = 0; pass < npts; pass += 32) {
@@ -314,9 +316,10 @@ __global__ void __launch_bounds__(BATCH_THREADS)
           a1[h] = mk(0, 0);
           a2[h] = 0;
         }
-        for (int rd = 0; rd < nrounds; ++rd) {
+        const bool need_rows = nrounds == 1 || __any_sync(0xffffffffu, kind == BP_PCC || kind == BP_PCG);
+        for (int rd = 0; need_rows && rd < nrounds; ++rd) {
           const int l0 = rd * 32;
-          if (nrounds > 1) centre_round(l0, pass == 0);
+          if (nrounds > 1) centre_round(l0, false);
           const int rows = min(32, nlook - l0);
           if (kind == BP_PCC) {
             const int nq = bp.nq;

@@ -17,7 +17,7 @@ LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().pare
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
             "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing",
-            "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
+            "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
@@ -78,6 +78,7 @@ def load() -> C.CDLL:
                                              C.c_double, C.POINTER(PwaResult), C.POINTER(C.c_int)]
         L.pwa_ctx_last_batch_ms.restype = C.c_double
         L.pwa_ctx_last_batch_ms.argtypes = [C.c_void_p]
+        L.pwa_ctx_batch_segment_ms.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
         L.pwa_ctx_last_kernel_ms.restype = C.c_double
         L.pwa_ctx_last_kernel_ms.argtypes = [C.c_void_p]
         L.pwa_ctx_last_launches.argtypes = [C.c_void_p]
@@ -259,6 +260,15 @@ class Context:
             k, n, ms = C.c_int(), C.c_int64(), C.c_double()
             check(self.L.pwa_ctx_segment_info(self.h, i, C.byref(k), C.byref(n), C.byref(ms)), "segment_info")
             out.append((k.value, n.value, ms.value))
+        return out
+
+    def batch_segment_ms(self) -> list:
+        """Device time (ms) per segment of the last batched evaluation with timing on."""
+        out = []
+        for i in range(self.L.pwa_ctx_segment_count(self.h)):
+            ms = C.c_double()
+            check(self.L.pwa_ctx_batch_segment_ms(self.h, i, C.byref(ms)), "batch_segment_ms")
+            out.append(ms.value)
         return out
 
     def segments_deferred(self) -> list:
