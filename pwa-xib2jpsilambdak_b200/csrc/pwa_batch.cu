@@ -613,10 +613,11 @@ __global__ void __launch_bounds__(BU_THREADS)
       }
     }
     if (!FIX) {
-      // a point's lineshape table must serve this mass too (checked before anything is summed)
+      // a point's lineshape table must serve this mass too (checked before anything is summed); the
+      // batch puts its lineshape points first
       for (int pi = 0; pi < npts; ++pi) {
         const BatchPoint& bp = pts[pi];
-        if (bp.kind != BP_PCG) continue;
+        if (bp.kind != BP_PCG) break;
         TabAt ta;
         fail |= !tab_at(bp.T->tab, mz, ta);
       }

@@ -129,6 +129,7 @@ int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupM
                        bool deferred);
 
 // Launches the batched passes over one segment: partial rows out[0 .. batch_segment_rows) x npts.
+// The points with kind BP_PCG must come first in d_pts.
 cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
                                  const BatchGroupMap& gm, const BatchPoint* d_pts, int npts, Partial* out,
                                  int32_t* defer, int* defer_count, int sm_count, cudaStream_t st);
