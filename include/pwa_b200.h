@@ -75,6 +75,15 @@ int pwa_ctx_set_device_events(pwa_ctx* ctx, const float* d_pp, const float* d_pp
                               const float* d_sw, int64_t n, int64_t n_size, int64_t nda, int64_t nda_smr,
                               int64_t nda_fine);
 
+/* Evaluate only the data events [first, first + n_data) (with all MC events): one toy of an ensemble
+ * whose toys' data were uploaded one after another, each sorted into its own m(J/psi p) bands, with
+ * the MC shared.  nda_smr / nda_fine are that toy's band arguments (as host_store_fx receives them),
+ * counted from `first`; the caller passes the toy's sum of data weights to pwa_ctx_eval_nll.
+ * n_data < 0 selects all data again (first ignored).  Per-event outputs hold values of the selected
+ * events only.  No counterpart in the reference, where each toy is a separate PDF object with its own
+ * upload of the same MC (gen_toys workflow). */
+int pwa_ctx_select_data(pwa_ctx* ctx, int64_t first, int64_t n_data, int64_t nda_smr, int64_t nda_fine);
+
 /* Zcs chain planes of the uploaded events (the reference's d_float_pp3 / d_float_pp4, filled from
  * cu_Jpsihh_dlz's mjpsik, AXRe/AXIm and DX members, src/RooDalitzAmplitude.cxx:564-717), needed by
  * models with Zcs entries (NX > 0).  Call after the event upload; the same n_size and event order

@@ -47,6 +47,9 @@ struct pwa_ctx {
   const float *pp3 = nullptr, *pp4 = nullptr;  // Zcs chain planes (models with Zcs entries)
   float *own_pp3 = nullptr, *own_pp4 = nullptr;
   int64_t n = 0, n_size = 0, nda = 0, nda_smr = 0, nda_fine = 0;
+  // selected data events [win_first, win_first + win_n) (win_n < 0: all data, the default); the band
+  // arguments then count from win_first
+  int64_t win_first = 0, win_n = -1;
   // resolution model: PWA_SMEAR_REFERENCE, or PWA_SMEAR_GAUSS with (offset, weight) pairs on the device
   int smear_mode = PWA_SMEAR_REFERENCE;
   double* d_grid = nullptr;
@@ -124,6 +127,8 @@ void free_events(pwa_ctx* c) {
   c->pp = c->pp1 = c->pp2 = c->sw = nullptr;
   c->order.clear();
   c->n = 0;
+  c->win_first = 0;
+  c->win_n = -1;
 }
 
 // Per-event outputs of the device order back into the caller's order (data uploaded unsorted).
@@ -142,11 +147,18 @@ int build_segments(pwa_ctx* c, const float* h_mz) {
   const int64_t n = c->n;
   if (c->smear_mode == PWA_SMEAR_GAUSS) {
     c->segs.clear();
-    if (n > 0) {
-      Segment g{SMEAR_GRID, 0, n, nullptr};
+    auto grid_segment = [&](int64_t b, int64_t e) {
+      if (e <= b) return;
+      Segment g{SMEAR_GRID, b, e, nullptr};
       g.grid = c->d_grid;
       g.grid_nb = c->grid_nb;
       c->segs.push_back(g);
+    };
+    if (c->win_n < 0) {
+      grid_segment(0, n);
+    } else {
+      grid_segment(c->win_first, c->win_first + c->win_n);
+      grid_segment(c->nda, n);
     }
   } else {
     const int rc = build_reference_segments(c, h_mz);
@@ -172,14 +184,27 @@ int build_segments(pwa_ctx* c, const float* h_mz) {
 
 int build_reference_segments(pwa_ctx* c, const float* h_mz) {
   const int64_t n = c->n;
-  const int64_t b1e = std::max<int64_t>(0, std::min(n, c->nda_smr));
-  const int64_t b2s = std::max<int64_t>(0, c->nda_smr);
-  const int64_t b2e = std::max<int64_t>(b2s, std::min(n, c->nda_smr + c->nda_fine));
-  const int64_t r0 = std::min(n, std::max<int64_t>(0, c->nda_smr + c->nda_fine));
   std::vector<int32_t> lw, lu;
-  lw.reserve(n / 4);
-  lu.reserve(n - r0);
-  for (int64_t e = r0; e < n; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+  int64_t b1s = 0, b1e, b2s, b2e;
+  if (c->win_n < 0) {
+    b1e = std::max<int64_t>(0, std::min(n, c->nda_smr));
+    b2s = std::max<int64_t>(0, c->nda_smr);
+    b2e = std::max<int64_t>(b2s, std::min(n, c->nda_smr + c->nda_fine));
+    const int64_t r0 = std::min(n, std::max<int64_t>(0, c->nda_smr + c->nda_fine));
+    lw.reserve(n / 4);
+    lu.reserve(n - r0);
+    for (int64_t e = r0; e < n; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+  } else {
+    // a window of the data: its bands counted from its first event, its tail with all MC events
+    const int64_t f = c->win_first, wn = c->win_n;
+    b1s = f;
+    b1e = f + std::max<int64_t>(0, std::min(wn, c->nda_smr));
+    b2s = f + std::max<int64_t>(0, std::min(wn, c->nda_smr));
+    b2e = std::max<int64_t>(b2s, f + std::min(wn, c->nda_smr + c->nda_fine));
+    const int64_t r0 = f + std::min(wn, std::max<int64_t>(0, c->nda_smr + c->nda_fine));
+    for (int64_t e = r0; e < f + wn; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+    for (int64_t e = c->nda; e < n; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+  }
   const size_t nl = lw.size() + lu.size();
   if (nl) {
     PWA_CUDA(cudaMalloc(&c->d_lists, nl * sizeof(int32_t)));
@@ -190,7 +215,7 @@ int build_reference_segments(pwa_ctx* c, const float* h_mz) {
   c->segs.clear();
   // heaviest work first so the long tiles start early
   if (b2e > b2s) c->segs.push_back({SMEAR_150, b2s, b2e, nullptr});
-  if (b1e > 0) c->segs.push_back({SMEAR_30, 0, b1e, nullptr});
+  if (b1e > b1s) c->segs.push_back({SMEAR_30, b1s, b1e, nullptr});
   if (!lw.empty()) c->segs.push_back({SMEAR_20, 0, (int64_t)lw.size(), c->d_lists});
   if (!lu.empty()) c->segs.push_back({SMEAR_NONE, 0, (int64_t)lu.size(), c->d_lists + lw.size()});
   return PWA_OK;
@@ -396,6 +421,21 @@ int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int ha
   c->smear_mode = mode;
   if (!c->pp) return PWA_OK;
   // re-split the uploaded events for the new model
+  free_segments(c);
+  std::vector<float> mz((size_t)std::max<int64_t>(c->n, 1));
+  if (c->n) PWA_CUDA(cudaMemcpy(mz.data(), c->pp + c->n_size, c->n * sizeof(float), cudaMemcpyDeviceToHost));
+  return build_segments(c, mz.data());
+}
+
+int pwa_ctx_select_data(pwa_ctx* c, int64_t first, int64_t n_data, int64_t nda_smr, int64_t nda_fine) {
+  if (!c) return PWA_E_ARG;
+  if (!c->pp) return PWA_E_STATE;
+  if (n_data >= 0 && (first < 0 || first + n_data > c->nda)) return PWA_E_ARG;
+  PWA_CUDA(cudaSetDevice(c->device));
+  c->win_first = n_data >= 0 ? first : 0;
+  c->win_n = n_data;
+  c->nda_smr = nda_smr;
+  c->nda_fine = nda_fine;
   free_segments(c);
   std::vector<float> mz((size_t)std::max<int64_t>(c->n, 1));
   if (c->n) PWA_CUDA(cudaMemcpy(mz.data(), c->pp + c->n_size, c->n * sizeof(float), cudaMemcpyDeviceToHost));

@@ -16,7 +16,7 @@ import os
 LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().parent / "libpwa_b200.so")))
 
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
-            "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing",
+            "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing", "pwa_ctx_select_data",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
@@ -69,6 +69,7 @@ def load() -> C.CDLL:
         L.pwa_ctx_upload_zcs_events.argtypes = [C.c_void_p, _fp, _fp]
         L.pwa_ctx_set_device_zcs_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.pwa_ctx_set_smearing.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int]
+        L.pwa_ctx_select_data.argtypes = [C.c_void_p] + [C.c_int64] * 4
         L.pwa_band_order.argtypes = [_fp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int64)]
         L.pwa_ctx_mc_integral.argtypes = [C.c_void_p, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -167,6 +168,11 @@ class Context:
         2 half_bins + 1 offsets spaced step GeV)."""
         modes = {"reference": 0, "gauss": 1}
         check(self.L.pwa_ctx_set_smearing(self.h, modes[mode], sigma, step, half_bins), "pwa_ctx_set_smearing")
+
+    def select_data(self, first: int, n_data: int, nda_smr: int, nda_fine: int):
+        """Evaluate only the data events [first, first + n_data) with all MC (pwa_ctx_select_data);
+        n_data < 0 selects all data again."""
+        check(self.L.pwa_ctx_select_data(self.h, first, n_data, nda_smr, nda_fine), "pwa_ctx_select_data")
 
     def upload_unsorted(self, sample):
         """Upload a Sample whose data events are in any order (pwa_ctx_upload_events_unsorted): the
