@@ -101,7 +101,7 @@ int pwa_ctx_set_device_zcs_events(pwa_ctx* ctx, const float* d_pp3, const float*
  * with a Gaussian of width sigma (GeV) sampled on offsets (b - half_bins) * step, b = 0 .. 2 half_bins
  * (at most 127 offsets), weights exp(-offset^2 / 2 sigma^2) normalised to 1: |A|^2 =
  * sum_b w_b |A(m + offset_b)|^2; the band arguments are then unused.  Applies to the uploaded
- * events and later uploads; the batch call evaluates point by point in PWA_SMEAR_GAUSS mode. */
+ * events and later uploads, and to the single-point and the batch call alike. */
 #define PWA_SMEAR_REFERENCE 0
 #define PWA_SMEAR_GAUSS 1
 int pwa_ctx_set_smearing(pwa_ctx* ctx, int mode, double sigma, double step, int half_bins);

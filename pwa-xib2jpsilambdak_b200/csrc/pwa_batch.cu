@@ -161,16 +161,17 @@ __device__ __forceinline__ const float* batch_offsets() {
   }
 }
 
-// NB = 0: unsmeared events (row 0 = the event mass).  NB > 0: NB resolution offsets; band 0 (tail
-// window events) adds row 0 at the event mass for the non-interfering MC term, band 1 (data bands)
-// does not.  FIX = false: table lookups only, events with a mass no table can serve (centre or a
+// NB > 0: NB resolution offsets (the reference's quantile schemes); band 0 (tail window events) adds
+// row 0 at the event mass for the non-interfering MC term, band 1 (data bands) does not.  NB = 0: the
+// weighted grid scheme of the Gaussian resolution model (grid[2b] absolute offset, grid[2b+1] weight,
+// grid_nb offsets, band 0).  FIX = false: table lookups only, events with a mass no table can serve (centre or a
 // lineshape point's) are appended to defer[]; FIX = true evaluates those masses exactly and runs over
 // the deferred list (events [0, *n_list)) or, without tables, over the whole segment.
 template <int NB, bool FIX>
 __global__ void __launch_bounds__(BATCH_THREADS)
     k_batch(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
             const PointTable* __restrict__ T0p, const BatchPoint* __restrict__ pts, int npts, Partial* parts,
-            int band, int32_t* defer, int* defer_count) {
+            int band, int32_t* defer, int* defer_count, const double* __restrict__ grid, int grid_nb) {
   extern __shared__ __align__(16) unsigned char sm[];
   const PointTable& T0 = *T0p;
   const int NR = T0.NR, NZ = T0.NZ;
@@ -195,11 +196,18 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   const StagedEv E{bs};
   const int h8 = lane & 7, part = lane >> 3;
   const float* qoff = batch_offsets<NB>();
+  constexpr bool GRID = NB == 0;
   const float wf = (float)(1.0 / (NB > 0 ? NB : 1));
-  const double wgt = wf;
-  const double c2 = wgt * wgt * (double)(1.0f / wf);
-  const int shift = (NB == 0 || band == 0) ? 1 : 0;  // row 0 at the event mass
-  const int nlook = (NB == 0) ? 1 : NB + shift;
+  const double wgt = GRID ? 1.0 : (double)wf;
+  const double c2 = GRID ? 1.0 : wgt * wgt * (double)(1.0f / wf);
+  const int shift = band == 0 ? 1 : 0;  // row 0 at the event mass
+  const int nlook = (GRID ? grid_nb : NB) + shift;
+  // mass and weight of lookup row l (row l < shift: the event mass)
+  auto row_mass = [&](int l, double mz, double mres) {
+    const int b = l - shift;
+    return b < 0 ? mz : GRID ? mz + __ldg(grid + 2 * b) : mz + (double)qoff[b] * mres;
+  };
+  auto row_weight = [&](int l) { return GRID ? __ldg(grid + 2 * (l - shift) + 1) : 1.0; };
   const int nrounds = (nlook + 31) / 32;
   const int nzp = Ly.nzp, rs = Ly.rs;
 
@@ -257,8 +265,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
       const int l = l0 + lane;
       cplx* row = R + lane * rs;
       if (l < nlook) {
-        const int b = l - shift;
-        const double m = b < 0 ? mz : mz + (double)qoff[b] * mres;
+        const double m = row_mass(l, mz, mres);
         if (FIX)
           lookup_entries(T0, m, row);
         else
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
         S0[lane * 9 + h] = s;
       }
       __syncwarp();
-      if (sums && NB > 0) {
+      if (sums) {
         // lane (h, part) sums the offset rows b = part, part + 4, ... of this round
         cplx a1 = mk(0, 0);
         double a2 = 0;
@@ -283,8 +290,9 @@ __global__ void __launch_bounds__(BATCH_THREADS)
           const int ll = l0 + b;
           if (ll < shift || ll >= nlook) continue;
           const cplx s = S0[b * 9 + h8];
-          a1 += s;
-          a2 += norm2(s);
+          const double wb = row_weight(ll);
+          a1 += wb * s;
+          a2 += wb * norm2(s);
         }
         a1 += shfl_xor(a1, 8);
         a1 += shfl_xor(a1, 16);
@@ -340,13 +348,12 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                   if (u >= nq) break;
                   cmac(sv, R[b * rs + pos[u]], d[u]);
                 }
-                if (NB == 0) {
-                  a1[h] = sv;
-                } else if (l0 + b < shift) {
+                if (l0 + b < shift) {
                   vns += norm2(sv);
                 } else {
-                  a1[h] += sv;
-                  a2[h] += norm2(sv);
+                  const double wb = row_weight(l0 + b);
+                  a1[h] += wb * sv;
+                  a2[h] += wb * norm2(sv);
                 }
               }
             }
@@ -356,8 +363,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
             const int first = Tp.grp[g].first, cnt = Tp.grp[g].count;
             for (int b = 0; b < rows; ++b) {
               const int l = l0 + b;
-              const int bo = l - shift;
-              const double m = (NB == 0 || bo < 0) ? mz : mz + (double)qoff[bo] * mres;
+              const double m = row_mass(l, mz, mres);
               cplx dr[MAX_GROUP_ENTRIES];
               if (!group_lineshapes<FIX>(Tp, g, m, dr)) {
                 fail = true;
@@ -375,13 +381,12 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                 for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
                   if (q < cnt) cmac(sv, dr[q], hz[(first + q) * 8 + h]);
                   else break;
-                if (NB == 0) {
-                  a1[h] = sv;
-                } else if (l < shift) {
+                if (l < shift) {
                   vns += norm2(sv);
                 } else {
-                  a1[h] += sv;
-                  a2[h] += norm2(sv);
+                  const double wb = row_weight(l);
+                  a1[h] += wb * sv;
+                  a2[h] += wb * norm2(sv);
                 }
               }
             }
@@ -422,23 +427,17 @@ __global__ void __launch_bounds__(BATCH_THREADS)
               }
             }
           }
-          if (!own && NB > 0 && shift) {
+          if (!own && shift) {
 #pragma unroll
             for (int h = 0; h < 8; ++h) vns += norm2(S0[h]);
           }
-          double v = 0, vn = (NB > 0) ? vns : 0.0;
+          double v = 0, vn = vns;
 #pragma unroll
           for (int h = 0; h < 8; ++h) {
-            if (NB == 0) {
-              const cplx hzp = own ? a1[h] : S0[h];
-              v += norm2(hlp[h] + hzp);
-              vn += norm2(hlp[h]) + norm2(hzp);
-            } else {
-              const cplx s1 = own ? a1[h] : a10[h];
-              const double s2 = own ? a2[h] : a20[h];
-              v += norm2(hlp[h]) + 2.0 * wgt * (hlp[h].re * s1.re + hlp[h].im * s1.im) + c2 * s2;
-              vn += norm2(hlp[h]);
-            }
+            const cplx s1 = own ? a1[h] : a10[h];
+            const double s2 = own ? a2[h] : a20[h];
+            v += norm2(hlp[h]) + 2.0 * wgt * (hlp[h].re * s1.re + hlp[h].im * s1.im) + c2 * s2;
+            vn += norm2(hlp[h]);
           }
           vbuf[pidx * 2] = v;
           vbuf[pidx * 2 + 1] = vn;
@@ -454,7 +453,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
       for (int pi = lane; pi < npts; pi += 32) {
         const double v = vbuf[pi * 2], vn = vbuf[pi * 2 + 1];
         double fxe = v, vnw = 0;
-        if (!(NB > 0 && band) && !data_w) {
+        if (!band && !data_w) {
           fxe = v * (double)wfe;
           vnw = vn * (double)wfe;
         }
@@ -464,7 +463,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
           atomicAdd(a + 0, (fxe > 0) ? log(fxe) * (double)__ldg(ev.sw + e) : -1e12);
         } else {
           atomicAdd(a + 1, fxe);
-          if (!(NB > 0 && band)) atomicAdd(a + 2, vnw);
+          if (!band) atomicAdd(a + 2, vnw);
         }
       }
     }
@@ -759,7 +758,8 @@ cudaError_t configure_batch_kernels() {
   optin -= 1024;  // the kernels' static shared memory stays below 1 KB
   if ((e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
       (e = set_batch_smem<30, false>(optin)) || (e = set_batch_smem<30, true>(optin)) ||
-      (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)))
+      (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)) ||
+      (e = set_batch_smem<0, false>(optin)) || (e = set_batch_smem<0, true>(optin)))
     return e;
   if ((e = cudaFuncSetAttribute(k_batch_un<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
       (e = cudaFuncSetAttribute(k_batch_un<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)))
@@ -877,7 +877,11 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
   return true;
 }
 
-static int batch_nb(int kind) { return kind == SMEAR_20 ? 20 : kind == SMEAR_30 ? 30 : kind == SMEAR_150 ? 150 : 0; }
+// Offsets of a segment's smearing scheme for the batched kernels: 0 unsmeared (k_batch_un), -1 the
+// weighted grid (k_batch<0>), else the quantile scheme's NB.
+static int batch_nb(int kind) {
+  return kind == SMEAR_20 ? 20 : kind == SMEAR_30 ? 30 : kind == SMEAR_150 ? 150 : kind == SMEAR_GRID ? -1 : 0;
+}
 
 static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count) {
   const int64_t n = s.end - s.begin;
@@ -893,6 +897,7 @@ static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMa
     switch (batch_nb(s.kind)) {
       case 20: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<20, false>, BATCH_THREADS, smem); break;
       case 30: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<30, false>, BATCH_THREADS, smem); break;
+      case -1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<0, false>, BATCH_THREADS, smem); break;
       default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<150, false>, BATCH_THREADS, smem); break;
     }
   }
@@ -912,20 +917,22 @@ int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupM
 template <int NB>
 static void launch_batch_kind(const EventSet& ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
                               const PointTable* d_T0, const BatchPoint* d_pts, int npts, Partial* out, int band,
-                              int32_t* defer, int* defer_count, bool fix, int grid, size_t smem, cudaStream_t st) {
+                              int32_t* defer, int* defer_count, bool fix, int grid, size_t smem, cudaStream_t st,
+                              const double* sgrid, int sgrid_nb) {
   if (fix)
     k_batch<NB, true><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
-                                                         defer, defer_count);
+                                                         defer, defer_count, sgrid, sgrid_nb);
   else
     k_batch<NB, false><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
-                                                          defer, defer_count);
+                                                          defer, defer_count, sgrid, sgrid_nb);
 }
 
 static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t end, const int32_t* list,
                             const int* n_list, const PointTable* d_T0, const BatchGroupMap& gm,
-                            const BatchPoint* d_pts, int npts, Partial* out,
-                            int band, int32_t* defer, int* defer_count, bool fix, int grid, size_t smem,
-                            cudaStream_t st) {
+                            const BatchPoint* d_pts, int npts, Partial* out, int band, int32_t* defer,
+                            int* defer_count, bool fix, int grid, size_t smem, cudaStream_t st, const Segment& seg) {
+  const double* sg = seg.grid;
+  const int sn = seg.grid_nb;
   switch (nb) {
     case 0:
       if (fix)
@@ -935,9 +942,10 @@ static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t e
         k_batch_un<false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts, out,
                                                            defer, defer_count);
       break;
-    case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
-    case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
-    default: launch_batch_kind<150>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st); break;
+    case -1: launch_batch_kind<0>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    default: launch_batch_kind<150>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
   }
 }
 
@@ -947,18 +955,19 @@ cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const P
   if (seg.end <= seg.begin) return cudaSuccess;
   if (npts < 1 || npts > BATCH_MAX_POINTS) return cudaErrorInvalidValue;
   const int nb = batch_nb(seg.kind);
+  if (nb < 0 && (!seg.grid || seg.grid_nb < 1 || seg.grid_nb > GRID_MAX_NB)) return cudaErrorInvalidValue;
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
   const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, gm.max_slots, npts).total
                               : batch_layout(T0.NR, T0.NZ, npts).total;
   const int grid = batch_grid(seg, T0, gm, npts, sm_count);
   if (defer) {
     launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, defer,
-                    defer_count, false, grid, smem, st);
+                    defer_count, false, grid, smem, st, seg);
     launch_batch_nb(nb, ev, 0, 0, defer, defer_count, d_T0, gm, d_pts, npts, out + (size_t)grid * npts, band,
-                    nullptr, nullptr, true, grid, smem, st);
+                    nullptr, nullptr, true, grid, smem, st, seg);
   } else {
     launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, nullptr,
-                    nullptr, true, grid, smem, st);
+                    nullptr, true, grid, smem, st, seg);
   }
   return cudaGetLastError();
 }

@@ -161,17 +161,20 @@ def test_gaussian_grid_smearing_matches_oracle(ctx, oracle_mod, name):
     assert ctx.eval_nll(blk).nll == r_ref.nll
 
 
-def test_gaussian_grid_batch_and_arguments(ctx):
+@pytest.mark.parametrize("name", ["small_kmatrix", "full_bw"])
+def test_gaussian_grid_batch_and_arguments(ctx, name):
+    """Gaussian resolution model: the batched gradient (every point formed from the centre) against
+    one-by-one evaluation, and argument checks."""
     from pwa_b200 import gradient, lib
-    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    mdl, vals, blk, smp = make_test_sample(name, 1500, 15000)
     ctx.upload(smp)
     ctx.set_smearing("gauss", 0.0027, 0.0005, 17)
     try:
         labels, blocks = gradient.gradient_blocks(mdl, vals)
-        res, nstruct = ctx.eval_nll_batch(blocks[:9])
-        assert nstruct == 0
-        for r, b in zip(res, blocks[:9]):
-            assert r.nll == ctx.eval_nll(b).nll
+        res, nstruct = ctx.eval_nll_batch(blocks)
+        assert nstruct == len(blocks)  # the batched kernels take the weighted grid too
+        for r, b in zip(res, blocks):
+            assert abs(r.nll - ctx.eval_nll(b).nll) < NLL_TOL
         with pytest.raises(lib.PwaError):
             ctx.set_smearing("gauss", 0.0027, 0.0005, 64)  # 129 offsets
         with pytest.raises(lib.PwaError):
