@@ -29,6 +29,16 @@ sys.path.insert(0, str(ROOT / "pwa-xib2jpsilambdak_b200"))
 
 METRIC = "NLL evals/s, 5M-event K-matrix model: batched vs plain on B200, |dNLL|<=1e-4"
 WORKLOAD = {"name": "kmatrix", "n_data": 500_000, "n_mc": 5_000_000, "w_range": (0.2, 1.0)}
+# --workload full_bw: the full Breit-Wigner model (14 Lambda* up to J = 7/2, 3 narrow Pc) with the
+# fixed-width Gaussian resolution (2.7 MeV on a 0.5 MeV grid) on 100k data + 1M MC events
+WORKLOADS = {
+    "kmatrix": dict(WORKLOAD, smearing=None,
+                    text="kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant)"),
+    "full_bw": dict(name="full_bw", n_data=100_000, n_mc=1_000_000, w_range=(0.2, 1.0),
+                    smearing=("gauss", 0.0027, 0.0005, 17),
+                    text="full_bw: 14 Lambda* BW (J <= 7/2) + 3 narrow Pc BW, Gaussian resolution 2.7 MeV on "
+                         "a 0.5 MeV grid"),
+}
 CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
 # DRAM bytes read + written per event of a segment (table-only and exact passes together), from one
 # ncu captures of the 50k data + 500k MC case (DRAM read + write of the table-only and the
@@ -47,6 +57,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
     ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
+                    help="kmatrix (the headline workload) or full_bw (the Breit-Wigner model with the "
+                         "Gaussian resolution)")
     return ap.parse_args()
 
 
@@ -184,7 +197,9 @@ def reference_arm(args):
     scale = (WORKLOAD["n_data"] + WORKLOAD["n_mc"]) / (nd + nm)
     value = 1.0 / (dt * scale)
     cores = os.cpu_count()
-    out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+    metric = METRIC if args.workload == "kmatrix" else ("NLL evals/s, 1M-event full Breit-Wigner model with Gaussian "
+                                                         "resolution: batched vs plain on B200")
+    out = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": dt * scale * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
            "config": {"workload": "kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
@@ -215,16 +230,19 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    mdl, vals = configs.kmatrix()
+    wl = WORKLOADS[args.workload]
+    mdl, vals = configs.MODELS[wl["name"]]()
     block = M.build_param_block(mdl, vals)
     frac = 10 if args.small else 1
-    nd, nm = WORKLOAD["n_data"] // frac, WORKLOAD["n_mc"] // frac
+    nd, nm = wl["n_data"] // frac, wl["n_mc"] // frac
     t_gen = time.perf_counter()
-    sample = gpu_sample.generate(block, nd, nm, WORKLOAD["w_range"], seed=1000 + rank, device=local)
+    sample = gpu_sample.generate(block, nd, nm, wl["w_range"], seed=1000 + rank, device=local)
     t_gen = time.perf_counter() - t_gen
     ctx = lib.Context(local)
     ctx.bind_device(sample)
     ctx.set_timing(True)
+    if wl["smearing"]:
+        ctx.set_smearing(*wl["smearing"])
     ctx.set_lineshape_tables(not args.exact)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     sums = torch.zeros(3, dtype=torch.float64, device=dev)
@@ -329,18 +347,21 @@ def main():
     e2e = world * args.steps / (e2e_ms / 1e3)
     hbm, bf16, peak_kind = measured_peaks()
     req_b, full_b = required_bytes_per_event(mdl)
-    names = {0: "k_unsmeared", 1: "k_smeared<20>", 2: "k_smeared<30>", 3: "k_smeared<150>", -1: "k_build_tables"}
+    names = {0: "k_unsmeared", 1: "k_smeared<20>", 2: "k_smeared<30>", 3: "k_smeared<150>", 4: "k_smeared<grid>",
+             -1: "k_build_tables"}
     total_seg = sum(t for t, _ in seg_time.values())
     shares = {names[k]: round(t / total_seg, 4) for k, (t, n) in seg_time.items()}
     dom = max(seg_time, key=lambda k: seg_time[k][0])
     dom_ms = seg_time[dom][0] / args.steps
     dom_bytes = seg_time[dom][1] * req_b + (sample.nda * 4 if dom in (2, 3) else 0)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+    metric = METRIC if args.workload == "kmatrix" else ("NLL evals/s, 1M-event full Breit-Wigner model with Gaussian "
+                                                         "resolution: batched vs plain on B200")
+    out = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
-                                  f"{nd} data + {nm} MC events per GPU", "global_events": world * (nd + nm),
+           "config": {"workload": f"{wl['text']}, {nd} data + {nm} MC events per GPU",
+                      "global_events": world * (nd + nm),
                       "parallelism": f"dp{world} event shards, NCCL all-reduce of 3 sums per step",
                       "l2": "inputs larger than L2 (events x 828 B >> 126 MB)", "precision": "plain FP64 path",
                       "lineshapes": "exact K-matrix solves" if args.exact else "FP64 K-matrix tables, exact near "
@@ -361,7 +382,10 @@ def main():
            "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(lib.load().pwa_point_table_bytes()),
                    "d2h_bytes_per_step": 48},
            "clocks": clocks, "setup_s": round(t_gen, 2)}
-    if world == 1 and not args.no_cpu_baseline:
+    if wl["smearing"] and not args.no_cpu_baseline:
+        out["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
+                               "sample": "not timed: the reference has no Gaussian resolution model"}
+    elif world == 1 and not args.no_cpu_baseline:
         try:
             smp = cpu_sample_from_device(sample, *CPU_SAMPLE)
             t_ref = cpu_reference_seconds(smp, block)
@@ -401,7 +425,7 @@ def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, h
     e2e = world * npts * args.steps / (bat["e2e_ms"] / 1e3)
     ms_step = bat["dev_ms"] / args.steps
     # dominant kernel: the batched passes of the costliest event class (CUDA events around its launches)
-    bnames = {0: "k_batch_un", 1: "k_batch<20>", 2: "k_batch<30>", 3: "k_batch<150>"}
+    bnames = {0: "k_batch_un", 1: "k_batch<20>", 2: "k_batch<30>", 3: "k_batch<150>", 4: "k_batch<grid>"}
     seg = bat["seg"]
     dom = max(seg, key=lambda k: seg[k][0])
     dom_ms = seg[dom][0] / args.steps
