@@ -80,3 +80,44 @@ def test_toy_batched_gradient_and_fit():
         assert np.max(np.abs(fits[0].x - fits[1].x)) > 1e-4
     finally:
         ctx.close()
+
+
+def test_toy_window_under_gaussian_resolution():
+    """A toy window with the Gaussian resolution model (all events on the weighted grid) equals the same
+    toy alone, and the batch segment timing reports the window's classes."""
+    from pwa_b200 import dataset as D, lib, toys
+    mdl, vals, blk, ens = _ensemble()
+    s = ens.sample
+    ctx, solo = lib.Context(0), lib.Context(0)
+    try:
+        ctx.upload(s)
+        ctx.set_smearing("gauss", 0.0027, 0.0005, 17)
+        v = toys.select(ctx, ens, 0)
+        r = ctx.eval_nll(blk)
+        cols = np.r_[v.first:v.first + v.nda, s.nda:s.n]
+        n = len(cols)
+        ns1 = (n // 32 + 1) * 32
+        planes = []
+        for p, k in ((s.pp, 111), (s.pp1, 96), (s.pp2, 96)):
+            a = np.zeros((k, ns1), np.float32)
+            a[:, :n] = np.asarray(p, np.float32).reshape(k, s.n_size)[:, cols]
+            planes.append(a.reshape(-1))
+        sw = np.zeros(ns1, np.float32)
+        sw[:v.nda] = np.asarray(s.sw, np.float32)[v.first:v.first + v.nda]
+        alone = D.Sample(planes[0], planes[1], planes[2], sw, n, ns1, v.nda, v.nda_smr1, v.nda_fine, s.sum_w_mc,
+                         v.sum_w_data, v.sum_w2_data)
+        solo.upload(alone)
+        solo.set_smearing("gauss", 0.0027, 0.0005, 17)
+        solo.sample = alone
+        assert abs(r.nll - solo.eval_nll(blk).nll) < NLL_TOL
+        # per-segment device time of a batched call
+        from pwa_b200 import gradient
+        labels, blocks = gradient.gradient_blocks(mdl, vals)
+        ctx.set_timing(True)
+        ctx.eval_nll_batch(blocks[:20])
+        ms = ctx.batch_segment_ms()
+        assert len(ms) == len(ctx.segments()) == 2 and all(m > 0 for m in ms)
+        assert sum(ms) <= ctx.last_batch_ms() + 1e-3
+    finally:
+        ctx.close()
+        solo.close()
