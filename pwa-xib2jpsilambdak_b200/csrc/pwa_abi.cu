@@ -606,8 +606,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   std::vector<int> sidx, fidx;
   int ntab = 0;
   for (int p = 0; p < npoints; ++p) {
-    // the structured kernels carry no Zcs terms: models with Zcs entries take the single-point path
-    bool ok = NX == 0 && classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
+    bool ok = classify_point(H[0], H[p], &bp[p], dch.data() + (size_t)p * 8 * 24);
     if (ok && bp[p].kind == BP_PCG && c->use_tables) ok = ntab++ < BATCH_MAX_TABLES;
     (ok ? sidx : fidx).push_back(p);
   }

@@ -17,464 +17,17 @@
 // BW1/BW2 form, kernel_calEva.cu:676-810).  Points that differ from the centre in anything else are
 // evaluated by the single-point path.
 //
-// Work split: one warp per event.  The warp stages the event's 303 basis planes in shared memory,
+// The smeared classes' kernel k_batch (pwa_batch_smeared.cuh, one translation unit per offset scheme)
+// and the unsmeared class's k_batch_un (below).  Work split of k_batch: one warp per event.  The warp stages the event's 303 basis planes in shared memory,
 // evaluates the centre (Lambda* terms, Pc angular amplitudes HZ_q[h], the entry lineshapes R at up to
 // 32 masses per round and S_b[h] = sum_q R_q(m_b) HZ_q[h]), then each lane takes one parameter point.
 // Per-point results go to per-block FP64 sums; a finalize kernel reduces them per point.
 #include <cstring>
 #include <vector>
 
-#include "pwa_device.cuh"
+#include "pwa_batch_smeared.cuh"
 
 namespace pwa {
-
-constexpr int BATCH_WARPS = 4;
-constexpr int BATCH_THREADS = BATCH_WARPS * 32;
-constexpr int BATCH_MAXQ = 8;  // Pc entries per coupling point
-constexpr int N_PLANES = 303;  // pp 111 + pp1 96 + pp2 96
-
-// Per-warp shared-memory layout of the batched kernel for a model with NR Lambda* and NZ Pc entries.
-struct BatchLayout {
-  int nzp, rs;  // Pc entries rounded up to 4; row stride of R (odd, conflict-free row writes)
-  size_t bs, lk, q0, f0, hl0, a10, a20, hz, R, S0, vbuf, warp_bytes, acc, total;
-};
-__host__ __device__ inline size_t bal16(size_t x) { return (x + 15) & ~size_t(15); }
-__host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts) {
-  BatchLayout L;
-  L.nzp = (NZ + 3) & ~3;
-  L.rs = L.nzp + 1;
-  size_t o = 0;
-  L.bs = o;
-  o = bal16(o + N_PLANES * sizeof(double));
-  L.lk = o;
-  o = bal16(o + sizeof(LstarKin));
-  L.q0 = o;
-  o = bal16(o + (size_t)(NR > 0 ? NR : 1) * sizeof(cplx));
-  L.f0 = o;
-  o = bal16(o + (size_t)(NR > 0 ? NR : 1) * 8 * sizeof(cplx));
-  L.hl0 = o;
-  o = bal16(o + 8 * sizeof(cplx));
-  L.a10 = o;
-  o = bal16(o + 8 * sizeof(cplx));
-  L.a20 = o;
-  o = bal16(o + 8 * sizeof(double));
-  L.hz = o;
-  o = bal16(o + (size_t)(L.nzp > 0 ? L.nzp : 1) * 8 * sizeof(cplx));
-  L.R = o;
-  o = bal16(o + (size_t)32 * L.rs * sizeof(cplx));
-  L.S0 = o;
-  o = bal16(o + (size_t)32 * 9 * sizeof(cplx));
-  L.vbuf = o;
-  o = bal16(o + (size_t)npts * 2 * sizeof(double));
-  L.warp_bytes = o;
-  L.acc = BATCH_WARPS * L.warp_bytes;
-  L.total = L.acc + (size_t)npts * 4 * sizeof(double);
-  return L;
-}
-
-// Event accessors on the staged planes.
-struct StagedEv {
-  const double* s;
-  __device__ __forceinline__ double mkp() const { return s[0]; }
-  __device__ __forceinline__ double mz() const { return s[1]; }
-  __device__ __forceinline__ float w() const { return s[2]; }
-  __device__ __forceinline__ cplx A(int i, int j, int m) const {
-    const int a = 3 + (i * 12 + j * 6 + m) * 2;
-    return mk(s[a], s[a + 1]);
-  }
-  __device__ __forceinline__ double DL(int sx, int k, int m) const { return s[51 + sx * 12 + k * 6 + m]; }
-  __device__ __forceinline__ cplx AZ(int i, int j, int m) const {
-    const int a = 111 + (i * 24 + j * 12 + m) * 2;
-    return mk(s[a], s[a + 1]);
-  }
-  __device__ __forceinline__ double DZ(int sx, int k, int m) const { return s[207 + sx * 24 + k * 12 + m]; }
-};
-
-// f_r[h] = sum_m c_rkm A_ijm DL_{s_r,k,m} for helicity h = (i, j, k).
-__device__ __forceinline__ cplx lstar_angular(const LstarEntry& L, const StagedEv& E, int h) {
-  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
-  cplx f = mk(0, 0);
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    const cplx c = L.c[k * 6 + m];
-    if (nonzero(c)) cmac(f, c, E.A(i, j, m) * E.DL(L.sidx, k, m));
-  }
-  return f;
-}
-
-// sum_m c_m AZ_ijm DZ_{sx,k,m} for helicity h and a 24-slot coupling array c[k * 12 + m].
-__device__ __forceinline__ cplx pc_angular(const cplx* c, int sx, const StagedEv& E, int h) {
-  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
-  cplx v = mk(0, 0);
-#pragma unroll
-  for (int m = 0; m < 12; ++m) {
-    const cplx cc = c[k * 12 + m];
-    if (nonzero(cc)) cmac(v, cc, E.AZ(i, j, m) * E.DZ(sx, k, m));
-  }
-  return v;
-}
-
-// Lineshape of every entry of group g at mass m from the point's table (false when it cannot serve
-// m), or exactly.
-template <bool FIX>
-__device__ __forceinline__ bool group_lineshapes(const PointTable& T, int g, double m, cplx (&out)[MAX_GROUP_ENTRIES]) {
-  const PcGroup& gr = T.grp[g];
-  const int first = gr.first, cnt = gr.count;
-  TabAt ta;
-  if (tab_at(T.tab, m, ta)) {
-#pragma unroll
-    for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) {
-      if (q >= cnt) break;
-      out[q] = tab_get(ta, T.tab.stride, first + q);
-    }
-    return true;
-  }
-  if (!FIX) return false;
-  cplx ex[MAX_GROUP_ENTRIES];
-  pc_group_exact(T, g, pc_kin(T, m), ex);
-#pragma unroll
-  for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) {
-    if (q >= cnt) break;
-    out[q] = ex[q];
-  }
-  return true;
-}
-
-// sum_m c[k * 6 + m] A_ijm DL_{sx,k,m} for helicity h (c: a Lambda* coupling array).
-__device__ __forceinline__ cplx lstar_angular_c(const cplx* c, int sx, const StagedEv& E, int h) {
-  const int i = h >> 2, j = (h >> 1) & 1, k = h & 1;
-  cplx f = mk(0, 0);
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    const cplx cc = c[k * 6 + m];
-    if (nonzero(cc)) cmac(f, cc, E.A(i, j, m) * E.DL(sx, k, m));
-  }
-  return f;
-}
-
-template <int NB>
-__device__ __forceinline__ const float* batch_offsets() {
-  if constexpr (NB == 0) {
-    return nullptr;
-  } else {
-    return smear_table<NB>();
-  }
-}
-
-// NB > 0: NB resolution offsets (the reference's quantile schemes); band 0 (tail window events) adds
-// row 0 at the event mass for the non-interfering MC term, band 1 (data bands) does not.  NB = 0: the
-// weighted grid scheme of the Gaussian resolution model (grid[2b] absolute offset, grid[2b+1] weight,
-// grid_nb offsets, band 0).  FIX = false: table lookups only, events with a mass no table can serve (centre or a
-// lineshape point's) are appended to defer[]; FIX = true evaluates those masses exactly and runs over
-// the deferred list (events [0, *n_list)) or, without tables, over the whole segment.
-template <int NB, bool FIX>
-__global__ void __launch_bounds__(BATCH_THREADS)
-    k_batch(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
-            const PointTable* __restrict__ T0p, const BatchPoint* __restrict__ pts, int npts, Partial* parts,
-            int band, int32_t* defer, int* defer_count, const double* __restrict__ grid, int grid_nb) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  const PointTable& T0 = *T0p;
-  const int NR = T0.NR, NZ = T0.NZ;
-  const BatchLayout Ly = batch_layout(NR, NZ, npts);
-  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
-  unsigned char* wb = sm + warp * Ly.warp_bytes;
-  double* bs = reinterpret_cast<double*>(wb + Ly.bs);
-  LstarKin* lks = reinterpret_cast<LstarKin*>(wb + Ly.lk);  // the event's Lambda* kinematics
-  cplx* q0 = reinterpret_cast<cplx*>(wb + Ly.q0);
-  cplx* f0 = reinterpret_cast<cplx*>(wb + Ly.f0);  // [r][h]
-  cplx* hl0 = reinterpret_cast<cplx*>(wb + Ly.hl0);
-  cplx* a10 = reinterpret_cast<cplx*>(wb + Ly.a10);
-  double* a20 = reinterpret_cast<double*>(wb + Ly.a20);
-  cplx* hz = reinterpret_cast<cplx*>(wb + Ly.hz);  // [q][h]
-  cplx* R = reinterpret_cast<cplx*>(wb + Ly.R);    // [row][q], stride Ly.rs
-  cplx* S0 = reinterpret_cast<cplx*>(wb + Ly.S0);  // [row][h], stride 9
-  double* vbuf = reinterpret_cast<double*>(wb + Ly.vbuf);
-  double* acc = reinterpret_cast<double*>(sm + Ly.acc);  // [p][4]
-  for (int i = threadIdx.x; i < npts * 4; i += BATCH_THREADS) acc[i] = 0.0;
-  __syncthreads();
-
-  const StagedEv E{bs};
-  const int h8 = lane & 7, part = lane >> 3;
-  const float* qoff = batch_offsets<NB>();
-  constexpr bool GRID = NB == 0;
-  const float wf = (float)(1.0 / (NB > 0 ? NB : 1));
-  const double wgt = GRID ? 1.0 : (double)wf;
-  const double c2 = GRID ? 1.0 : wgt * wgt * (double)(1.0f / wf);
-  const int shift = band == 0 ? 1 : 0;  // row 0 at the event mass
-  const int nlook = (GRID ? grid_nb : NB) + shift;
-  // mass and weight of lookup row l (row l < shift: the event mass)
-  auto row_mass = [&](int l, double mz, double mres) {
-    const int b = l - shift;
-    return b < 0 ? mz : GRID ? mz + __ldg(grid + 2 * b) : mz + (double)qoff[b] * mres;
-  };
-  auto row_weight = [&](int l) { return GRID ? __ldg(grid + 2 * (l - shift) + 1) : 1.0; };
-  const int nrounds = (nlook + 31) / 32;
-  const int nzp = Ly.nzp, rs = Ly.rs;
-
-  if (n_list) end = begin + *n_list;
-  const int64_t count = end - begin;
-  int64_t c0, c1, w0, wstep;
-  if (n_list) {
-    c0 = 0;
-    c1 = count;
-    w0 = (int64_t)blockIdx.x * BATCH_WARPS + warp;
-    wstep = (int64_t)gridDim.x * BATCH_WARPS;
-  } else {
-    int64_t chunk = (count + gridDim.x - 1) / gridDim.x;
-    c0 = (int64_t)blockIdx.x * chunk;
-    c1 = min(count, c0 + chunk);
-    w0 = warp;
-    wstep = BATCH_WARPS;
-  }
-
-  for (int64_t p = c0 + w0; p < c1; p += wstep) {
-    const int64_t e = event_index(list, begin, p);
-    for (int i = lane; i < N_PLANES; i += 32) {
-      const float* src = i < 111 ? ev.pp + (int64_t)i * ev.n_size
-                                 : (i < 207 ? ev.pp1 + (int64_t)(i - 111) * ev.n_size
-                                            : ev.pp2 + (int64_t)(i - 207) * ev.n_size);
-      bs[i] = (double)__ldg(src + e);
-    }
-    __syncwarp();
-    const double mkp = E.mkp(), mz = E.mz();
-    const double mres = MRES0 + mz * (MRES1 + mz * MRES2);
-    // centre: Lambda* lineshapes, f_r[h], H_L[h]; Pc angular amplitudes HZ_q[h]
-    if (lane < NR || lane == 0) {
-      const LstarKin lk = lstar_kin(T0, mkp);
-      if (lane < NR) q0[lane] = lstar_lineshape(T0.L[lane], lk);
-      if (lane == 0) *lks = lk;
-    }
-    __syncwarp();
-    {
-      cplx hl = mk(0, 0);
-      for (int r = part; r < NR; r += 4) {
-        const cplx f = lstar_angular(T0.L[r], E, h8);
-        f0[r * 8 + h8] = f;
-        cmac(hl, q0[r], f);
-      }
-      hl += shfl_xor(hl, 8);
-      hl += shfl_xor(hl, 16);
-      if (part == 0) hl0[h8] = hl;
-      for (int q = part; q < nzp; q += 4)
-        hz[q * 8 + h8] = q < NZ ? pc_angular(T0.Z[T0.order[q]].c, T0.Z[T0.order[q]].sidx, E, h8) : mk(0, 0);
-    }
-    __syncwarp();
-    bool fail = false;
-    // one round of centre rows: R[b][q] at lookup l0 + b, S0[b][h]; the centre's smeared sums
-    auto centre_round = [&](int l0, bool sums) {
-      const int l = l0 + lane;
-      cplx* row = R + lane * rs;
-      if (l < nlook) {
-        const double m = row_mass(l, mz, mres);
-        if (FIX)
-          lookup_entries(T0, m, row);
-        else
-          fail |= !lookup_table(T0, m, row);
-      } else {
-        for (int q = 0; q < NZ; ++q) row[q] = mk(0, 0);
-      }
-      for (int q = NZ; q < nzp; ++q) row[q] = mk(0, 0);
-      __syncwarp();
-#pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        cplx s = mk(0, 0);
-        for (int q = 0; q < NZ; ++q) cmac(s, row[q], hz[q * 8 + h]);
-        S0[lane * 9 + h] = s;
-      }
-      __syncwarp();
-      if (sums) {
-        // lane (h, part) sums the offset rows b = part, part + 4, ... of this round
-        cplx a1 = mk(0, 0);
-        double a2 = 0;
-        for (int b = part; b < 32; b += 4) {
-          const int ll = l0 + b;
-          if (ll < shift || ll >= nlook) continue;
-          const cplx s = S0[b * 9 + h8];
-          const double wb = row_weight(ll);
-          a1 += wb * s;
-          a2 += wb * norm2(s);
-        }
-        a1 += shfl_xor(a1, 8);
-        a1 += shfl_xor(a1, 16);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 8);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 16);
-        if (part == 0) {
-          a10[h8] = (l0 == 0 ? mk(0, 0) : a10[h8]) + a1;
-          a20[h8] = (l0 == 0 ? 0.0 : a20[h8]) + a2;
-        }
-        __syncwarp();
-      }
-    };
-    // the centre's sums over all offset rows first; with several rounds the rows are recomputed
-    // below only in passes whose points read them
-    for (int rd = 0; rd < nrounds; ++rd) centre_round(rd * 32, true);
-    const bool centre_fail = !FIX && __any_sync(0xffffffffu, fail);
-    if (!centre_fail) {
-      for (int pass = 0; pass < npts; pass += 32) {
-        const int pidx = pass + lane;
-        const bool act = pidx < npts;
-        const BatchPoint& bp = pts[act ? pidx : 0];
-        const int kind = act ? bp.kind : BP_SAME;
-        const bool own = kind == BP_PCC || kind == BP_PCG;  // sums over the rows are the point's own
-        cplx a1[8];
-        double a2[8];
-        double vns = 0;  // sum_h |S_0[h]|^2 at the event mass (non-interfering term, smeared band 0)
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          a1[h] = mk(0, 0);
-          a2[h] = 0;
-        }
-        const bool need_rows = nrounds == 1 || __any_sync(0xffffffffu, kind == BP_PCC || kind == BP_PCG);
-        for (int rd = 0; need_rows && rd < nrounds; ++rd) {
-          const int l0 = rd * 32;
-          if (nrounds > 1) centre_round(l0, false);
-          const int rows = min(32, nlook - l0);
-          if (kind == BP_PCC) {
-            const int nq = bp.nq;
-#pragma unroll
-            for (int h = 0; h < 8; ++h) {
-              cplx d[BATCH_MAXQ];
-              int pos[BATCH_MAXQ];
-#pragma unroll
-              for (int u = 0; u < BATCH_MAXQ; ++u) {
-                if (u >= nq) break;
-                pos[u] = bp.qpos[u];
-                d[u] = pc_angular(bp.dc + u * 24, bp.qsidx[u], E, h);
-              }
-              for (int b = 0; b < rows; ++b) {
-                cplx sv = S0[b * 9 + h];
-#pragma unroll
-                for (int u = 0; u < BATCH_MAXQ; ++u) {
-                  if (u >= nq) break;
-                  cmac(sv, R[b * rs + pos[u]], d[u]);
-                }
-                if (l0 + b < shift) {
-                  vns += norm2(sv);
-                } else {
-                  const double wb = row_weight(l0 + b);
-                  a1[h] += wb * sv;
-                  a2[h] += wb * norm2(sv);
-                }
-              }
-            }
-          } else if (kind == BP_PCG) {
-            const PointTable& Tp = *bp.T;
-            const int g = bp.group;
-            const int first = Tp.grp[g].first, cnt = Tp.grp[g].count;
-            for (int b = 0; b < rows; ++b) {
-              const int l = l0 + b;
-              const double m = row_mass(l, mz, mres);
-              cplx dr[MAX_GROUP_ENTRIES];
-              if (!group_lineshapes<FIX>(Tp, g, m, dr)) {
-                fail = true;
-#pragma unroll
-                for (int q = 0; q < MAX_GROUP_ENTRIES; ++q) dr[q] = mk(0, 0);
-              }
-#pragma unroll
-              for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
-                if (q < cnt) dr[q] -= R[b * rs + first + q];
-                else break;
-#pragma unroll
-              for (int h = 0; h < 8; ++h) {
-                cplx sv = S0[b * 9 + h];
-#pragma unroll
-                for (int q = 0; q < MAX_GROUP_ENTRIES; ++q)
-                  if (q < cnt) cmac(sv, dr[q], hz[(first + q) * 8 + h]);
-                  else break;
-                if (l < shift) {
-                  vns += norm2(sv);
-                } else {
-                  const double wb = row_weight(l);
-                  a1[h] += wb * sv;
-                  a2[h] += wb * norm2(sv);
-                }
-              }
-            }
-          }
-        }
-        // the point's Lambda* amplitudes, then |A|^2 with and without interference
-        if (act) {
-          cplx hlp[8];
-#pragma unroll
-          for (int h = 0; h < 8; ++h) hlp[h] = hl0[h];
-          if (kind == BP_LSTAR) {
-            // the kinematic inputs of the lineshapes (barrier orders, radii) equal the centre's
-            const PointTable& Tp = *bp.T;
-            const LstarKin& lk = *lks;
-            const unsigned lm = bp.lmask, lsm = bp.lsmask, lcm = bp.lcmask;
-            int u = 0;
-            for (int r = 0; r < NR; ++r) {
-              if (!(lm >> r & 1)) continue;
-              const bool ls = lsm >> r & 1, cc = lcm >> r & 1;
-              if (!ls && cc && bp.ldc) {  // couplings only: q_r * f(dc)
-                const cplx* dc = bp.dc + 24 * u++;
-#pragma unroll
-                for (int h = 0; h < 8; ++h) cmac(hlp[h], q0[r], lstar_angular_c(dc, T0.L[r].sidx, E, h));
-              } else {
-                if (cc) ++u;
-                const cplx qp = lstar_lineshape(Tp.L[r], lk);
-                if (!cc) {  // lineshape only: (q^p - q^0) f_r
-                  const cplx dq = qp - q0[r];
-#pragma unroll
-                  for (int h = 0; h < 8; ++h) cmac(hlp[h], dq, f0[r * 8 + h]);
-                } else {
-#pragma unroll
-                  for (int h = 0; h < 8; ++h) {
-                    cmac(hlp[h], qp, lstar_angular(Tp.L[r], E, h));
-                    cmac(hlp[h], mk(-q0[r].re, -q0[r].im), f0[r * 8 + h]);
-                  }
-                }
-              }
-            }
-          }
-          if (!own && shift) {
-#pragma unroll
-            for (int h = 0; h < 8; ++h) vns += norm2(S0[h]);
-          }
-          double v = 0, vn = vns;
-#pragma unroll
-          for (int h = 0; h < 8; ++h) {
-            const cplx s1 = own ? a1[h] : a10[h];
-            const double s2 = own ? a2[h] : a20[h];
-            v += norm2(hlp[h]) + 2.0 * wgt * (hlp[h].re * s1.re + hlp[h].im * s1.im) + c2 * s2;
-            vn += norm2(hlp[h]);
-          }
-          vbuf[pidx * 2] = v;
-          vbuf[pidx * 2 + 1] = vn;
-        }
-      }
-    }
-    const bool deferred = !FIX && (centre_fail || __any_sync(0xffffffffu, fail));
-    if (deferred) {
-      if (lane == 0) defer[atomicAdd(defer_count, 1)] = (int32_t)e;
-    } else {
-      const float wfe = E.w();
-      const bool data_w = wfe <= -1000.f;
-      for (int pi = lane; pi < npts; pi += 32) {
-        const double v = vbuf[pi * 2], vn = vbuf[pi * 2 + 1];
-        double fxe = v, vnw = 0;
-        if (!band && !data_w) {
-          fxe = v * (double)wfe;
-          vnw = vn * (double)wfe;
-        }
-        double* a = acc + pi * 4;
-        if (!(fxe > 0) || !isfinite(fxe)) atomicAdd(a + 3, 1.0);
-        if (e < ev.nda) {
-          atomicAdd(a + 0, (fxe > 0) ? log(fxe) * (double)__ldg(ev.sw + e) : -1e12);
-        } else {
-          atomicAdd(a + 1, fxe);
-          if (!band) atomicAdd(a + 2, vnw);
-        }
-      }
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  for (int pi = threadIdx.x; pi < npts; pi += BATCH_THREADS) {
-    const double* a = acc + pi * 4;
-    parts[(size_t)blockIdx.x * npts + pi] = Partial{a[0], a[1], a[2], a[3]};
-  }
-}
 
 // ------------------------------------------------------------------------------- unsmeared events
 // Unsmeared events: lane = event (32 consecutive events per warp), all lanes walk the points
@@ -488,9 +41,9 @@ constexpr int BU_WARPS = 4;
 constexpr int BU_THREADS = BU_WARPS * 32;
 
 struct BatchUnLayout {
-  size_t q0, r0, hzg, warp_bytes, acc, total;
+  size_t q0, r0, hzg, hxs, warp_bytes, acc, total;
 };
-__host__ __device__ inline BatchUnLayout batch_un_layout(int NR, int NZ, int gmax, int npts) {
+__host__ __device__ inline BatchUnLayout batch_un_layout(int NR, int NZ, int NX, int gmax, int npts) {
   BatchUnLayout L;
   size_t o = 0;
   L.q0 = o;
@@ -499,6 +52,8 @@ __host__ __device__ inline BatchUnLayout batch_un_layout(int NR, int NZ, int gma
   o = bal16(o + (size_t)(NZ > 0 ? NZ : 1) * 32 * sizeof(cplx));
   L.hzg = o;
   o = bal16(o + (size_t)(gmax > 0 ? gmax : 1) * 8 * 32 * sizeof(cplx));
+  L.hxs = o;  // the centre's Zcs amplitudes [h][lane] (models with Zcs entries)
+  o = bal16(o + (size_t)(NX > 0 ? 8 * 32 : 0) * sizeof(cplx));
   L.warp_bytes = o;
   L.acc = BU_WARPS * o;
   L.total = L.acc + (size_t)npts * 4 * sizeof(double);
@@ -546,7 +101,8 @@ __device__ __forceinline__ void pc_acc(const cplx* c, int sx, const Ev& E, cplx 
   }
 }
 
-template <bool FIX>
+// ZCS: the model has Zcs entries (instantiated apart so that the common kernel stays as it was)
+template <bool FIX, bool ZCS>
 __global__ void __launch_bounds__(BU_THREADS)
     k_batch_un(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
                const PointTable* __restrict__ T0p, const __grid_constant__ BatchGroupMap gm,
@@ -554,12 +110,14 @@ __global__ void __launch_bounds__(BU_THREADS)
   extern __shared__ __align__(16) unsigned char sm[];
   const PointTable& T0 = *T0p;
   const int NR = T0.NR, NZ = T0.NZ;
-  const BatchUnLayout Ly = batch_un_layout(NR, NZ, gm.max_slots, npts);
+  constexpr bool has_x = ZCS;  // Zcs entries (their amplitudes join the centre's H_L)
+  const BatchUnLayout Ly = batch_un_layout(NR, NZ, T0.NX, gm.max_slots, npts);
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   unsigned char* wb = sm + warp * Ly.warp_bytes;
   cplx* q0s = reinterpret_cast<cplx*>(wb + Ly.q0);   // [r][lane]
   cplx* r0s = reinterpret_cast<cplx*>(wb + Ly.r0);   // [q][lane]
   cplx* hzg = reinterpret_cast<cplx*>(wb + Ly.hzg);  // [entry of group][h][lane]
+  cplx* hxs = reinterpret_cast<cplx*>(wb + Ly.hxs);  // [h][lane]
   double* acc = reinterpret_cast<double*>(sm + Ly.acc);
   for (int i = threadIdx.x; i < npts * 4; i += BU_THREADS) acc[i] = 0.0;
   __syncthreads();
@@ -596,6 +154,20 @@ __global__ void __launch_bounds__(BU_THREADS)
         const cplx q = lstar_lineshape(T0.L[r], lk0);
         q0s[r * 32 + lane] = q;
         lstar_acc(T0.L[r].c, T0.L[r].sidx, E, q, HL0);
+      }
+    }
+    // Zcs joins the centre's H_L; kept apart for the non-interfering term
+    if (has_x) {
+      for (int k = 0; k < 2; ++k) {
+        cplx t[4];
+#pragma unroll
+        for (int ij = 0; ij < 4; ++ij) t[ij] = mk(0, 0);
+        zcs_amplitudes<4>(T0, EvX{ev.pp3, ev.pp4, ev.n_size, E.e}, k, 0, t);
+#pragma unroll
+        for (int ij = 0; ij < 4; ++ij) {
+          HL0[2 * ij + k] += t[ij];
+          hxs[(2 * ij + k) * 32 + lane] = t[ij];
+        }
       }
     }
     bool fail = false;
@@ -709,7 +281,12 @@ __global__ void __launch_bounds__(BU_THREADS)
       for (int h = 0; h < 8; ++h) {
         const cplx hl = to_hl ? HL0[h] + d[h] : HL0[h], hz = to_hl ? HZ0[h] : HZ0[h] + d[h];
         v += norm2(hl + hz);
-        vn += norm2(hl) + norm2(hz);
+        if (has_x) {
+          const cplx hx = hxs[h * 32 + lane];
+          vn += norm2(hl - hx) + norm2(hx) + norm2(hz);
+        } else {
+          vn += norm2(hl) + norm2(hz);
+        }
       }
       const double fxe = data_w ? v : v * (double)wf;
       double a0 = 0, a1 = 0, a2 = 0;
@@ -745,24 +322,19 @@ __global__ void __launch_bounds__(BU_THREADS)
 }
 
 // ------------------------------------------------------------------------------- host side
-template <int NB, bool FIX>
-static cudaError_t set_batch_smem(int optin) {
-  return cudaFuncSetAttribute(k_batch<NB, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-}
-
 cudaError_t configure_batch_kernels() {
   int dev = 0, optin = 0;
   cudaError_t e;
   if ((e = cudaGetDevice(&dev))) return e;
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
   optin -= 1024;  // the kernels' static shared memory stays below 1 KB
-  if ((e = set_batch_smem<20, false>(optin)) || (e = set_batch_smem<20, true>(optin)) ||
-      (e = set_batch_smem<30, false>(optin)) || (e = set_batch_smem<30, true>(optin)) ||
-      (e = set_batch_smem<150, false>(optin)) || (e = set_batch_smem<150, true>(optin)) ||
-      (e = set_batch_smem<0, false>(optin)) || (e = set_batch_smem<0, true>(optin)))
+  if ((e = batch_set_smem_20(optin)) || (e = batch_set_smem_30(optin)) || (e = batch_set_smem_150(optin)) ||
+      (e = batch_set_smem_grid(optin)))
     return e;
-  if ((e = cudaFuncSetAttribute(k_batch_un<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
-      (e = cudaFuncSetAttribute(k_batch_un<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)))
+  if ((e = cudaFuncSetAttribute(k_batch_un<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
+      (e = cudaFuncSetAttribute(k_batch_un<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
+      (e = cudaFuncSetAttribute(k_batch_un<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)) ||
+      (e = cudaFuncSetAttribute(k_batch_un<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin)))
     return e;
   return cudaSuccess;
 }
@@ -796,6 +368,10 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
       T0.lmask_lstar_R != Tp.lmask_lstar_R || T0.lmask_lstar_B != Tp.lmask_lstar_B ||
       T0.lmask_pc_B != Tp.lmask_pc_B || T0.lmask_pc_R != Tp.lmask_pc_R || T0.needs_sigma_pi != Tp.needs_sigma_pi ||
       !same_bytes(T0.order, Tp.order, sizeof(T0.order)))
+    return false;
+  // Zcs entries are part of the centre's H_L: a point that moves one goes through the single-point path
+  if (T0.NX != Tp.NX || T0.lmask_x_R != Tp.lmask_x_R || T0.lmask_x_B != Tp.lmask_x_B ||
+      !same_bytes(T0.x_mmask, Tp.x_mmask, sizeof(T0.x_mmask)) || !same_bytes(T0.X, Tp.X, sizeof(T0.X)))
     return false;
   for (int g = 0; g < T0.ngroups; ++g) {
     const PcGroup &a = T0.grp[g], &b = Tp.grp[g];
@@ -889,16 +465,16 @@ static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMa
   int64_t b;
   if (batch_nb(s.kind) == 0) {
     b = (n + BU_THREADS - 1) / BU_THREADS;
-    const size_t smem = batch_un_layout(T0.NR, T0.NZ, gm.max_slots, npts).total;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_un<false>, BU_THREADS, smem);
+    const size_t smem = batch_un_layout(T0.NR, T0.NZ, T0.NX, gm.max_slots, npts).total;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_un<false, false>, BU_THREADS, smem);
   } else {
     b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
     const size_t smem = batch_layout(T0.NR, T0.NZ, npts).total;
     switch (batch_nb(s.kind)) {
-      case 20: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<20, false>, BATCH_THREADS, smem); break;
-      case 30: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<30, false>, BATCH_THREADS, smem); break;
-      case -1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<0, false>, BATCH_THREADS, smem); break;
-      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<150, false>, BATCH_THREADS, smem); break;
+      case 20: occ = batch_occupancy_20(smem); break;
+      case 30: occ = batch_occupancy_30(smem); break;
+      case -1: occ = batch_occupancy_grid(smem); break;
+      default: occ = batch_occupancy_150(smem); break;
     }
   }
   if (occ < 1) occ = 1;
@@ -914,19 +490,6 @@ int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupM
   return deferred ? 2 * g : g;
 }
 
-template <int NB>
-static void launch_batch_kind(const EventSet& ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
-                              const PointTable* d_T0, const BatchPoint* d_pts, int npts, Partial* out, int band,
-                              int32_t* defer, int* defer_count, bool fix, int grid, size_t smem, cudaStream_t st,
-                              const double* sgrid, int sgrid_nb) {
-  if (fix)
-    k_batch<NB, true><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
-                                                         defer, defer_count, sgrid, sgrid_nb);
-  else
-    k_batch<NB, false><<<grid, BATCH_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band,
-                                                          defer, defer_count, sgrid, sgrid_nb);
-}
-
 static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t end, const int32_t* list,
                             const int* n_list, const PointTable* d_T0, const BatchGroupMap& gm,
                             const BatchPoint* d_pts, int npts, Partial* out, int band, int32_t* defer,
@@ -935,17 +498,23 @@ static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t e
   const int sn = seg.grid_nb;
   switch (nb) {
     case 0:
-      if (fix)
-        k_batch_un<true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts, out,
-                                                          defer, defer_count);
+      if (ev.pp3 && fix)
+        k_batch_un<true, true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts,
+                                                                out, defer, defer_count);
+      else if (ev.pp3)
+        k_batch_un<false, true><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts,
+                                                                 out, defer, defer_count);
+      else if (fix)
+        k_batch_un<true, false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts,
+                                                                 out, defer, defer_count);
       else
-        k_batch_un<false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts, npts, out,
-                                                           defer, defer_count);
+        k_batch_un<false, false><<<grid, BU_THREADS, smem, st>>>(ev, begin, end, list, n_list, d_T0, gm, d_pts,
+                                                                  npts, out, defer, defer_count);
       break;
-    case -1: launch_batch_kind<0>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
-    case 20: launch_batch_kind<20>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
-    case 30: launch_batch_kind<30>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
-    default: launch_batch_kind<150>(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    case -1: batch_launch_grid(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    case 20: batch_launch_20(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    case 30: batch_launch_30(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
+    default: batch_launch_150(ev, begin, end, list, n_list, d_T0, d_pts, npts, out, band, defer, defer_count, fix, grid, smem, st, sg, sn); break;
   }
 }
 
@@ -957,7 +526,7 @@ cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const P
   const int nb = batch_nb(seg.kind);
   if (nb < 0 && (!seg.grid || seg.grid_nb < 1 || seg.grid_nb > GRID_MAX_NB)) return cudaErrorInvalidValue;
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
-  const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, gm.max_slots, npts).total
+  const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, T0.NX, gm.max_slots, npts).total
                               : batch_layout(T0.NR, T0.NZ, npts).total;
   const int grid = batch_grid(seg, T0, gm, npts, sm_count);
   if (defer) {

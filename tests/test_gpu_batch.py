@@ -95,7 +95,14 @@ def test_batch_repeated_and_chunked(ctx):
 
 
 def test_gradient_batch_with_zcs_entries(ctx):
-    """A model with Zcs entries: the batch call evaluates every point through the single-point path
-    (the structured kernels carry no Zcs terms) and matches one-by-one calls."""
+    """A model with Zcs entries: the centre's Lambda* amplitudes carry the Zcs terms, points that move a
+    Lambda* or Pc parameter are formed from it, points that move a Zcs parameter go through the
+    single-point path; every point matches one-by-one calls."""
+    from pwa_b200 import configs
     labels, blocks, res, nstruct, smp = _check_batch(ctx, "small_zcs", 1500, 15000)
-    assert nstruct == 0
+    mdl, _ = configs.small_zcs()
+    zn = {ref for r in mdl.zcs for ref in (*r.couplings, *r.extra, r.mass, r.width) if isinstance(ref, str)}
+    n_zcs = sum(1 for name, _ in labels if name in zn)
+    # (a Zcs coupling that only fills slots the reference kernel does not read leaves the point equal to
+    # the centre, so such points are formed from it as well)
+    assert n_zcs > 0 and len(blocks) - n_zcs <= nstruct < len(blocks), (nstruct, len(blocks), n_zcs)
