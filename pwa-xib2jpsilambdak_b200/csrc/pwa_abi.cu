@@ -623,6 +623,16 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     if (x.kind == BP_PCC) return x.nq < y.nq;
     return false;
   });
+  {
+    // a warp whose points differ in kind runs each kind's code: fill the last warp of lineshape points
+    // with Lambda* points (the cheapest kind) rather than with coupling points
+    const auto is_kind = [&](int k) { return [&, k](int p) { return bp[p].kind == k; }; };
+    const auto pcg_end = std::find_if_not(sidx.begin(), sidx.end(), is_kind(BP_PCG));
+    const int fill = (32 - (int)((pcg_end - sidx.begin()) % 32)) % 32;
+    const auto lst = std::find_if(pcg_end, sidx.end(), is_kind(BP_LSTAR));
+    const int nl = (int)std::min<std::ptrdiff_t>(fill, std::count_if(lst, sidx.end(), is_kind(BP_LSTAR)));
+    if (fill > 0 && nl > 0) std::rotate(pcg_end, lst, lst + nl);
+  }
   const bool tables = c->use_tables != 0 && H[0].NZ > 0;
   const int chunk_cap = BATCH_MAX_POINTS;
   if (!c->d_btables) {
