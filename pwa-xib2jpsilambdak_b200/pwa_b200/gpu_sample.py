@@ -67,7 +67,8 @@ def _planes(n_size, device):
 
 
 def generate(block, n_data: int, n_mc: int, w_range=(0.2, 1.0), seed: int = 1, device: int = 0,
-             batch: int = 4_000_000, max_scale: float = 1.05, ordered: bool = True) -> DeviceSample:
+             batch: int = 4_000_000, max_scale: float = 1.05, ordered: bool = True,
+             toy_sizes=None) -> DeviceSample:
     """ordered: MC events in the 20-offset smearing windows first, each class sorted by m(J/psi p),
     so every event class is one contiguous, coalesced range (the likelihood does not depend on the
     order; only the summation order changes)."""
@@ -122,7 +123,15 @@ def generate(block, n_data: int, n_mc: int, w_range=(0.2, 1.0), seed: int = 1, d
     band = B.band_of(mz)
     # bands 1, 2, 3 as the reference requires; inside a band by mass, so neighbouring events share
     # lineshape-table nodes
-    order = np.lexsort((mz, band)) if ordered else B.order_data_by_band(mz)
+    if toy_sizes is not None:
+        # consecutive accepted events form consecutive toys, each sorted into its own bands
+        edges = np.concatenate([[0], np.cumsum(np.asarray(toy_sizes, np.int64))])
+        if edges[-1] != n_data:
+            raise ValueError("toy sizes must add up to n_data")
+        order = np.concatenate([a + (np.lexsort((mz[a:b], band[a:b])) if ordered else B.order_data_by_band(mz[a:b]))
+                                for a, b in zip(edges[:-1], edges[1:])]).astype(np.int64)
+    else:
+        order = np.lexsort((mz, band)) if ordered else B.order_data_by_band(mz)
     o = torch.as_tensor(order, device=dev, dtype=torch.long)
     pp[:, :n_data] = dp[:, o]
     pp[2, :n_data] = -1001.0

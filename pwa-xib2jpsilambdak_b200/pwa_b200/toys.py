@@ -118,6 +118,22 @@ def make_ensemble(sizes, n_mc: int, w_range: tuple, seed: int, amp2_of_angles, z
     return build_ensemble(toys, mc, mcw)
 
 
+def make_ensemble_gpu(block, sizes, n_mc: int, w_range: tuple = (0.2, 1.0), seed: int = 1,
+                      device: int = 0) -> ToyEnsemble:
+    """The same ensemble drawn on the GPU (flat phase space and hit-or-miss against the model's
+    |A|^2 at `block`): toys of the given sizes, each in its own bands, then the shared MC, in
+    torch-owned device planes (bind with Context.bind_device(ens.sample))."""
+    from . import gpu_sample
+    sizes = np.asarray(sizes, np.int64)
+    ds = gpu_sample.generate(block, int(sizes.sum()), n_mc, w_range, seed=seed, device=device, toy_sizes=sizes)
+    mz = ds.pp[1, :ds.nda].cpu().numpy()
+    band = B.band_of(mz)
+    offsets = np.concatenate([[0], np.cumsum(sizes)])
+    b1 = np.array([int((band[a:b] == 1).sum()) for a, b in zip(offsets[:-1], offsets[1:])])
+    b2 = np.array([int((band[a:b] == 2).sum()) for a, b in zip(offsets[:-1], offsets[1:])])
+    return ToyEnsemble(ds, offsets, b1, b2, sizes.astype(float), sizes.astype(float))
+
+
 def select(ctx, ens: ToyEnsemble, t: int) -> ToyView:
     """Make toy t the data the context evaluates (its window of the uploaded ensemble)."""
     v = ens.view(t)
@@ -128,7 +144,8 @@ def select(ctx, ens: ToyEnsemble, t: int) -> ToyView:
 
 
 def select_all(ctx, ens: ToyEnsemble):
-    """All toys' data at once again (the upload's default)."""
+    """Back to the selection an upload starts with (all data, the sample's band arguments).  An
+    ensemble's bands are per toy, so its likelihood is meaningful one toy at a time."""
     ctx.select_data(0, -1, *ens.sample.reference_band_args())
     ctx.sample = ens.sample
 

@@ -121,3 +121,28 @@ def test_toy_window_under_gaussian_resolution():
     finally:
         ctx.close()
         solo.close()
+
+
+def test_toy_ensemble_generated_on_gpu(oracle_mod):
+    """Toys drawn on the GPU share one MC block; each toy's window is in its own band order and its
+    NLL equals the FP64 oracle on a host copy of that toy with the MC."""
+    from pwa_b200 import basis as B, configs, lib, model as M, toys
+    mdl, vals = configs.small_kmatrix()
+    blk = M.build_param_block(mdl, vals)
+    sizes = toys.toy_sizes(3, lo=500, hi=3000, seed=7)
+    ens = toys.make_ensemble_gpu(blk, sizes, 20000, seed=11)
+    ds = ens.sample
+    assert ds.nda == int(sizes.sum()) and list(ens.offsets[1:] - ens.offsets[:-1]) == list(sizes)
+    ctx = lib.Context(0)
+    try:
+        ctx.bind_device(ds)
+        for t in range(ens.n_toys):
+            v = toys.select(ctx, ens, t)
+            band = B.band_of(ds.pp[1, v.first:v.first + v.nda].cpu().numpy())
+            assert np.all(np.diff(band) >= 0)
+            r = ctx.eval_nll(blk)
+            host = ds.to_host(data_idx=np.arange(v.first, v.first + v.nda))
+            o, _, _, _ = oracle_mod.nll(host, blk)
+            assert abs(r.nll - o) < NLL_TOL, (t, r.nll, o)
+    finally:
+        ctx.close()
