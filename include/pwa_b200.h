@@ -224,8 +224,18 @@ int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles
  * the array, which keeps the last call's contents; calls that overlap on the GPU race on it (calls
  * from threads of one process are serialised inside the library).  The first call on a device
  * resolves the array's device address for that device; make that first call before any stream
- * capture.  Work is queued on `stream` (cudaStream_t, NULL for the default stream) and the call
- * returns when the result is on the host. */
+ * capture.  Under CUDA's default lazy module loading, that first call is also when the library's
+ * device code and the array are loaded onto the device, i.e. when their memory is taken: make the
+ * first call before handing the device's free memory to another allocator, or run the process with
+ * CUDA_MODULE_LOADING=EAGER (module and array loaded with the CUDA context).  Later calls take no
+ * device memory.  Work is queued on `stream` (cudaStream_t, NULL for the default stream) and the
+ * call waits on the host until the result is there.
+ *
+ * Lineshapes: with no room for the interpolation tables of pwa_ctx_eval_nll (about 49 MB per point),
+ * this entry point evaluates every Pc lineshape exactly (one K-matrix solve per event and offset),
+ * which costs about twice the time of the context entry point on the K-matrix model; results agree
+ * with it to FP64 rounding.  Spline blocks (spline_size > 0) and Zcs models (NX > 0) return
+ * PWA_E_UNSUPPORTED.  An empty sample (n = 0) gives sumint = data_term = 0. */
 #define PWA_NOALLOC_MAX_EVENTS (1 << 20)
 #define PWA_NOALLOC_SCRATCH_BYTES 4718592 /* 4.5 MiB */
 int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* d_pp1, const float* d_pp2, const float* d_sw,

@@ -17,7 +17,9 @@ Recipe (no reference source is copied into the repository; all output goes to or
 
 The result, ``oracle/_ref/libref_<NR>_<NZ>_<NX>_<IKM>.so``, runs the reference's FP32 arithmetic
 on host cores (OpenMP over thread blocks).  It is the parity anchor for the FP64 oracle and the
-CPU baseline of bench.py.  It needs /root/reference, so it is built here and shipped prebuilt.
+CPU baseline of bench.py.  It needs the reference tree, named by the environment variable
+``PWA_REFERENCE_TREE`` (the build entry point sets it where the tree is mounted), so it is built
+where that tree exists and shipped prebuilt.
 """
 from __future__ import annotations
 
@@ -31,7 +33,16 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("PWA_REFERENCE_TREE", "/root/reference"))
+REF = Path(os.environ["PWA_REFERENCE_TREE"]) if os.environ.get("PWA_REFERENCE_TREE") else None
+
+
+def reference_tree() -> Path:
+    """The reference tree named by PWA_REFERENCE_TREE; a clear error when it is unset or missing."""
+    if REF is None:
+        raise FileNotFoundError("PWA_REFERENCE_TREE is not set: it must name the reference source tree")
+    if not (REF / "src" / "kernel_calEva.cu").is_file():
+        raise FileNotFoundError(f"PWA_REFERENCE_TREE={REF} holds no src/kernel_calEva.cu")
+    return REF
 CUDA_INC = "/usr/local/cuda/include"
 
 # Model-size buckets used by the tests and the bench (NR, NZ, NX, max_ikmcount).
@@ -51,7 +62,7 @@ def lib_path(nr: int, nz: int, nx: int, ikm: int = 6) -> Path:
 
 
 def available() -> bool:
-    return (REF / "src" / "kernel_calEva.cu").is_file()
+    return REF is not None and (REF / "src" / "kernel_calEva.cu").is_file()
 
 
 def _ndefine(nr: int, nz: int, nx: int, ikm: int) -> str:
@@ -71,8 +82,7 @@ static constexpr unsigned MYXN = Constant::number_of_Zcs;
 
 
 def build_bucket(nr: int, nz: int, nx: int, ikm: int = 6, verbose: bool = False) -> Path:
-    if not available():
-        raise FileNotFoundError(f"reference tree not found at {REF}")
+    reference_tree()
     OUT.mkdir(parents=True, exist_ok=True)
     target = lib_path(nr, nz, nx, ikm)
     work = OUT / f"b_{nr}_{nz}_{nx}_{ikm}"
@@ -128,8 +138,7 @@ def build_aux(verbose: bool = False) -> Path:
     """Clebsch-Gordan tables (src/EvtCGCoefSingle.cpp, src/EvtOrthogVector.cpp, compiled in place) and
     the Wigner d-functions of src/RooDalitzAmplitude.cxx (the block from ``dfunhalf`` to the end of
     ``dfun``, extracted at build time and renamed with an ``_impl`` suffix)."""
-    if not available():
-        raise FileNotFoundError(f"reference tree not found at {REF}")
+    reference_tree()
     OUT.mkdir(parents=True, exist_ok=True)
     work = OUT / "b_aux"
     if work.exists():
@@ -163,7 +172,7 @@ def main(argv=None) -> int:
     ap.add_argument("-v", action="store_true")
     args = ap.parse_args(argv)
     if not available():
-        print(f"reference tree not found at {REF}; nothing built")
+        print(f"reference tree not available (PWA_REFERENCE_TREE={REF}); nothing built")
         return 0
     buckets = [tuple(int(x) for x in b.split(",")) for b in args.bucket] or DEFAULT_BUCKETS
     for b in buckets:

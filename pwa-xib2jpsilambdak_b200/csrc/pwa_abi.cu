@@ -20,11 +20,17 @@ cudaError_t configure_kernels();
 
 namespace {
 thread_local std::string g_last_cuda = "no error";
+}  // namespace
 
+namespace pwa {
+// Records the message of a failed CUDA call for pwa_last_cuda_error and maps it to a status code.
 int cuda_fail(cudaError_t e) {
   g_last_cuda = cudaGetErrorString(e);
   return e == cudaErrorMemoryAllocation ? PWA_E_NOMEM : PWA_E_CUDA;
 }
+}  // namespace pwa
+
+namespace {
 #define PWA_CUDA(x)                      \
   do {                                   \
     cudaError_t _e = (x);                \

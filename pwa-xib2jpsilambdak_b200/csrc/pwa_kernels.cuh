@@ -61,6 +61,10 @@ int segment_blocks(const Segment& s, int sm_count);
 // Partial slots a segment uses: its pass, plus the pass over deferred events when deferred is true.
 int segment_parts(const Segment& s, int sm_count, bool deferred);
 
+// Records a failed CUDA call's message (pwa_last_cuda_error) and returns PWA_E_CUDA, or PWA_E_NOMEM
+// for a failed allocation.
+int cuda_fail(cudaError_t e);
+
 // Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                       float ffr, float ffb, PointTable* out);

@@ -14,7 +14,13 @@
 // before reading it.  Calls that overlap on the GPU race on the array; calls from threads of one
 // process are serialised by a lock here, overlapping use from elsewhere must be avoided by the
 // caller.  The first call on a device looks up the array's device address (cudaGetSymbolAddress, with
-// that device current) and caches it; make that first call before any stream capture.
+// that device current) and caches it; make that first call before any stream capture.  Under CUDA's
+// default lazy module loading that lookup is also what loads this library's device code onto the
+// device, and with it the array: the first call on each device takes the array's memory (and the
+// code's), later calls take none.  A caller that hands the device's free memory to another
+// allocator should therefore make its first call before doing so, or run with
+// CUDA_MODULE_LOADING=EAGER, which loads the module (and the array) when the CUDA context is created.
+// Every call waits on the host for its result (it synchronises `stream`).
 //
 // The event-class kernels and the final reduction are the ones of pwa_ctx_eval_nll, launched with
 // the same segments, grid sizes and partial-slot layout, so both entry points give the same result.
@@ -108,8 +114,10 @@ int scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return PWA_E_ARG;
   if (!g_addr[device]) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PWA_E_CUDA;
-    if (configure_kernels() != cudaSuccess) return PWA_E_CUDA;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (!p) return PWA_E_CUDA;
+    if ((e = configure_kernels()) != cudaSuccess) return cuda_fail(e);
     g_addr[device] = static_cast<unsigned char*>(p);
   }
   *out = g_addr[device];
@@ -134,15 +142,19 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
   int rc = build_point_table(h_paraList, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, &table);
   if (rc) return rc;
   int prev = 0;
-  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return PWA_E_CUDA;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e == cudaSuccess) e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e);
   auto finish = [&](int code) {
     cudaSetDevice(prev);
     return code;
   };
+  // every CUDA failure below is recorded for pwa_last_cuda_error
+  auto fail = [&](cudaError_t err) { return finish(cuda_fail(err)); };
   unsigned char* base = nullptr;
   if ((rc = scratch_address(device, &base))) return finish(rc);
   int sm_count = 0;
-  if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return finish(PWA_E_CUDA);
+  if ((e = cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return fail(e);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   PointTable* d_table = reinterpret_cast<PointTable*>(base + kOffTable);
   EvalResult* d_res = reinterpret_cast<EvalResult*>(base + kOffResult);
@@ -158,18 +170,21 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
   const int64_t r0 = std::min(n, std::max<int64_t>(0, nda_smr + nda_fine));
   const int64_t tail = n - r0;
   int nw = 0;
-  if (cudaMemcpyAsync(d_table, &table, sizeof(PointTable), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return finish(PWA_E_CUDA);
+  if ((e = cudaMemcpyAsync(d_table, &table, sizeof(PointTable), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return fail(e);
   if (tail > 0) {
     const int nchunks = (int)((tail + kChunk - 1) / kChunk);
     k_count<<<nchunks, 32, 0, st>>>(d_pp, n_size, r0, n, d_counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     k_scan<<<1, 1, 0, st>>>(d_counts, nchunks, d_offsets);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     // the window list takes the front of the list region and the other tail events follow it, so the
     // window total is needed before the scatter
-    if (cudaMemcpyAsync(&nw, d_offsets + nchunks, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return finish(PWA_E_CUDA);
+    if ((e = cudaMemcpyAsync(&nw, d_offsets + nchunks, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return fail(e);
     k_scatter<<<nchunks, 32, 0, st>>>(d_pp, n_size, r0, n, d_offsets, d_lists, d_lists + nw);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
   }
   Segment segs[4];
   int nseg = 0;
@@ -186,14 +201,18 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
   if (tot > kMaxParts) return finish(PWA_E_SIZE);
   const EventSet ev{d_pp, d_pp1, d_pp2, d_sw, n_size, n, nda};
   for (int i = 0; i < nseg; ++i)
-    if (launch_segment(ev, segs[i], d_table, d_parts + offs[i], nullptr, nullptr, nullptr, sm_count, st) != cudaSuccess)
-      return finish(PWA_E_CUDA);
-  if (launch_finalize(d_parts, std::max(tot, 1), sum_w_mc, sum_w_data, nll_shift, d_res, st) != cudaSuccess)
-    return finish(PWA_E_CUDA);
+    if ((e = launch_segment(ev, segs[i], d_table, d_parts + offs[i], nullptr, nullptr, nullptr, sm_count, st)) !=
+        cudaSuccess)
+      return fail(e);
+  // An empty sample launches no segment: the one slot finalize reads is cleared here, since the
+  // array still holds the previous call's partials (a memset allocates nothing).
+  if (tot == 0 && (e = cudaMemsetAsync(d_parts, 0, sizeof(Partial), st)) != cudaSuccess) return fail(e);
+  if ((e = launch_finalize(d_parts, std::max(tot, 1), sum_w_mc, sum_w_data, nll_shift, d_res, st)) != cudaSuccess)
+    return fail(e);
   EvalResult r;
-  if (cudaMemcpyAsync(&r, d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return finish(PWA_E_CUDA);
+  if ((e = cudaMemcpyAsync(&r, d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return fail(e);
   out->nll = r.nll;
   out->sumint = r.sumint;
   out->sum_noint = r.sum_noint;

@@ -1,5 +1,6 @@
-"""Generates the golden fixtures of tests/golden/ from the reference tree (run here, where
-/root/reference exists; the fixtures are committed and the tests never read the reference).
+"""Generates the golden fixtures of tests/golden/ from the reference tree, named by the environment
+variable PWA_REFERENCE_TREE (run where that tree exists; the fixtures are committed and the tests
+never read the reference).
 
 * smear_schemes.json : the three resolution-offset tables (RooTDalitz/Resonances.h:31-54)
 * cg_c2.json         : the reference's tabulated <L 0; S 1/2 | 1/2 1/2> (RooDalitzAmplitude.cxx:96-107)
@@ -21,9 +22,11 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = Path("/root/reference")
 sys.path.insert(0, str(ROOT / "pwa-xib2jpsilambdak_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
+import build_ref  # noqa: E402
+
+REF = build_ref.reference_tree()
 
 
 def smear():

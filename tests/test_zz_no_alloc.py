@@ -53,12 +53,39 @@ def test_noalloc_matches_context_entry_point_twice(name, nd, nm):
     ctx.upload(smp)
     want = ctx.eval_nll(blk)
     ctx.close()
-    for _ in range(2):  # consecutive calls share the library's scratch array
+    torch.cuda.synchronize()
+    for i in range(2):  # consecutive calls share the library's scratch array
+        free0 = torch.cuda.mem_get_info()[0]
         rc, got = _noalloc(L, planes, smp, blk, band)
         assert rc == 0, lib.load().pwa_error_string(rc)
+        if i == 1:  # after the first call (which loads the module on this device) no memory is taken
+            assert torch.cuda.mem_get_info()[0] == free0
         assert abs(got.nll - want.nll) < NLL_TOL
         assert abs(got.sumint / want.sumint - 1) < 1e-12 and abs(got.sum_noint / want.sum_noint - 1) < 1e-12
         assert got.n_nonpos == want.n_nonpos
+
+
+def test_noalloc_on_a_torch_stream_and_empty_sample():
+    """Work queued on a caller's stream gives the same result; an empty sample after a full one
+    returns zero sums, not the previous call's partials left in the shared array."""
+    import copy
+    import torch
+    from pwa_b200 import lib
+    L = _bind(lib.load())
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    planes = [torch.as_tensor(a, device="cuda") for a in (smp.pp, smp.pp1, smp.pp2, smp.sw)]
+    band = smp.reference_band_args()
+    rc, want = _noalloc(L, planes, smp, blk, band)
+    assert rc == 0
+    s = torch.cuda.Stream()
+    rc, got = _noalloc(L, planes, smp, blk, band, stream=C.c_void_p(s.cuda_stream))
+    assert rc == 0, lib.load().pwa_error_string(rc)
+    assert abs(got.nll - want.nll) < NLL_TOL and abs(got.sumint / want.sumint - 1) < 1e-12
+    empty = copy.copy(smp)
+    empty.n, empty.nda = 0, 0
+    rc, got = _noalloc(L, planes, empty, blk, (-1, 0))
+    assert rc == 0, lib.load().pwa_error_string(rc)
+    assert got.sumint == 0.0 and got.sum_noint == 0.0 and got.data_term == 0.0
 
 
 def test_noalloc_rejects_oversize_sample():
