@@ -39,12 +39,23 @@ WORKLOADS = {
                     text="full_bw: 14 Lambda* BW (J <= 7/2) + 3 narrow Pc BW, Gaussian resolution 2.7 MeV on "
                          "a 0.5 MeV grid"),
 }
-CPU_SAMPLE = (2_000, 20_000)  # data, MC events of the bounded CPU sample
+CPU_FRAC = 10  # the bounded CPU sample: 1/CPU_FRAC of the bench sample's data and MC events
 # DRAM bytes read + written per event of a segment (table-only and exact passes together), from one
 # ncu captures of the 50k data + 500k MC case (DRAM read + write of the table-only and the
 # exact-capable pass of the window segment); the traffic of a launch scales with its events.
 DRAM_BYTES_PER_EVENT = {1: 3120.0}
 BATCH_DRAM_BYTES_PER_EVENT = {1: 210900.0}
+# The resource that binds the FP64 kernels: FP64 pipe utilisation of the dominant kernel (ncu,
+# sm__pipe_fp64_cycles_active as % of peak, small case of the same kernel), with its summary file.
+FP64_PIPE = {("plain", 1): (0.186, "profiles/k_smeared20_kmatrix_50k_500k.md"),
+             ("batch", 1): (0.126, "profiles/k_batch20_kmatrix_50k_500k.md")}
+
+
+def fp64_pipe(kind: str, seg: int):
+    v = FP64_PIPE.get((kind, seg))
+    if v is None:
+        return None
+    return {"frac": v[0], "metric": "sm__pipe_fp64_cycles_active, % of peak (ncu)", "source": v[1]}
 
 
 def parse():
@@ -57,6 +68,8 @@ def parse():
     ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
     ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
+    ap.add_argument("--no-full-parity", action="store_true",
+                    help="skip the FP64 oracle check of the whole sample (centre and one point per batch kind)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
                     help="kmatrix (the headline workload) or full_bw (the Breit-Wigner model with the "
                          "Gaussian resolution)")
@@ -138,78 +151,110 @@ def required_bytes_per_event(model) -> tuple:
 
 
 # ------------------------------------------------------------------------------ CPU side
-def cpu_reference_seconds(sample, block, reps: int = 2) -> float:
-    """Seconds per host_store_fx of the reference's own code built for host cores on `sample`."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    ref = O.RefHost(sample, block)
-    ref.store_fx(block)
-    t = time.perf_counter()
-    for _ in range(reps):
-        ref.store_fx(block)
-    return (time.perf_counter() - t) / reps
-
-
-def cpu_oracle_seconds(sample, block) -> float:
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    t = time.perf_counter()
-    O.nll(sample, block)
-    return time.perf_counter() - t
-
-
-def cpu_sample_from_device(dsample, n_data: int, n_mc: int, seed: int = 5):
+def cpu_sample_from_device(dsample, frac: int = CPU_FRAC, seed: int = 5):
+    """The bounded CPU sample: a seeded 1/frac of the bench sample's data and of its MC events (band
+    order kept, band counts recomputed), copied to host memory.  Both CPU legs (the GPU arm's
+    cpu_baseline and --impl reference) time this same selection."""
     rng = np.random.default_rng(seed)
-    di = np.sort(rng.choice(dsample.nda, size=min(n_data, dsample.nda), replace=False))
-    mi = np.sort(rng.choice(dsample.nmc, size=min(n_mc, dsample.nmc), replace=False))
+    di = np.sort(rng.choice(dsample.nda, size=dsample.nda // frac, replace=False))
+    mi = np.sort(rng.choice(dsample.nmc, size=dsample.nmc // frac, replace=False))
     return dsample.to_host(di, mi)
 
 
+def bench_sample(block, wl: dict, device: int, rank: int = 0, small: bool = False):
+    """The benchmark sample of this rank, generated on the GPU (seeded; identical in both arms)."""
+    from pwa_b200 import gpu_sample
+    frac = 10 if small else 1
+    return gpu_sample.generate(block, wl["n_data"] // frac, wl["n_mc"] // frac, wl["w_range"], seed=1000 + rank,
+                               device=device)
+
+
+def time_reference(sample, block, steps: int, warmup: int) -> float:
+    """Seconds per host_store_fx of the reference's own code built for host cores (OpenMP over all
+    cores) on `sample`: `warmup` untimed calls, then the mean of `steps` timed calls."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    ref = O.RefHost(sample, block)
+    for _ in range(max(warmup, 1)):
+        ref.store_fx(block)
+    t = time.perf_counter()
+    for _ in range(steps):
+        ref.store_fx(block)
+    return (time.perf_counter() - t) / steps
+
+
 def reference_arm(args):
-    """--impl reference: the reference's own likelihood code (FP32, OpenMP over all host cores) on a
-    bounded sample of the workload, reported in evals/s of the full workload."""
+    """--impl reference: the reference's own likelihood code (FP32, OpenMP over all host cores) on the
+    bounded CPU sample of the workload (1/CPU_FRAC of the bench sample's events, drawn as the GPU
+    arm's cpu_baseline draws them), reported in evals/s of the full workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    from pwa_b200 import configs, dataset as D, model as M
-    mdl, vals = configs.kmatrix()
+    from pwa_b200 import configs, model as M
+    wl = WORKLOADS[args.workload]
+    mdl, vals = configs.MODELS[wl["name"]]()
     block = M.build_param_block(mdl, vals)
+    if wl["smearing"]:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no Gaussian resolution model "
+                                                              "(full_bw workload)"}))
+        return 0
     L = O.ref_lib(block.NR, block.NZ, block.NX, build_if_missing=False)
     if L is None:
         print(json.dumps({"impl": "reference", "unavailable": "host build of the reference not found in oracle/_ref"}))
         return 0
-    nd, nm = CPU_SAMPLE
-
-    def amp2(ang):
-        s = D.build_sample({k: v[:0] for k, v in ang.items()}, ang, np.ones(len(ang["mLk"])))
-        return O.RefHost(s, block).amp2s(block)
-
-    sample = D.make_sample(nd, nm, WORKLOAD["w_range"], 4242, amp2)
-    ref = O.RefHost(sample, block)
-    for _ in range(max(args.warmup, 1)):
-        ref.store_fx(block)
+    # input preparation (outside the timed region): the bench sample from the seeded device
+    # generator, then the CPU selection; the timed code is the reference's alone
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dsample = bench_sample(block, wl, local, small=args.small)
+    smp = cpu_sample_from_device(dsample)
+    n_full = dsample.n
+    del dsample
+    torch.cuda.empty_cache()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ref.store_fx(block)
-    dt = (time.perf_counter() - t0) / args.steps
-    scale = (WORKLOAD["n_data"] + WORKLOAD["n_mc"]) / (nd + nm)
+    dt = time_reference(smp, block, args.steps, args.warmup)
+    run_s = time.perf_counter() - t0
+    scale = n_full / smp.n
     value = 1.0 / (dt * scale)
     cores = os.cpu_count()
-    metric = METRIC if args.workload == "kmatrix" else ("NLL evals/s, 1M-event full Breit-Wigner model with Gaussian "
-                                                         "resolution: batched vs plain on B200")
-    out = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": dt * scale * 1e3, "higher_is_better": True, "scaling": "weak",
+    out = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": "kmatrix: 6 Lambda* BW + 4-channel Pc K-matrix (4 poles, 8 non-resonant), "
-                                  "500k data + 5M MC", "parallelism": "host cores (OpenMP)"},
+           "config": {"workload": f"{wl['text']}, {wl['n_data']} data + {wl['n_mc']} MC events",
+                      "parallelism": "host cores (OpenMP)"},
+           "step": f"one host_store_fx of the reference's host build over {smp.n} events (1/{CPU_FRAC} of the "
+                   f"workload: {smp.nda} data + {smp.nmc} MC drawn from the bench sample); value = 1 / "
+                   f"(seconds per step x {scale:.2f})",
+           "sample_scale": scale, "timed_s": round(run_s, 2),
            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
-                            "sample": f"{nd} data + {nm} MC events per step, time scaled by {scale:.1f} to the "
-                                      f"full workload"},
+                            "sample": f"{smp.nda} data + {smp.nmc} MC events drawn from the bench sample "
+                                      f"(seed 5); time x{scale:.2f} to the full workload"},
            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
+
+
+def full_size_parity(dsample, block, ctx, labels, gblocks, bres, probe) -> dict:
+    """GPU plain and batched NLL against the FP64 oracle on the whole bench sample (host cores), at
+    the centre and one gradient point of every batch kind."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    host = dsample.to_host()
+    rows = []
+    for name in probe:
+        i = 0 if name == "centre" else labels.index((name, +1))
+        v_or, s_or, _, _ = O.nll(host, gblocks[i])
+        v_pl = ctx.eval_nll(gblocks[i]).nll
+        rows.append({"point": name, "nll_oracle": v_or, "dnll_plain": v_pl - v_or,
+                     "dnll_batched": (bres[i].nll - v_or) if bres is not None else None})
+    del host
+    worst = max(max(abs(r["dnll_plain"]), abs(r["dnll_batched"] or 0.0)) for r in rows)
+    return {"sample_events": dsample.n, "points": rows, "max_abs_dnll": worst,
+            "oracle_threads": os.cpu_count(), "seconds": round(time.perf_counter() - t0, 1)}
 
 
 # ------------------------------------------------------------------------------ GPU arm
@@ -236,7 +281,7 @@ def main():
     frac = 10 if args.small else 1
     nd, nm = wl["n_data"] // frac, wl["n_mc"] // frac
     t_gen = time.perf_counter()
-    sample = gpu_sample.generate(block, nd, nm, wl["w_range"], seed=1000 + rank, device=local)
+    sample = bench_sample(block, wl, local, rank, args.small)
     t_gen = time.perf_counter() - t_gen
     ctx = lib.Context(local)
     ctx.bind_device(sample)
@@ -328,7 +373,7 @@ def main():
         idx = [0] + [labels.index((n, +1)) for n in probe if (n, +1) in labels]
         dmax = max(abs(bres[i].nll - ctx.eval_nll(gblocks[i]).nll) for i in idx)
         bat = dict(npts=npts, nstruct=nstruct, dev_ms=bdev_ms, e2e_ms=be2e_ms, launches=blaunch, dnll=dmax,
-                   nprobe=len(idx), seg=bseg)
+                   nprobe=len(idx), seg=bseg, labels=labels, blocks=gblocks, res=bres)
     clocks = clk.stop()
     if world > 1:
         t = torch.tensor([dev_ms, e2e_ms, bat["dev_ms"] if bat else 0.0, bat["e2e_ms"] if bat else 0.0],
@@ -377,6 +422,7 @@ def main():
                         "traffic": (DRAM_BYTES_PER_EVENT[dom] * seg_time[dom][1]
                                     if dom in DRAM_BYTES_PER_EVENT else None),
                         "traffic_unit": "bytes per step of this segment (ncu, scaled by events)",
+                        "fp64_pipe": fp64_pipe("plain", dom),
                         "note": f"algorithmic bytes = {req_b} B per event (planes the model reads) of the "
                                 f"{full_b} B reference row; peak {peak_kind}"},
            "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(lib.load().pwa_point_table_bytes()),
@@ -387,13 +433,15 @@ def main():
                                "sample": "not timed: the reference has no Gaussian resolution model"}
     elif world == 1 and not args.no_cpu_baseline:
         try:
-            smp = cpu_sample_from_device(sample, *CPU_SAMPLE)
-            t_ref = cpu_reference_seconds(smp, block)
-            scale = (nd + nm) / smp.n
+            smp = cpu_sample_from_device(sample)
+            t_ref = time_reference(smp, block, args.steps, args.warmup)
+            scale = sample.n / smp.n
             out["cpu_baseline"] = {"value": 1.0 / (t_ref * scale), "unit": "evals/s", "cores": os.cpu_count(),
-                                   "kind": "reference",
-                                   "sample": f"{smp.nda} data + {smp.nmc} MC events drawn from the bench sample; "
-                                             f"time x{scale:.0f} to the full workload"}
+                                   "kind": "reference", "seconds_per_step": t_ref, "steps": args.steps,
+                                   "sample": f"{smp.nda} data + {smp.nmc} MC events (1/{CPU_FRAC}) drawn from the "
+                                             f"bench sample (seed 5), {args.steps} timed calls after "
+                                             f"{max(args.warmup, 1)} warm-up; time x{scale:.2f} to the full "
+                                             f"workload"}
             # parity on the same sample: this GPU path and the reference FP32 code vs the FP64 oracle
             sys.path.insert(0, str(ROOT / "oracle"))
             import oracle as O
@@ -405,9 +453,20 @@ def main():
             v_ref, _ = O.RefHost(smp, block).store_fx(block)
             out["parity"] = {"sample_events": smp.n, "dnll_gpu_vs_oracle": v_gpu - v_or,
                              "dnll_reference_fp32_vs_oracle": v_ref - v_or}
+            del smp
         except Exception as ex:  # the baseline is reported, never required for the GPU number
             out["cpu_baseline"] = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"failed: {ex}"}
+    if world == 1 and bat and not args.no_full_parity and not wl["smearing"]:
+        # every batch kind: Lambda* coupling and mass, Pc coupling, K-matrix pole coupling and mass,
+        # scattering term
+        probe = ["centre", "a_p1p1_1520", "m0_1670", "a_L0_Pc4312", "g1_Pc4312", "m0_Pc4440", "fsc_ZM3SC2"]
+        probe = [p for p in probe if p == "centre" or (p, +1) in bat["labels"]]
+        try:
+            out["parity_full"] = full_size_parity(sample, block, ctx, bat["labels"], bat["blocks"], bat["res"],
+                                                  probe)
+        except Exception as ex:
+            out["parity_full"] = {"failed": str(ex)}
     if bat:
         out = batched_line(out, bat, args, world, sample, req_b, hbm, peak_kind)
     print(json.dumps(out))
@@ -453,6 +512,7 @@ def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, h
                      "traffic": (BATCH_DRAM_BYTES_PER_EVENT[dom] * dom_ev if dom in BATCH_DRAM_BYTES_PER_EVENT
                                  else None),
                      "traffic_unit": "bytes per step of this segment (ncu, scaled by events)",
+                     "fp64_pipe": fp64_pipe("batch", dom),
                      "note": f"algorithmic bytes = {req_b} B of planes + 4 B index per event, read once per "
                              f"batch of {npts} points; the kernel is FP64-issue bound, peak {peak_kind}"},
         "e2e": {"value": e2e, "unit": "evals/s",

@@ -43,6 +43,26 @@ class Sample:
         them to host_store_fx (RooDalitzAmplitude.cxx:1943-1946): the first count minus one."""
         return self.nda_smr1 - 1, self.nda_fine
 
+    def shard(self, begin: int, end: int) -> "Sample":
+        """Events [begin, end) as a sample of their own (planes copied), with the band arguments that
+        keep every event in the class the whole sample gives it (dist.shard_band_args) and the
+        whole sample's normalisation weights (sum_w_mc, sum_w_data), as one device of the
+        reference's multi-device split evaluates its shard."""
+        from .dist import shard_band_args
+        n = end - begin
+        ns = B.n_size_of(n)
+
+        def cut(a, rows):
+            out = np.zeros((rows, ns), np.float32)
+            out[:, :n] = np.asarray(a, np.float32).reshape(rows, self.n_size)[:, begin:end]
+            return out.reshape(-1)
+        nda, smr, fine = shard_band_args(self.nda, *self.reference_band_args(), begin, end)
+        sw = np.zeros(ns, np.float32)
+        sw[:n] = self.sw[begin:end]
+        return Sample(cut(self.pp, 111), cut(self.pp1, 96), cut(self.pp2, 96), sw, n, ns, nda, smr + 1, fine,
+                      self.sum_w_mc, self.sum_w_data, self.sum_w2_data,
+                      None if self.pp3 is None else cut(self.pp3, 97), None if self.pp4 is None else cut(self.pp4, 96))
+
 
 def events_from_angles(ang: dict) -> tuple:
     bas = B.fill_basis(ang)

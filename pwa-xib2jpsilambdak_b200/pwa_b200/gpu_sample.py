@@ -34,6 +34,19 @@ class DeviceSample:
     def reference_band_args(self):
         return self.nda_smr1 - 1, self.nda_fine
 
+    @classmethod
+    def from_host(cls, sample, device: int = 0) -> "DeviceSample":
+        """Device copy of a host Sample (dataset.Sample, reference layout)."""
+        import torch
+        dev = torch.device("cuda", device)
+        ns = sample.n_size
+
+        def planes(a, rows):
+            return torch.as_tensor(np.asarray(a, np.float32).reshape(rows, ns), device=dev)
+        return cls(planes(sample.pp, 111), planes(sample.pp1, 96), planes(sample.pp2, 96),
+                   torch.as_tensor(np.asarray(sample.sw, np.float32), device=dev), sample.n, ns, sample.nda,
+                   sample.nda_smr1, sample.nda_fine, sample.sum_w_mc, sample.sum_w_data, sample.sum_w2_data)
+
     def to_host(self, data_idx=None, mc_idx=None):
         """Host Sample (dataset.Sample) of a subset: data columns data_idx (in band order) and MC
         columns mc_idx (relative to the MC block)."""

@@ -86,7 +86,8 @@ def ref_nll():
     from pwa_b200 import configs, dataset as D, model as M
     rows = []
     for name, nd, nm, seed in (("small_kmatrix", 1500, 15000, 21), ("small_bw", 1500, 15000, 22),
-                               ("kmatrix", 1000, 10000, 23), ("lstar_only", 1000, 10000, 24)):
+                               ("kmatrix", 1000, 10000, 23), ("lstar_only", 1000, 10000, 24),
+                               ("full_bw", 1000, 10000, 25)):
         mdl, vals = configs.MODELS[name]()
         blk = M.build_param_block(mdl, vals)
 
@@ -117,11 +118,12 @@ def func_example():
 
 
 if __name__ == "__main__":
-    smear()
-    c2()
-    L = aux()
-    cg(L)
-    dfun(L)
-    func_example()
+    if "--nll-only" not in sys.argv:
+        smear()
+        c2()
+        L = aux()
+        cg(L)
+        dfun(L)
+        func_example()
     ref_nll()
     print("fixtures written to", HERE)

@@ -23,10 +23,13 @@ def test_oracle_reproduces_golden(row, oracle_mod):
     assert abs(row["sumint_reference_fp32"] / s - 1) < 5e-5
 
 
-@pytest.mark.parametrize("name", ["small_kmatrix", "small_bw", "small_zcs"])
+BUCKETS = {"small_kmatrix": (3, 4, 0), "small_bw": (2, 2, 0), "small_zcs": (2, 1, 2), "kmatrix": (6, 12, 0),
+           "full_bw": (14, 3, 0)}
+
+
+@pytest.mark.parametrize("name", ["small_kmatrix", "small_bw", "small_zcs", "kmatrix", "full_bw"])
 def test_oracle_vs_reference_live(name, oracle_mod):
-    L = oracle_mod.ref_lib(*{"small_kmatrix": (3, 4, 0), "small_bw": (2, 2, 0), "small_zcs": (2, 1, 2)}[name],
-                           build_if_missing=True)
+    L = oracle_mod.ref_lib(*BUCKETS[name], build_if_missing=True)
     if L is None:
         pytest.skip("reference host build unavailable")
     mdl, vals, blk, smp = make_test_sample(name, 600, 6000, seed=31)
@@ -34,8 +37,12 @@ def test_oracle_vs_reference_live(name, oracle_mod):
     ref = oracle_mod.RefHost(smp, blk)
     rv, rs = ref.store_fx(blk)
     rel = np.abs(ref.fx - fx) / np.abs(fx)
-    assert np.median(rel) < 1e-5 and np.max(rel) < 2e-3
-    assert abs(rv - v) < 0.05
+    assert np.median(rel) < 1e-5
+    # per-event maxima sit on steep lineshape structures (see the next test); the K-matrix model has
+    # structures steep enough for FP32 rounding of the mass to move |A|^2 by percent
+    assert np.max(rel) < (0.1 if name == "kmatrix" else 2e-3)
+    # those events move the reference's FP32 NLL of the K-matrix model by ~0.1 already at 6.6k events
+    assert abs(rv - v) < (0.2 if name == "kmatrix" else 0.05)
     # swapping the coupling read order breaks agreement by orders of magnitude
     v2, _, _, _ = oracle_mod.nll(smp, blk, swap_coupling_parts=True)
     assert abs(rv - v2) > 100 * abs(rv - v)
@@ -52,3 +59,32 @@ def test_oracle_grid_smearing_limits(oracle_mod):
     a2 = oracle_mod.amp2(smp, blk)
     wt = np.where(np.arange(smp.n) < smp.nda, 1.0, np.asarray(smp.pp[2 * smp.n_size:2 * smp.n_size + smp.n], np.float64))
     assert np.max(np.abs(fx - a2 * wt) / (a2 * wt)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["small_kmatrix", "small_bw", "kmatrix", "full_bw"])
+def test_reference_error_is_mass_rounding_noise(name, oracle_mod):
+    """Breakdown of the reference's FP32 deviation from the FP64 oracle by m(J/psi p): every event's
+    relative deviation is bounded by a small multiple of the oracle's own sensitivity to one float ulp
+    of m(J/psi p) (the rounding the reference's float smeared masses carry), and where |A|^2 is not
+    steep in the mass (sensitivity < 1e-6) the deviation stays below 2e-5.  A systematic slip
+    (a wrong threshold, pole or branch) would show deviations that the rounding does not explain."""
+    import copy
+    if oracle_mod.ref_lib(*BUCKETS[name], build_if_missing=True) is None:
+        pytest.skip("reference host build unavailable")
+    mdl, vals, blk, smp = make_test_sample(name, 600, 6000, seed=31)
+    a, b = smp.reference_band_args()
+    fx, _ = oracle_mod.eval_fx(smp, blk, a, b)
+    ref = oracle_mod.RefHost(smp, blk)
+    ref.store_fx(blk)
+    rel = np.abs(ref.fx - fx) / np.abs(fx)
+    ns = smp.n_size
+    sens = np.zeros(smp.n)
+    for direction in (np.inf, -np.inf):
+        s2 = copy.copy(smp)
+        s2.pp = smp.pp.copy()
+        s2.pp[ns:ns + smp.n] = np.nextafter(smp.pp[ns:ns + smp.n], np.float32(direction))
+        f2, _ = oracle_mod.eval_fx(s2, blk, a, b)
+        sens = np.maximum(sens, np.abs(f2 - fx) / np.abs(fx))
+    assert np.all(rel <= 10.0 * (sens + 1e-6)), np.max(rel / (sens + 1e-6))
+    flat = sens < 1e-6
+    assert flat.sum() > 0.5 * smp.n and np.max(rel[flat]) < 2e-5
