@@ -46,7 +46,8 @@ def reference_tree() -> Path:
 CUDA_INC = "/usr/local/cuda/include"
 
 # Model-size buckets used by the tests and the bench (NR, NZ, NX, max_ikmcount).
-DEFAULT_BUCKETS = [(6, 0, 0, 6), (6, 12, 0, 6), (14, 3, 0, 6), (3, 4, 0, 6), (2, 2, 0, 6), (2, 1, 2, 6)]
+DEFAULT_BUCKETS = [(6, 0, 0, 6), (6, 12, 0, 6), (14, 3, 0, 6), (3, 4, 0, 6), (2, 2, 0, 6), (2, 1, 2, 6),
+                   (5, 5, 0, 6)]
 
 LAUNCH_RE = re.compile(r"(\b\w+)<<<\s*([^,>]+?)\s*,\s*([^>]+?)\s*>>>\s*\(")
 COUPLING_RE = re.compile(

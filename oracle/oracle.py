@@ -63,6 +63,11 @@ def lib():
         for f in ("oracle_barrier_lb_lstar", "oracle_barrier_lb_pc"):
             getattr(L, f).restype = C.c_double
             getattr(L, f).argtypes = [C.c_double] * 4
+        L.oracle_lineshapes.restype = C.c_int
+        L.oracle_lineshapes.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_double, C.c_double, _dp, _dp]
+        L.oracle_lineshapes_lstar_km.restype = C.c_int
+        L.oracle_lineshapes_lstar_km.argtypes = [_fp, C.c_int, C.c_int, C.c_float, _fp, _dp, _dp, _dp, _dp]
         L.oracle_kmatrix.restype = C.c_int
         L.oracle_kmatrix.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_int, _dp]
@@ -145,6 +150,32 @@ def amp2(sample, block, threads: int | None = None) -> np.ndarray:
     return out
 
 
+def lineshapes(block, mkp: float, mz: float) -> tuple:
+    """Every Lambda* lineshape times its production barrier at mkp and every Pc lineshape times its
+    barrier at mz (complex arrays of NR and NZ), as the amplitude uses them."""
+    pl = np.ascontiguousarray(block.data, np.float32)
+    ls = np.zeros(2 * max(block.NR, 1))
+    pc = np.zeros(2 * max(block.NZ, 1))
+    rc = lib().oracle_lineshapes(pl.ctypes.data_as(_fp), block.para_size, block.vamp_size, block.spline_size,
+                                 block.NR, block.NZ, block.ffr, block.ffb, mkp, mz, ls.ctypes.data_as(_dp),
+                                 pc.ctypes.data_as(_dp))
+    if rc != 0:
+        raise RuntimeError(f"oracle_lineshapes failed: {rc}")
+    return ls[0::2][:block.NR] + 1j * ls[1::2][:block.NR], pc[0::2][:block.NZ] + 1j * pc[1::2][:block.NZ]
+
+
+def lineshapes_lstar_km(block, mkp) -> tuple:
+    """host_store_lineshapeLsKM's outputs (revised K-matrix and Breit-Wigner lineshape of every Lambda*
+    entry, each times the Lambda_b barrier with radius FFR) as complex [NR, n] arrays."""
+    m = np.ascontiguousarray(mkp, np.float32)
+    n, nr = len(m), block.NR
+    out = [np.zeros(n * nr) for _ in range(4)]
+    pl = np.ascontiguousarray(block.data, np.float32)
+    lib().oracle_lineshapes_lstar_km(m.ctypes.data_as(_fp), n, nr, block.ffr, pl.ctypes.data_as(_fp),
+                                     *[o.ctypes.data_as(_dp) for o in out])
+    return (out[0] + 1j * out[1]).reshape(nr, n), (out[2] + 1j * out[3]).reshape(nr, n)
+
+
 def assemble_nll(sample, fx, fxn) -> tuple:
     out = C.c_double()
     sw = np.ascontiguousarray(sample.sw, np.float32)
@@ -187,6 +218,8 @@ def ref_lib(NR: int, NZ: int, NX: int = 0, ikm: int = 6, build_if_missing: bool 
                                         C.c_double, C.c_double, C.c_float, C.c_float, C.c_int, C.c_int]
         L.ref_host_store_amp2s.argtypes = [_fp, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int, _dp, C.c_int,
                                            C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.ref_host_store_lineshapeLsKM.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_float,
+                                                   _fp, C.c_int, C.c_int, C.c_int]
         _ref_libs[key] = L
     return _ref_libs[key]
 
@@ -231,3 +264,23 @@ class RefHost:
                                     out.ctypes.data_as(_dp), self.s.n, block.NR, block.NZ, block.NX, block.ffr,
                                     block.ffb)
         return out
+
+
+def ref_lineshapes_lstar_km(block, mkp) -> tuple:
+    """The reference's own host_store_lineshapeLsKM (FP32, host build) as complex [NR, n] arrays; n must
+    be a multiple of 32 (its kernel has no bounds check)."""
+    L = ref_lib(block.NR, block.NZ, block.NX)
+    if L is None:
+        raise FileNotFoundError("reference host build unavailable")
+    m = np.ascontiguousarray(mkp, np.float32)
+    n, nr = len(m), block.NR
+    if n % 32:
+        raise ValueError("n must be a multiple of 32")
+    out = [np.zeros(n * nr, np.float32) for _ in range(4)]
+    pl = np.ascontiguousarray(block.data, np.float32).copy()
+    L.ref_configure(pl.ctypes.data_as(_fp), block.para_size)
+    L.ref_host_store_lineshapeLsKM(m.ctypes.data_as(_fp), *[o.ctypes.data_as(_fp) for o in out], n, nr, nr,
+                                   block.ffr, pl.ctypes.data_as(_fp), block.para_size, block.vamp_size,
+                                   block.spline_size)
+    return ((out[0] + 1j * out[1]).reshape(nr, n).astype(complex),
+            (out[2] + 1j * out[3]).reshape(nr, n).astype(complex))

@@ -49,7 +49,13 @@ constexpr double MRES2 = F(-0.00655841f);
 // Parameter table layout (Resonances.h:97-112).
 constexpr int NSET = 6;
 enum { P_MASS = 0, P_WIDTH, P_SPIN, P_LRESON, P_TYPE, P_PARITY };
-enum { T_BREITWIGNER = 1, T_KMATRIX = 240, T_NONRESONANT = 361 };
+enum { T_BREITWIGNER = 1, T_MODELINDEPENDENT = 3, T_TRIANGLE = 7, T_KMATRIX = 240, T_REVISEDKMATRIX = 360,
+       T_NONRESONANT = 361 };
+// Spline knots of the Lambda* and Pc model-independent waves (Resonances.h:5-6); a spline block holds
+// the knots, then 4 coefficients per knot of the real part, then 4 of the imaginary part.
+constexpr int NUMSP = 24;
+constexpr int NUMSPZ = 11;
+constexpr double M_CHIC1 = F(3.51067f);  // cu_DPFPropogator.cu:15
 constexpr int NPMAX = 4;
 constexpr int NKMC = 4;
 
@@ -245,6 +251,196 @@ cd bw_x(double m_r, double gamma_r, double mpp, int LR, double ffr) {  // BW_AMP
   return factor * breit_wigner(m_r, gamma, mpp * mpp);
 }
 
+// ---------------------------------------------------------------- spline waves (cu_DPFPropogator.cu:1118-1221)
+// Piecewise cubic in (x - knot) from a spline block: knots poly[0 .. n), real-part coefficients
+// poly[n + 4k ..], imaginary-part coefficients poly[5n + 4k ..]; zero outside [xmin, xmax]; the
+// interval is found by the reference's bisection over the knots (ModelIndependentWave3 for the
+// Lambda* chain with n = NUMSP, ModelIndependentWave for the Pc chain with n = NUMSPZ).
+cd spline_wave(const float* poly, int n, double xmin, double xmax, double x) {
+  if (x < xmin || x > xmax) return cd(0, 0);
+  int klow = 0, khig = n - 1;
+  if (x <= xmin) {
+    klow = 0;
+  } else if (x >= xmax) {
+    klow = khig;
+  } else {
+    while (khig - klow > 1) {
+      const int khalf = (klow + khig) / 2;
+      if (x > poly[khalf])
+        klow = khalf;
+      else
+        khig = khalf;
+    }
+  }
+  const double dx = x - poly[klow];
+  const float* a = poly + n + 4 * klow;
+  const float* b = a + 4 * n;
+  return cd(a[0] + dx * (a[1] + dx * (a[2] + dx * a[3])), b[0] + dx * (b[1] + dx * (b[2] + dx * b[3])));
+}
+// Domains: float sums of the reference (m_p + m_k - 0.002f etc.).
+const double SPL_LSTAR_LO = (double)(0.938272046f + 0.493677f - 0.002f);
+const double SPL_LSTAR_HI = (double)(5.61951f - 3.096916f + 0.002f);
+const double SPL_PC_LO = (double)(0.938272046f + 3.096916f - 0.002f);
+const double SPL_PC_HI = F(4.6f);
+
+// ---------------------------------------------------------------- revised K-matrix (cu_DPFPropogator.cu:825-1115)
+// Effective mass of a resonance for its reference momentum (the tanh map below threshold, the
+// midpoint for non-resonant entries).
+double eff_mass(double m_r, double thr, double mmax) {
+  if (m_r > thr) return m_r;
+  if (m_r >= 0) return thr + 0.5 * (mmax - thr) * (1.0 + std::tanh((m_r - (thr + mmax) / 2.0) / (mmax - thr)));
+  return (thr + mmax) / 2.0;
+}
+
+// KMatrixTerm: the term of another entry of the same J^P (always with the p K masses, whichever
+// chain calls it).  The first non-resonant entry (m_r < 0) fixes fsc, which every later one returns.
+double kmatrix_term(double m_r, double gamma_r, double mpp, int LR, double& fsc, double ffr) {
+  const double s = mpp * mpp;
+  const double pR = two_body_p(mpp, M_P, M_K);
+  const double pR0 = two_body_p(eff_mass(m_r, M_P + M_K, M_LB - M_JPSI), M_P, M_K);
+  const double FR = barrier_ratio(ffr, LR, pR, pR0);
+  const double gamma = gamma_r * std::pow(pR / pR0, 2 * LR + 1) * (m_r / mpp) * FR * FR;
+  if (m_r < 0) {
+    if (std::fabs(fsc) < 1e-10) fsc = gamma;
+    return fsc;
+  }
+  if (std::fabs(m_r * m_r - s) < 1e-10) return 0;
+  return m_r * gamma / (m_r * m_r - s);
+}
+
+struct Entry {
+  double m, g;
+  int S2, LR, type, P;
+};
+inline Entry entry(const float* pl, int r) {
+  const float* q = pl + r * NSET;
+  return Entry{q[P_MASS], q[P_WIDTH], (int)q[P_SPIN], (int)q[P_LRESON], (int)q[P_TYPE], (int)q[P_PARITY]};
+}
+
+// Revised_KMAMP: entry nr coupled to the entries [irst, ired) of its type, spin and parity.
+cd revised_km(const float* pl, double mpp, int nr, int irst, int ired, bool pc_chain, double ffr) {
+  const double s = mpp * mpp;
+  const double m1 = pc_chain ? M_JPSI : M_P, m2 = pc_chain ? M_P : M_K, m3 = pc_chain ? M_K : M_JPSI;
+  const Entry R = entry(pl, nr);
+  double totG = 0, fsc = 0, denorm = 1;
+  if (R.m > 0) denorm = R.m * R.m - s;
+  for (int ir = irst; ir < ired; ++ir) {
+    const Entry E = entry(pl, ir);
+    if (E.type == R.type && E.S2 == R.S2 && E.P == R.P) {
+      if (ir == nr) continue;
+      totG += kmatrix_term(E.m, E.g, mpp, E.LR, fsc, ffr) * denorm;
+    }
+  }
+  const double pR = two_body_p(mpp, m1, m2);
+  double pR0 = two_body_p(eff_mass(R.m, m1 + m2, M_LB - m3), m1, m2);
+  double FR = barrier_ratio(ffr, R.LR, pR, pR0);
+  double factor = FR * std::pow(pR / pR0, R.LR);
+  if (R.m > 0) {
+    double gamma = R.g;
+    if (R.m > m1 + m2) gamma = R.g * std::pow(pR / pR0, 2 * R.LR + 1) * (R.m / mpp) * FR * FR;
+    if (R.m < m1 + m2) {  // the Sigma pi channel of the reference (written for the Lambda(1405))
+      const double msig = F(1.18937f), mpi0 = F(0.13957018f);
+      const double pRSigPi = two_body_p(mpp, msig, mpi0);
+      pR0 = two_body_p(R.m, msig, mpi0);
+      FR = 1.0;
+      gamma = R.g * std::pow(pR / pR0, 2 * R.LR + 1) * (R.m / mpp);
+      const double sp = F(0.0505f) * std::pow(pRSigPi / pR0, 2 * R.LR + 1) * (R.m / mpp);
+      gamma += sp;
+      denorm -= fsc * sp * R.m;
+    }
+    totG += R.m * gamma;
+    const double kr = std::sqrt(R.m * R.m + R.g * R.g);
+    factor *= F(0.948850f) * R.m * std::sqrt(R.g * kr / std::sqrt(R.m * (R.m + kr)));
+  } else {
+    totG += R.g * std::pow(pR / pR0, 2 * R.LR + 1) * (R.m / mpp) * FR * FR;
+  }
+  const double d2 = denorm * denorm + totG * totG;
+  return cd(denorm / d2, totG / d2) * factor;
+}
+
+// Revised_KMAMP_refactor (the form storeLineshapeLsKM evaluates): products of the other entries'
+// (m_j^2 - s) instead of the per-term division.
+cd revised_km_refactor(const float* pl, double mpp, int nr, int irst, int ired, bool pc_chain, double ffr) {
+  const double s = mpp * mpp;
+  const double m1 = pc_chain ? M_JPSI : M_P, m2 = pc_chain ? M_P : M_K, m3 = pc_chain ? M_K : M_JPSI;
+  const Entry R = entry(pl, nr);
+  auto prod_delta = [&](int ir, const Entry& X) {  // product_delta_S
+    double pr = 1;
+    for (int j = irst; j < ired; ++j) {
+      if (j == ir) continue;
+      const Entry E = entry(pl, j);
+      if (E.type == X.type && E.S2 == X.S2 && E.P == X.P) pr *= E.m * E.m - s;
+    }
+    return pr;
+  };
+  double fsc = 0;
+  const double pR = two_body_p(mpp, m1, m2);
+  const double pR0 = two_body_p(eff_mass(R.m, m1 + m2, M_LB - m3), m1, m2);
+  const double FR = barrier_ratio(ffr, R.LR, pR, pR0);
+  const double gamma = R.g * std::pow(pR / pR0, 2 * R.LR + 1) * (R.m / mpp) * FR * FR;
+  const double pds_r = prod_delta(nr, R);
+  const double pds_all = pds_r * (R.m * R.m - s);
+  double sum = pds_r * R.m * gamma;
+  for (int ir = irst; ir < ired; ++ir) {
+    if (ir == nr) continue;
+    const Entry E = entry(pl, ir);
+    if (E.S2 == R.S2 && E.P == R.P && E.type == R.type) {
+      // m_gamma with the p K masses
+      const double qR = two_body_p(mpp, M_P, M_K);
+      const double qR0 = two_body_p(eff_mass(E.m, M_P + M_K, M_LB - M_JPSI), M_P, M_K);
+      const double fr = barrier_ratio(ffr, E.LR, qR, qR0);
+      const double g = E.g * std::pow(qR / qR0, 2 * E.LR + 1) * (E.m / mpp) * fr * fr;
+      double mg;
+      if (E.m < 0) {
+        if (std::fabs(fsc) < 1e-10) fsc = g;
+        mg = fsc * (E.m * E.m - mpp * mpp);
+      } else {
+        mg = E.m * g;
+      }
+      sum += mg * prod_delta(ir, E);
+    }
+  }
+  const double den = pds_all * pds_all + sum * sum;
+  const double kr = std::sqrt(R.m * R.m + R.g * R.g);
+  const double factor = FR * std::pow(pR / pR0, R.LR) * F(0.948850f) * R.m * std::sqrt(R.g * kr / std::sqrt(R.m * (R.m + kr)));
+  return cd(pds_r * pds_all / den, pds_r * sum / den) * factor;
+}
+
+// ---------------------------------------------------------------- triangle cusp (cu_DPFPropogator.cu:1223-1343)
+// The reference's complex logarithm and arctangent (RooTDalitz/cuComplex.h:660-676): the argument
+// from acos(Re / |z|), negative for Im < 0; atan(z) = -i/2 log((1 + i z) / (1 - i z)).
+cd clog_ref(cd x) {
+  const double r = std::sqrt(x.real() * x.real() + x.imag() * x.imag());
+  double th = std::acos(x.real() / r);
+  if (x.imag() < 0) th = -th;
+  return cd(std::log(r), th);
+}
+cd catan_ref(cd x) {
+  const cd ii(0, 1);
+  return -0.5 * (ii * clog_ref((1.0 + ii * x) / (1.0 - ii * x)));
+}
+
+cd cusp_amp(double m_r, double gamma, double mpp) {  // GetCusp_AMP
+  const cd ii(0, 1);
+  const double p12 = M_LB, p13 = M_K;
+  const cd m1(m_r, -gamma / 2.0);
+  const double m2 = M_CHIC1, m3 = M_P;
+  const double p23 = mpp;
+  cd integral(0, 0);
+  const int bins = 100;
+  const double dx = F(1.f / bins);
+  for (int i = 0; i < bins; ++i) {
+    const double alpha = (double)((float)i * (float)dx + (float)dx / 2.0f);
+    const cd b = (alpha * (p12 * p12 - p13 * p13 - p23 * p23) + m3 * m3 - m2 * m2) / p23 / p23 + 1.0 - 0.001 * ii;
+    const cd c = (alpha * (m1 * m1 - m3 * m3) + m3 * m3 - alpha * (1.0 - alpha) * p13 * p13) / (p23 * p23);
+    const cd sv = csqrt_branch(4.0 * c - b * b);
+    const cd t1 = catan_ref(b / sv);
+    const cd t2 = catan_ref((b + 2.0 * (alpha - 1.0)) / sv);
+    integral += dx * ((1.0 / sv) * (t1 - t2));
+  }
+  return integral * (1.0 / mpp / mpp);
+}
+
 // ---------------------------------------------------------------- K-matrix (cu_DPFPropogator.cu:588-813)
 // First row of the inverse of a complex n x n matrix S, via an unpivoted LU of S^T with b = e0
 // (RooTDalitz/cuSolve4x4.h:278-353 uses this construction).
@@ -285,6 +481,7 @@ struct Model {
   int kmcount = 0;
   std::vector<int> ampcount;  // first coupling index of each resonance
   std::vector<int> ikmslot;   // K-matrix output slot of each Pc entry
+  std::vector<int> splcount;  // first float of each resonance's spline block
   bool swap_coupling_parts = false;
 };
 
@@ -336,6 +533,13 @@ void configure(Model& m) {
     }
   }
   m.kmcount = m.para_size + m.vamp_size + m.spline_size;
+  // spline blocks follow the couplings (cuda_configure_splcount, kernel_calEva.cu:1100-1135)
+  m.splcount.assign(m.NR + m.NZ, 0);
+  int sc = m.para_size + m.vamp_size;
+  for (int r = 0; r < m.NR + m.NZ; ++r) {
+    m.splcount[r] = sc;
+    if ((int)pl[r * NSET + P_TYPE] == T_MODELINDEPENDENT) sc += 9 * (r < m.NR ? NUMSP : NUMSPZ);
+  }
 }
 
 // One J^P group of the coupled-channel Pc K-matrix at invariant mass mpp.  Writes Npole + 4 P-vector
@@ -460,12 +664,18 @@ bool amp_lstar(const Model& md, const Ev& e, cd* H) {
     const int S2 = (int)q[P_SPIN], LR = (int)q[P_LRESON], type = (int)q[P_TYPE];
     const double S = 0.5 * S2;
     cd bw(0, 0);
-    if (type == T_BREITWIGNER)
+    if (type == T_BREITWIGNER) {
       bw = bw_lstar(m0, g0, mkp, LR, md.FFR);
-    else if (type == T_NONRESONANT)
+    } else if (type == T_NONRESONANT) {
       bw = cd(1, 0);
-    else
-      return false;  // spline / revised K-matrix Lambda* lineshapes are not restated here
+    } else if (type == T_MODELINDEPENDENT) {
+      bw = spline_wave(md.pl + md.splcount[r], NUMSP, SPL_LSTAR_LO, SPL_LSTAR_HI, mkp);
+      m0 = -0.5;  // the production barrier of a spline wave is the non-resonant one
+    } else if (type == T_REVISEDKMATRIX) {
+      bw = revised_km(md.pl, mkp, r, 0, md.NR, false, md.FFR);
+    } else {
+      return false;
+    }
     bw *= barrier_lb_lstar(S, mkp, m0, md.FFB);
     int cnt = md.ampcount[r];
     const int s = (S2 - 1) / 2;
@@ -570,6 +780,13 @@ bool pc_lineshapes(const Model& md, double mz, double weight, cd* bw) {
     cd b(0, 0);
     if (type == T_BREITWIGNER) {
       b = bw_pc(m0, g0, mz, LR, md.FFR);
+    } else if (type == T_MODELINDEPENDENT) {
+      b = spline_wave(md.pl + md.splcount[md.NR + i], NUMSPZ, SPL_PC_LO, SPL_PC_HI, mz);
+      m0 = -0.5;
+    } else if (type == T_REVISEDKMATRIX) {
+      b = revised_km(md.pl, mz, md.NR + i, md.NR, md.NR + md.NZ, true, md.FFR);
+    } else if (type == T_TRIANGLE) {
+      b = cusp_amp(m0, g0, mz);
     } else if (type == T_KMATRIX) {
       const int ik = pc_group(S2, LR);
       if (!have[ik]) {
@@ -857,6 +1074,71 @@ int oracle_kmatrix(const float* paraList, int para_size, int vamp_size, int spli
     out[2 * i + 1] = M[i].imag();
   }
   return n;
+}
+
+// host_store_lineshapeLsKM (kernel_calEva.cu:1490-1584): for every Lambda* entry iLz < NR and mass
+// h_mkp[i], the revised K-matrix lineshape in its refactored form times the Lambda_b barrier, and the
+// Breit-Wigner times the same barrier; both barriers with radius FFR, as the reference calls them.
+// Outputs [iLz * n_points + i].
+int oracle_lineshapes_lstar_km(const float* h_mkp, int n_points, int NR, float FFR, const float* paraList,
+                               double* km_re, double* km_im, double* bw_re, double* bw_im) {
+  for (int i = 0; i < n_points; ++i) {
+    const double mkp = h_mkp[i];
+    for (int r = 0; r < NR; ++r) {
+      const Entry E = entry(paraList, r);
+      const double bt = barrier_lb_lstar(0.5 * E.S2, mkp, E.m, FFR);
+      const cd km = revised_km_refactor(paraList, mkp, r, 0, NR, false, FFR) * bt;
+      const cd bw = bw_lstar(E.m, E.g, mkp, E.LR, FFR) * bt;
+      km_re[r * n_points + i] = km.real();
+      km_im[r * n_points + i] = km.imag();
+      bw_re[r * n_points + i] = bw.real();
+      bw_im[r * n_points + i] = bw.imag();
+    }
+  }
+  return 0;
+}
+
+// Every Lambda* lineshape times its production barrier at mkp (lstar: 2 NR doubles) and every Pc
+// lineshape times its barrier at mz (pc: 2 NZ doubles), as the amplitude kernels use them.
+int oracle_lineshapes(const float* paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                      float FFR, float FFB, double mkp, double mz, double* lstar, double* pc) {
+  Model md;
+  md.pl = paraList;
+  md.para_size = para_size;
+  md.vamp_size = vamp_size;
+  md.spline_size = spline_size;
+  md.NR = NR;
+  md.NZ = NZ;
+  md.FFR = FFR;
+  md.FFB = FFB;
+  configure(md);
+  for (int r = 0; r < NR; ++r) {
+    const Entry E = entry(paraList, r);
+    double m0 = E.m;
+    cd bw(1, 0);
+    if (E.type == T_BREITWIGNER) {
+      bw = bw_lstar(E.m, E.g, mkp, E.LR, FFR);
+    } else if (E.type == T_MODELINDEPENDENT) {
+      bw = spline_wave(paraList + md.splcount[r], NUMSP, SPL_LSTAR_LO, SPL_LSTAR_HI, mkp);
+      m0 = -0.5;
+    } else if (E.type == T_REVISEDKMATRIX) {
+      bw = revised_km(paraList, mkp, r, 0, NR, false, FFR);
+    } else if (E.type != T_NONRESONANT) {
+      return -1;
+    }
+    bw *= barrier_lb_lstar(0.5 * E.S2, mkp, m0, FFB);
+    lstar[2 * r] = bw.real();
+    lstar[2 * r + 1] = bw.imag();
+  }
+  if (NZ > 0) {
+    std::vector<cd> b(NZ);
+    if (!pc_lineshapes(md, mz, 1.0, b.data())) return -2;
+    for (int i = 0; i < NZ; ++i) {
+      pc[2 * i] = b[i].real();
+      pc[2 * i + 1] = b[i].imag();
+    }
+  }
+  return 0;
 }
 
 }  // extern "C"

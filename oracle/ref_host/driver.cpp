@@ -22,6 +22,8 @@ void cuda_configure_ampcount(const float*, const int);
 void cuda_configure_smear();
 void host_store_amp2s(std::vector<float*>, std::vector<float*>, std::vector<float*>, std::vector<float*>,
                       std::vector<float*>, float*, int, int, int, double*, int, int, int, int, int, float, float);
+void host_store_lineshapeLsKM(const float*, float*, float*, float*, float*, const int, const int, const int,
+                              const float, float*, const int, const int, const int);
 
 extern "C" {
 
@@ -64,5 +66,14 @@ void ref_host_store_amp2s(float* pp, float* pp1, float* pp2, float* pp3, float* 
                           int NX, float ffr, float ffb) {
   host_store_amp2s({pp}, {pp1}, {pp2}, {pp3}, {pp4}, h_paraList, para_size, vamp_size, spline_size, out, n, 0,
                    NR, NZ, NX, ffr, ffb);
+}
+
+// Lambda* lineshape diagnostic (host_store_lineshapeLsKM, kernel_calEva.cu:1545-1584).  Its kernel
+// has no bounds check: n_points must be a multiple of its 32-thread blocks.
+void ref_host_store_lineshapeLsKM(const float* mkp, float* km_re, float* km_im, float* bw_re, float* bw_im,
+                                  int n_points, int NR, int nLz, float ffr, float* h_paraList, int para_size,
+                                  int vamp_size, int spline_size) {
+  host_store_lineshapeLsKM(mkp, km_re, km_im, bw_re, bw_im, n_points, NR, nLz, ffr, h_paraList, para_size,
+                           vamp_size, spline_size);
 }
 }

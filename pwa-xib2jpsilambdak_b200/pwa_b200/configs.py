@@ -9,7 +9,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .model import BREITWIGNER, KMATRIX, NONRESONANT, Model, Resonance
+from .model import (BREITWIGNER, KMATRIX, MODELINDEPENDENT, NONRESONANT, NUMSP, NUMSPZ, REVISEDKMATRIX, TRIANGLE,
+                    Model, Resonance)
 
 # name, mass, width, 2J, parity
 LSTAR_ALL = [
@@ -70,6 +71,51 @@ def zcs_bw(name: str, s2: int, par: int) -> Resonance:
     # RooTDalitz/ResX.h: four Lambda_b -> Zcs p couplings (L0..L3), then the Zcs -> J/psi K one (Bp)
     coup = tuple(f"{ap}_{t}_{name}" for t in ("L0", "L1", "L2", "L3", "Bp") for ap in ("a", "p"))
     return Resonance("X", name, s2, par, BREITWIGNER, f"m0_{name}", f"width_{name}", coup)
+
+
+def _lstar_couplings(name: str) -> tuple:
+    coup = []
+    for t in ("p1p1", "p100", "m100", "m1m1", "p3p1", "m3m1"):
+        coup += [f"a_{t}_{name}", f"p_{t}_{name}"]
+    return tuple(coup)
+
+
+def lstar_spline(name: str, knot_masses) -> Resonance:
+    """Model-independent S-wave (2J = 1, parity -1) of the Lambda* chain: NUMSP spline knots with real
+    and imaginary parameters SR_/SI_ at fixed masses (RooTDalitz/ResL.h:1139-1180)."""
+    if len(knot_masses) != NUMSP:
+        raise ValueError(f"a Lambda* spline wave has {NUMSP} knots")
+    knots = tuple((f"SR_{name}_{i:02d}", f"SI_{name}_{i:02d}", float(m)) for i, m in enumerate(knot_masses))
+    return Resonance("L", name, 1, -1, MODELINDEPENDENT, f"m0_{name}", f"width_{name}", _lstar_couplings(name),
+                     ("scRe", "scIm"), knots)
+
+
+def lstar_rkm(name: str, s2: int, par: int, mass="", width="") -> Resonance:
+    """Lambda* entry of a revised K-matrix (type REVISEDKMATRIX): the entries of one type, spin and
+    parity form one coupled set (RooTDalitz/ResL_KM.h)."""
+    return Resonance("L", name, s2, par, REVISEDKMATRIX, mass or f"m0_{name}", width or f"width_{name}",
+                     _lstar_couplings(name), ("scRe", "scIm"))
+
+
+def pc_rkm(name: str, s2: int, par: int) -> Resonance:
+    """Pc entry of a revised K-matrix (RooTDalitz/ResZKM.h:340-360, the L_Z2BW list)."""
+    coup = tuple(f"{ap}_{t}_{name}" for t in ("Bp", "L0", "L1", "L2") for ap in ("a", "p"))
+    return Resonance("Z", name, s2, par, REVISEDKMATRIX, f"m0_{name}", f"width_{name}", coup)
+
+
+def pc_cusp(name: str, s2: int, par: int) -> Resonance:
+    """Pc-chain triangle cusp (type TRIANGLE, GetCusp_AMP): mass and width of the particle in the loop."""
+    coup = tuple(f"{ap}_{t}_{name}" for t in ("Bp", "L0", "L1", "L2") for ap in ("a", "p"))
+    return Resonance("Z", name, s2, par, TRIANGLE, f"m0_{name}", f"width_{name}", coup)
+
+
+def pc_spline(name: str, s2: int, par: int, knot_masses) -> Resonance:
+    """Model-independent wave of the Pc chain: NUMSPZ knots (MakeSplineZ)."""
+    if len(knot_masses) != NUMSPZ:
+        raise ValueError(f"a Pc spline wave has {NUMSPZ} knots")
+    coup = tuple(f"{ap}_{t}_{name}" for t in ("Bp", "L0", "L1", "L2") for ap in ("a", "p"))
+    knots = tuple((f"SR_{name}_{i:02d}", f"SI_{name}_{i:02d}", float(m)) for i, m in enumerate(knot_masses))
+    return Resonance("Z", name, s2, par, MODELINDEPENDENT, f"m0_{name}", f"width_{name}", coup, (), knots)
 
 
 def _seed_couplings(model: Model, vals: dict, rng, scale=1.0):
@@ -196,8 +242,49 @@ def small_bw(seed: int = 5) -> tuple:
     return m, vals
 
 
+# Knot masses of the Lambda* S-wave (24 knots from just above the pK threshold to the upper edge) and
+# of the Pc spline wave (11 knots over the m(J/psi p) range the reference's Pc spline covers).
+SWAVE_KNOTS = (1.435, 1.44, 1.45, 1.5, 1.525, 1.55, 1.575, 1.6, 1.625, 1.65, 1.675, 1.7, 1.75, 1.8, 1.85, 1.9,
+               1.95, 2.0, 2.05, 2.1, 2.2, 2.3, 2.4, 2.5)
+PC_SPLINE_KNOTS = (4.04, 4.1, 4.2, 4.25, 4.3, 4.35, 4.4, 4.45, 4.5, 4.55, 4.6)
+
+
+def lineshapes(seed: int = 8, swave=None) -> tuple:
+    """Every lineshape type the reference kernels dispatch on besides Breit-Wigners and the coupled-
+    channel K-matrix: a Lambda* S-wave spline, a Lambda* revised K-matrix of three 1/2- entries (one
+    below the pK threshold, one non-resonant), a Pc revised K-matrix pair (3/2-), a Pc triangle cusp and
+    a Pc spline wave, next to a Breit-Wigner of each chain.  swave: optional NUMSP (Re, Im) knot values
+    of the S-wave (default: a smooth seeded shape)."""
+    lst = [lstar_resonance("1520"), lstar_spline("S01", SWAVE_KNOTS), lstar_rkm("1405", 1, -1),
+           lstar_rkm("1670", 1, -1), lstar_rkm("NRK", 1, -1, mass=-0.5)]
+    pcs = [pc_bw("Pc4312", 1, -1), pc_rkm("Z4440", 3, -1), pc_rkm("Z4457", 3, -1), pc_cusp("T4337", 1, +1),
+           pc_spline("ZS01", 1, -1, PC_SPLINE_KNOTS)]
+    m = Model(lst, pcs)
+    vals = {}
+    _lstar_vals(["1520", "1405", "1670"], vals)
+    vals["m0_S01"], vals["width_S01"] = 0.95, 0.3
+    vals["width_NRK"] = 0.3
+    rng = np.random.default_rng(seed)
+    _seed_couplings(m, vals, rng)
+    for i, x in enumerate(SWAVE_KNOTS):
+        if swave is not None:
+            re, im = swave[i]
+        else:
+            bw = 1.0 / complex(1.7 ** 2 - x * x, -1.7 * 0.25)
+            re, im = 3.0 * bw.real, 3.0 * bw.imag
+        vals[f"SR_S01_{i:02d}"], vals[f"SI_S01_{i:02d}"] = float(re), float(im)
+    for i, x in enumerate(PC_SPLINE_KNOTS):
+        z = 1.0 / complex(4.38 ** 2 - x * x, -4.38 * 0.12)
+        vals[f"SR_ZS01_{i:02d}"], vals[f"SI_ZS01_{i:02d}"] = float(0.5 * z.real), float(0.5 * z.imag)
+    for n, mass, width in (("Pc4312", 4.312, 0.010), ("Z4440", 4.440, 0.020), ("Z4457", 4.457, 0.006),
+                           ("T4337", 1.52, 0.016), ("ZS01", -0.5, 0.0)):
+        vals[f"m0_{n}"], vals[f"width_{n}"] = mass, width
+    return m, vals
+
+
 MODELS = {"lstar_only": lstar_only, "full_bw": full_bw, "kmatrix": kmatrix, "small_kmatrix": small_kmatrix,
-          "small_bw": small_bw, "small_zcs": small_zcs}
+          "small_bw": small_bw, "small_zcs": small_zcs,
+          "lineshapes": lineshapes}
 
 # Workloads: model, data events, MC events, MC weight range.
 WORKLOADS = {

@@ -7,6 +7,10 @@ restate the reference host code that builds it every FCN call:
   (RooDalitzAmplitude::setup_paraList, src/RooDalitzAmplitude.cxx:3068-3139),
 * helicity couplings as (Re, Im) float pairs (ConfigureCouplings :2669-2986, PartWaveCoff :5533-5599,
   PartWaveCoffZ :5601-5710),
+* spline blocks of the model-independent waves (ConfigureCouplings :2738-2765 for the Lambda* chain,
+  the same for the Pc chain with MakeSplineZ :1737-1752): the knot masses, then (y, b, c, d) per
+  knot of the real part, then of the imaginary part, from a cubic spline through the knots with
+  TSpline3's default (not-a-knot) end conditions,
 * K-matrix blocks, per J^P group 16 pole couplings g then the 4x4 scattering matrix f
   (cu_init_data :3141-3210).
 
@@ -25,7 +29,8 @@ from typing import Callable
 
 import numpy as np
 
-BREITWIGNER, MODELINDEPENDENT, KMATRIX, REVISEDKMATRIX, NONRESONANT = 1, 3, 240, 360, 361
+BREITWIGNER, MODELINDEPENDENT, TRIANGLE, KMATRIX, REVISEDKMATRIX, NONRESONANT = 1, 3, 7, 240, 360, 361
+NUMSP, NUMSPZ = 24, 11  # spline knots of the Lambda* and Pc model-independent waves (Resonances.h:5-6)
 NSET, NPMAX, NKMC = 6, 4, 4
 KM_BLOCK = (NPMAX + NKMC) * NKMC  # floats per J^P group
 KM_SIZE = 4 * KM_BLOCK
@@ -170,7 +175,9 @@ class Resonance:
     four Lambda_b -> Zcs p couplings, then the Zcs -> J/psi K ones after the first).
     extra: 'L': (scRe, scIm) names; 'Z' K-matrix pole: g1..g4 names; 'Z' K-matrix NR: (fsc,).
     mass / width: parameter names or constants (for a K-matrix pole the width slot holds the
-    channel index used for the near-threshold mass shift)."""
+    channel index used for the near-threshold mass shift).
+    knots: model-independent (spline) waves only: (Re, Im, mass) references per knot, NUMSP of them
+    for 'L', NUMSPZ for 'Z' (RooDalitzAmplitude::MakeSpline / MakeSplineZ read them in this order)."""
     chain: str
     name: str
     spin2: int
@@ -180,6 +187,11 @@ class Resonance:
     width: str | float
     couplings: tuple
     extra: tuple = ()
+    knots: tuple = ()
+
+    def refs(self) -> list:
+        """Every parameter reference this entry reads."""
+        return [*self.couplings, *self.extra, self.mass, self.width, *(x for k in self.knots for x in k)]
 
 
 @dataclasses.dataclass
@@ -217,7 +229,7 @@ class Model:
     def parameter_names(self) -> list:
         names = []
         for r in self.resonances:
-            for ref in (*r.couplings, *r.extra, r.mass, r.width):
+            for ref in r.refs():
                 if isinstance(ref, str) and ref not in names and ref not in self.derived:
                     names.append(ref)
         return names
@@ -360,6 +372,44 @@ def part_wave_x(lsc: list, parity: int, J: int, lamZ: int, lamPsi: int, lamp: in
     return c * HZ
 
 
+def spline_coefficients(x, y) -> np.ndarray:
+    """[n, 4] coefficients (y, b, c, d) of the cubic spline through (x_i, y_i), S(x) = y_i + b_i t +
+    c_i t^2 + d_i t^3 with t = x - x_i on [x_i, x_i+1], with not-a-knot end conditions (the third
+    derivative continuous at the second and the next-to-last knot: the default end conditions of
+    TSpline3, which follows de Boor's CUBSPL).  The last knot's row continues the last interval's
+    cubic.  Computed in double precision."""
+    x = np.asarray(x, float)
+    y = np.asarray(y, float)
+    n = len(x)
+    if n < 4 or np.any(np.diff(x) <= 0):
+        raise ValueError("a spline needs at least 4 strictly increasing knots")
+    h = np.diff(x)
+    A = np.zeros((n, n))
+    r = np.zeros(n)
+    for i in range(1, n - 1):  # second derivatives M_i: continuity of the first derivative
+        A[i, i - 1], A[i, i], A[i, i + 1] = h[i - 1], 2 * (h[i - 1] + h[i]), h[i]
+        r[i] = 6 * ((y[i + 1] - y[i]) / h[i] - (y[i] - y[i - 1]) / h[i - 1])
+    A[0, 0], A[0, 1], A[0, 2] = h[1], -(h[0] + h[1]), h[0]  # not-a-knot at x_1
+    A[n - 1, n - 3], A[n - 1, n - 2], A[n - 1, n - 1] = h[n - 2], -(h[n - 3] + h[n - 2]), h[n - 3]  # at x_n-2
+    M = np.linalg.solve(A, r)
+    out = np.zeros((n, 4))
+    out[:, 0] = y
+    out[:-1, 1] = (y[1:] - y[:-1]) / h - h * (2 * M[:-1] + M[1:]) / 6
+    out[:, 2] = M / 2
+    out[:-1, 3] = (M[1:] - M[:-1]) / (6 * h)
+    hl = h[-1]
+    out[-1, 1] = out[-2, 1] + 2 * out[-2, 2] * hl + 3 * out[-2, 3] * hl * hl
+    out[-1, 3] = out[-2, 3]
+    return out
+
+
+def spline_block(x, re, im) -> list:
+    """The float spline block of one model-independent wave: knots, (y, b, c, d) of the real part per
+    knot, then of the imaginary part (RooDalitzAmplitude.cxx:2741-2764)."""
+    cr, ci = spline_coefficients(x, re), spline_coefficients(x, im)
+    return [f32(v) for v in x] + [f32(v) for v in cr.reshape(-1)] + [f32(v) for v in ci.reshape(-1)]
+
+
 def _pow_m1(e) -> float:
     return 1.0 if int(round(e)) % 2 == 0 else -1.0
 
@@ -383,8 +433,9 @@ class ParamBlock:
 
 def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tuple:
     """The pieces of the parameter block one resonance contributes: its table row (NSET floats), its
-    helicity couplings (float Re/Im pairs) and its K-matrix inputs (('g', group, g1..g4) for a pole,
-    ('f', group, f) for a non-resonant term, or None)."""
+    helicity couplings (float Re/Im pairs), its K-matrix inputs (('g', group, g1..g4) for a pole,
+    ('f', group, f) for a non-resonant term, or None) and its spline block (empty unless the entry is
+    a model-independent wave)."""
     r = model.resonances[ir]
     q = np.zeros(NSET, f32)
     q[0] = f32(model.value(vals, r.mass))
@@ -411,7 +462,7 @@ def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tu
                         vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
         if r.type != BREITWIGNER:
             raise NotImplementedError(f"Zcs lineshape type {r.type}")
-        return q, vamp, km
+        return q, vamp, km, []
     if r.chain == "L":
         S = f32(r.spin2) / f32(2)
         sc = complex(model.value(vals, r.extra[0]), model.value(vals, r.extra[1]))
@@ -425,7 +476,7 @@ def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tu
                 a = a * _pow_m1(1 - h2)
                 a = a * sc
                 vamp += [f32(a.real), f32(a.imag)] if keep else [f32(0), f32(0)]
-        if r.type not in (BREITWIGNER, NONRESONANT):
+        if r.type not in (BREITWIGNER, NONRESONANT, MODELINDEPENDENT, REVISEDKMATRIX):
             raise NotImplementedError(f"Lambda* lineshape type {r.type}")
     else:
         S = r.spin2 / 2.0
@@ -446,17 +497,27 @@ def _resonance_parts(model: Model, vals: dict, ir: int, keep: bool = True) -> tu
                 km = ("g", ik, [f32(model.value(vals, g)) for g in r.extra[:4]])
             else:
                 km = ("f", ik, f32(model.value(vals, r.extra[0])))
-        elif r.type not in (BREITWIGNER, NONRESONANT):
+        elif r.type not in (BREITWIGNER, NONRESONANT, MODELINDEPENDENT, REVISEDKMATRIX, TRIANGLE):
             raise NotImplementedError(f"Pc lineshape type {r.type}")
-    return q, vamp, km
+    spl: list = []
+    if r.type == MODELINDEPENDENT:
+        nk = NUMSP if r.chain == "L" else NUMSPZ
+        if len(r.knots) != nk:
+            raise ValueError(f"{r.name}: a model-independent wave of chain {r.chain} has {nk} knots")
+        re = [model.value(vals, k[0]) for k in r.knots]
+        im = [model.value(vals, k[1]) for k in r.knots]
+        xs = [model.value(vals, k[2]) for k in r.knots]
+        spl = spline_block(xs, re, im)
+    return q, vamp, km, spl
 
 
 def _assemble_block(model: Model, parts: list) -> ParamBlock:
     table = np.concatenate([p[0] for p in parts]) if parts else np.zeros(0, f32)
     vamp = [x for p in parts for x in p[1]]
+    spl = [x for p in parts for x in p[3]]  # Lambda* splines, then Pc splines (resonance order)
     galpha = [[] for _ in range(4)]
     fscat = [[] for _ in range(4)]
-    for _, _, km in parts:
+    for _, _, km, _ in parts:
         if km is None:
             continue
         if km[0] == "g":
@@ -472,8 +533,9 @@ def _assemble_block(model: Model, parts: list) -> ParamBlock:
         for i in range(1, NKMC):
             f[NKMC * i] = f[i]
         km += g + [f32(0)] * (NPMAX * NKMC - len(g)) + f
-    data = np.concatenate([table.astype(f32), np.array(vamp, f32), np.array(km, f32)]).astype(f32)
-    return ParamBlock(data, len(table), len(vamp), 0, model.NR, model.NZ, model.NX, model.ffr, model.ffb)
+    data = np.concatenate([table.astype(f32), np.array(vamp, f32), np.array(spl, f32),
+                           np.array(km, f32)]).astype(f32)
+    return ParamBlock(data, len(table), len(vamp), len(spl), model.NR, model.NZ, model.NX, model.ffr, model.ffb)
 
 
 def build_param_block(model: Model, vals: dict, include: tuple | None = None) -> ParamBlock:
@@ -506,7 +568,7 @@ class BlockBuilder:
         self.uses: dict = {}
         everything = list(range(len(model.resonances)))
         for i, r in enumerate(model.resonances):
-            refs = [x for x in (*r.couplings, *r.extra, r.mass, r.width) if isinstance(x, str)]
+            refs = [x for x in r.refs() if isinstance(x, str)]
             for x in refs:
                 if x in model.derived:  # derived values may read any parameter
                     for n in list(vals):

@@ -21,8 +21,34 @@ def test_block_layout(name):
         exp += 2 * 2 * sum(1 for hpsi in (-1, 0, 1) if abs(hpsi) <= S for hp in (-0.5, 0.5)
                            for hz in (hp - 0.5, hp + 0.5) if abs(hz) <= S)
     assert b.vamp_size == exp
-    assert len(b.data) == b.para_size + b.vamp_size + M.KM_SIZE
+    spl = sum(9 * (M.NUMSP if r.chain == "L" else M.NUMSPZ) for r in mdl.resonances if r.type == M.MODELINDEPENDENT)
+    assert b.spline_size == spl
+    assert len(b.data) == b.para_size + b.vamp_size + b.spline_size + M.KM_SIZE
     assert b.data.dtype == np.float32
+
+
+def test_spline_coefficients_not_a_knot():
+    """The spline blocks' coefficients: a cubic through the knots with not-a-knot end conditions
+    (TSpline3's default), checked against scipy's independent implementation, and the block layout
+    (knots, then (y, b, c, d) per knot of Re, then of Im) of RooDalitzAmplitude.cxx:2741-2764."""
+    from scipy.interpolate import CubicSpline
+    rng = np.random.default_rng(3)
+    x = np.sort(rng.uniform(1.43, 2.52, 24))
+    y = rng.normal(size=24)
+    c = M.spline_coefficients(x, y)
+    ref = CubicSpline(x, y, bc_type="not-a-knot")
+    assert np.allclose(c[:-1, ::-1].T, ref.c, rtol=1e-9, atol=1e-9)
+    t = np.linspace(x[0], x[-1], 777)
+    k = np.clip(np.searchsorted(x, t, side="right") - 1, 0, len(x) - 2)
+    dt = t - x[k]
+    v = c[k, 0] + dt * (c[k, 1] + dt * (c[k, 2] + dt * c[k, 3]))
+    assert np.allclose(v, ref(t), rtol=1e-9, atol=1e-9)
+    blk = M.spline_block(x, y, 2 * y)
+    n = len(x)
+    assert len(blk) == 9 * n
+    assert np.allclose(np.array(blk[:n]), x.astype(np.float32))
+    assert np.allclose(np.array(blk[n:5 * n]).reshape(n, 4), c.astype(np.float32))
+    assert np.allclose(np.array(blk[5 * n:]).reshape(n, 4), (2 * c).astype(np.float32))
 
 
 def test_pc_couplings_do_not_depend_on_proton_helicity():
