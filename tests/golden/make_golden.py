@@ -9,6 +9,7 @@ never read the reference).
 * ref_nll.json       : NLL of seeded small samples from the reference's own likelihood code on host
                        cores (FP32) next to the FP64 oracle
 * func_example.json  : a parameter file of the reference parsed by pwa_b200.model.read_func
+* swave_knots.json   : the reference's 24-knot S-wave spline (mass, Re, Im) of Fit_Jpsippi/toyr_fine_bin.dat
 """
 from __future__ import annotations
 
@@ -87,7 +88,7 @@ def ref_nll():
     rows = []
     for name, nd, nm, seed in (("small_kmatrix", 1500, 15000, 21), ("small_bw", 1500, 15000, 22),
                                ("kmatrix", 1000, 10000, 23), ("lstar_only", 1000, 10000, 24),
-                               ("full_bw", 1000, 10000, 25)):
+                               ("full_bw", 1000, 10000, 25), ("lineshapes", 1000, 10000, 26)):
         mdl, vals = configs.MODELS[name]()
         blk = M.build_param_block(mdl, vals)
 
@@ -109,6 +110,12 @@ def _sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
 
 
+def swave_knots():
+    rows = [[float(x) for x in ln.split()] for ln in
+            (REF / "Fit_Jpsippi" / "toyr_fine_bin.dat").read_text().splitlines() if ln.strip()]
+    (HERE / "swave_knots.json").write_text(json.dumps(rows))
+
+
 def func_example():
     from pwa_b200 import model as M
     text = (REF / "Fit_Jpsippi" / "func" / "yujie_test.func").read_text()
@@ -125,5 +132,6 @@ if __name__ == "__main__":
         cg(L)
         dfun(L)
         func_example()
+        swave_knots()
     ref_nll()
     print("fixtures written to", HERE)
