@@ -43,4 +43,13 @@ void host_store_amp2s(std::vector<float*> d_float_pp, std::vector<float*> d_floa
                       int paraSpline_size, double* h_amp2s, int end, int begin, int NUMLz, int NUMPc, int NUMZcs,
                       float _FFR, float _FFB);
 
+/* Lambda* lineshape diagnostic (kernel_calEva.cu:1545-1584): revised K-matrix and Breit-Wigner
+ * lineshapes of every Lambda* entry (times the Lambda_b barrier with radius _FFR) at n_points masses,
+ * written as floats to [iLz * n_points + i] for iLz < NR (nLz >= NR rows must fit).  Computed in FP64 by
+ * pwa_lineshapes_lstar_km and rounded to float. */
+void host_store_lineshapeLsKM(const float* h_mkp, float* h_KM_real, float* h_KM_imag, float* h_BW_real,
+                              float* h_BW_imag, const int n_points, const int NR, const int nLz, const float _FFR,
+                              float* h_paraList, const int para_size, const int vamp_size,
+                              const int paraSpline_size);
+
 #endif

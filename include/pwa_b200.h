@@ -42,7 +42,7 @@ enum {
   PWA_E_ARG = 2,         /* null pointer or negative size */
   PWA_E_LAYOUT = 3,      /* parameter block sizes inconsistent with the resonance table */
   PWA_E_SIZE = 4,        /* a model size exceeds the compiled maximum */
-  PWA_E_UNSUPPORTED = 5, /* lineshape type not built (spline, revised K-matrix) */
+  PWA_E_UNSUPPORTED = 5, /* lineshape type or entry point option not supported */
   PWA_E_PARAM = 6,       /* invalid resonance parameters (spin, K-matrix channel) */
   PWA_E_STATE = 7,       /* no events uploaded (or no Zcs planes for a model with Zcs entries) */
   PWA_E_NOMEM = 8        /* device allocation failed */
@@ -191,6 +191,18 @@ int pwa_ctx_last_launches(pwa_ctx* ctx);
  * K-matrix lineshapes. */
 int pwa_host_lineshapes(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
                         int NX, float FFR, float FFB, double mkp, double mz, double* lstar, double* pc);
+
+/* Lambda* lineshape diagnostic on the device (replaces host_store_lineshapeLsKM,
+ * RooTDalitz/kernel_calEva.h:27, src/kernel_calEva.cu:1490-1584): for every Lambda* entry r < NR of the
+ * parameter block and every mass h_mkp[i], the revised K-matrix lineshape in its refactored form
+ * (Revised_KMAMP_refactor, src/cu_DPFPropogator.cu:998-1063) and the Breit-Wigner (BW_AMP), each times
+ * the Lambda_b barrier BTerm with radius FFR, whatever the entry's type, as the reference computes
+ * them.  FP64 on the float parameters; outputs km_re/km_im/bw_re/bw_im[r * n_points + i] (host
+ * memory, NR * n_points doubles each).  Only the resonance table (the first 6 NR floats) is read.
+ * Allocates and frees its own device buffers; blocks until the outputs are on the host. */
+int pwa_lineshapes_lstar_km(int device, const float* h_mkp, int n_points, int NR, float FFR,
+                            const float* h_paraList, int para_size, double* km_re, double* km_im, double* bw_re,
+                            double* bw_im);
 
 /* Synthetic events on the device (flat phase space, the reference ntuple maker's helicity angles,
  * the filldlz basis), written into columns [col0, col0 + n) of device planes with stride n_size.

@@ -172,3 +172,26 @@ void host_store_amp2s(std::vector<float*> d_float_pp, std::vector<float*> d_floa
   if (rc) report("host_store_amp2s", rc);
   pwa_ctx_destroy(ctx);
 }
+
+void host_store_lineshapeLsKM(const float* h_mkp, float* h_KM_real, float* h_KM_imag, float* h_BW_real,
+                              float* h_BW_imag, const int n_points, const int NR, const int nLz, const float _FFR,
+                              float* h_paraList, const int para_size, const int vamp_size,
+                              const int paraSpline_size) {
+  (void)vamp_size;
+  (void)paraSpline_size;
+  if (nLz < NR) {
+    std::fprintf(stderr, "host_store_lineshapeLsKM: %d output rows for %d Lambda* entries\n", nLz, NR);
+    return;
+  }
+  const size_t n = (size_t)n_points * (size_t)(NR > 0 ? NR : 0);
+  std::vector<double> buf(4 * n);
+  const int rc = pwa_lineshapes_lstar_km(current_device(), h_mkp, n_points, NR, _FFR, h_paraList, para_size,
+                                         buf.data(), buf.data() + n, buf.data() + 2 * n, buf.data() + 3 * n);
+  if (rc) {
+    report("host_store_lineshapeLsKM", rc);
+    return;
+  }
+  float* outs[4] = {h_KM_real, h_KM_imag, h_BW_real, h_BW_imag};
+  for (int k = 0; k < 4; ++k)
+    for (size_t i = 0; i < n; ++i) outs[k][i] = (float)buf[k * n + i];
+}

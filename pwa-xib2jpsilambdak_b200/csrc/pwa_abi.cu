@@ -492,8 +492,9 @@ int pwa_ctx_set_device_zcs_events(pwa_ctx* c, const float* d_pp3, const float* d
 
 // The event set of an evaluation: the Zcs planes go with it only for a model with Zcs entries
 // (they select the kernels with the Zcs terms).
-static int event_set(const pwa_ctx* c, int NX, EventSet* ev) {
+static int event_set(const pwa_ctx* c, int NX, const PointTable& T, EventSet* ev) {
   *ev = EventSet{c->pp, c->pp1, c->pp2, c->sw, c->n_size, c->n, c->nda};
+  ev->lgen = lstar_has_general(T);
   if (NX > 0) {
     if (!c->pp3 || !c->pp4) return PWA_E_STATE;
     ev->pp3 = c->pp3;
@@ -522,7 +523,6 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
                      pwa_result* out, double* h_fx) {
   if (!c || !pl || !out) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  if (spline_size != 0) return PWA_E_UNSUPPORTED;
   int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
@@ -533,7 +533,7 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
     c->fx_cap = c->n;
   }
   EventSet ev;
-  if ((rc = event_set(c, NX, &ev))) return rc;
+  if ((rc = event_set(c, NX, *c->h_table, &ev))) return rc;
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
@@ -598,7 +598,6 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
                            int* n_structured) {
   if (!c || !pls || !out || npoints < 1 || block_stride < para_size + vamp_size + spline_size) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  if (spline_size != 0) return PWA_E_UNSUPPORTED;
   PWA_CUDA(cudaSetDevice(c->device));
   std::vector<PointTable> H(npoints);
   for (int p = 0; p < npoints; ++p) {
@@ -655,7 +654,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   }
   int launches = 0, rc = 0;
   EventSet ev;
-  if ((rc = event_set(c, NX, &ev))) return rc;
+  if ((rc = event_set(c, NX, H[0], &ev))) return rc;
   PWA_CUDA(cudaEventRecord(c->e0, c->st));
   // centre: the context's table and lineshape tables
   *c->h_table = H[0];
@@ -767,7 +766,6 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
                  float FFR, float FFB, double* h_amp2) {
   if (!c || !pl || !h_amp2) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  if (spline_size != 0) return PWA_E_UNSUPPORTED;
   int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
@@ -778,7 +776,7 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
     c->fx_cap = c->n;
   }
   EventSet ev;
-  if ((rc = event_set(c, NX, &ev))) return rc;
+  if ((rc = event_set(c, NX, *c->h_table, &ev))) return rc;
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const bool defer = c->h_table->tab.enabled != 0;
@@ -795,7 +793,6 @@ int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_siz
                         int NX, float FFR, float FFB, double* integral) {
   if (!c || !pl || !integral) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  if (spline_size != 0) return PWA_E_UNSUPPORTED;
   int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
@@ -806,7 +803,7 @@ int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_siz
     c->fx_cap = c->n;
   }
   EventSet ev;
-  if ((rc = event_set(c, NX, &ev))) return rc;
+  if ((rc = event_set(c, NX, *c->h_table, &ev))) return rc;
   int launches = 0;
   if ((rc = upload_point(c, &launches))) return rc;
   const bool defer = c->h_table->tab.enabled != 0;

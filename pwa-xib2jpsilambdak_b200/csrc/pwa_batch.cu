@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(BU_THREADS)
     const LstarKin lk0 = lstar_kin(T0, mkp);
     {
       for (int r = 0; r < NR; ++r) {
-        const cplx q = lstar_lineshape(T0.L[r], lk0);
+        const cplx q = lstar_lineshape(T0, r, lk0);
         q0s[r * 32 + lane] = q;
         lstar_acc(T0.L[r].c, T0.L[r].sidx, E, q, HL0);
       }
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(BU_THREADS)
             lstar_acc(bp.dc + 24 * u++, sx, E, q0, d);
           } else {
             if (cc) ++u;
-            const cplx qp = lstar_lineshape(Tp.L[r], lk0);
+            const cplx qp = lstar_lineshape(Tp, r, lk0);
             if (!cc) {
               lstar_acc(T0.L[r].c, sx, E, qp - q0, d);
             } else {
@@ -363,13 +363,26 @@ BatchGroupMap batch_group_map(const PointTable& T0) {
   return m;
 }
 
+// Inputs of a lineshape that live outside its own entry: the spline block it reads, or every entry of
+// its revised K-matrix set (chain c: 0 Lambda*, 1 Pc).
+static bool shape_inputs_differ(const PointTable& A, const PointTable& B, int c, int type, int aux) {
+  if (type == LT_SPLINE)
+    return !same_bytes(A.spl + aux, B.spl + aux, 9 * (c ? SPL_KNOTS_Z : SPL_KNOTS_L) * sizeof(float));
+  if (type == LT_RKM) {
+    const int set = A.rkm[c][aux].set;
+    for (int j = 0; j < A.nrkm[c]; ++j)
+      if (A.rkm[c][j].set == set && !same_bytes(&A.rkm[c][j], &B.rkm[c][j], sizeof(RkmEntry))) return true;
+  }
+  return false;
+}
+
 bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, cplx* dc_host) {
   *bp = BatchPoint{};
   // structure and global constants must agree
   if (T0.NR != Tp.NR || T0.NZ != Tp.NZ || T0.ngroups != Tp.ngroups || T0.ffr != Tp.ffr || T0.ffb != Tp.ffb ||
       T0.lmask_lstar_R != Tp.lmask_lstar_R || T0.lmask_lstar_B != Tp.lmask_lstar_B ||
       T0.lmask_pc_B != Tp.lmask_pc_B || T0.lmask_pc_R != Tp.lmask_pc_R || T0.needs_sigma_pi != Tp.needs_sigma_pi ||
-      !same_bytes(T0.order, Tp.order, sizeof(T0.order)))
+      !same_bytes(T0.order, Tp.order, sizeof(T0.order)) || !same_bytes(T0.nrkm, Tp.nrkm, sizeof(T0.nrkm)))
     return false;
   // Zcs entries are part of the centre's H_L: a point that moves one goes through the single-point path
   if (T0.NX != Tp.NX || T0.lmask_x_R != Tp.lmask_x_R || T0.lmask_x_B != Tp.lmask_x_B ||
@@ -381,7 +394,9 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
   }
   unsigned lmask = 0;
   for (int r = 0; r < T0.NR; ++r)
-    if (!same_bytes(&T0.L[r], &Tp.L[r], sizeof(LstarEntry))) lmask |= 1u << r;
+    if (!same_bytes(&T0.L[r], &Tp.L[r], sizeof(LstarEntry)) ||
+        shape_inputs_differ(T0, Tp, 0, T0.L[r].type, T0.L[r].aux))
+      lmask |= 1u << r;
   // Pc entries by order position: couplings changed, anything else changed
   int ncoup = 0, nconst = 0, cgroup = -1;
   bool multi_group = false;
@@ -392,7 +407,7 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
     const bool coup = !same_bytes(a.c, b.c, sizeof(a.c));
     std::memset(a.c, 0, sizeof(a.c));
     std::memset(b.c, 0, sizeof(b.c));
-    const bool cons = !same_bytes(&a, &b, sizeof(PcEntry));
+    const bool cons = !same_bytes(&a, &b, sizeof(PcEntry)) || shape_inputs_differ(T0, Tp, 1, a.type, a.aux);
     if (coup) qpos[ncoup++] = pos;
     if (cons) {
       ++nconst;
@@ -427,7 +442,8 @@ bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, 
       const bool coup = !same_bytes(a.c, b.c, sizeof(a.c));
       std::memset(a.c, 0, sizeof(a.c));
       std::memset(b.c, 0, sizeof(b.c));
-      if (!same_bytes(&a, &b, sizeof(LstarEntry))) bp->lsmask |= 1u << r;
+      if (!same_bytes(&a, &b, sizeof(LstarEntry)) || shape_inputs_differ(T0, Tp, 0, a.type, a.aux))
+        bp->lsmask |= 1u << r;
       if (coup) {
         bp->lcmask |= 1u << r;
         if (u < BATCH_MAXQ)

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     // centre: Lambda* lineshapes, f_r[h], H_L[h]; Pc angular amplitudes HZ_q[h]
     if (lane < NR || lane == 0) {
       const LstarKin lk = lstar_kin(T0, mkp);
-      if (lane < NR) q0[lane] = lstar_lineshape(T0.L[lane], lk);
+      if (lane < NR) q0[lane] = lstar_lineshape(T0, lane, lk);
       if (lane == 0) *lks = lk;
     }
     __syncwarp();
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                 for (int h = 0; h < 8; ++h) cmac(hlp[h], q0[r], lstar_angular_c(dc, T0.L[r].sidx, E, h));
               } else {
                 if (cc) ++u;
-                const cplx qp = lstar_lineshape(Tp.L[r], lk);
+                const cplx qp = lstar_lineshape(Tp, r, lk);
                 if (!cc) {  // lineshape only: (q^p - q^0) f_r
                   const cplx dq = qp - q0[r];
 #pragma unroll

@@ -5,6 +5,7 @@
 #include <cmath>
 
 #include "pwa_kernels.cuh"
+#include "pwa_lineshapes.cuh"
 
 namespace pwa {
 
@@ -62,11 +63,25 @@ __host__ __device__ inline PcKin pc_kin(const PointTable& T, double mz) {
   return k;
 }
 
-// Lambda* Breit-Wigner times the Lambda_b -> Lambda* J/psi barrier (BW_AMP, cu_DPFPropogator.cu:248-314;
-// BTerm :155-181) with the parameter-only constants of the point table.
-__host__ __device__ inline cplx lstar_lineshape(const LstarEntry& L, const LstarKin& k) {
+// Spline and revised K-matrix Lambda* lineshapes (GetAmpLz's MODELINDEPENDENT and REVISEDKMATRIX
+// cases, kernel_calEva.cu:136-150).
+static __host__ __device__ __forceinline__ cplx lstar_general(const PointTable& T, int r, double mkp) {
+  const LstarEntry& L = T.L[r];
+  if (L.type == LT_SPLINE) return spline_wave(T.spl + L.aux, SPL_KNOTS_L, SPL_L_LO, SPL_L_HI, mkp);
+  return rkm_lineshape(T, 0, L.aux, mkp);
+}
+
+// Lambda* lineshape r times the Lambda_b -> Lambda* J/psi barrier (BW_AMP, cu_DPFPropogator.cu:248-314;
+// BTerm :155-181; a spline wave takes the non-resonant barrier) with the parameter-only constants of
+// the point table.
+// GEN = false: the model has Breit-Wigner and non-resonant Lambda* entries only.
+template <bool GEN = true>
+__host__ __device__ inline cplx lstar_lineshape(const PointTable& T, int r, const LstarKin& k) {
+  const LstarEntry& L = T.L[r];
   cplx bw = mk(1, 0);
-  if (L.type == LT_BW) {
+  if (GEN && (L.type == LT_SPLINE || L.type == LT_RKM)) {
+    bw = lstar_general(T, r, k.mkp);
+  } else if (L.type == LT_BW) {
     if (L.branch == 2) {
       bw = mk(ipow(k.pR * L.inv_pR0, L.LR), 0);
     } else if (L.branch == 4) {
@@ -93,6 +108,14 @@ __host__ __device__ inline cplx lstar_lineshape(const LstarEntry& L, const Lstar
   }
   const double bt = (L.LB ? L.sqrt_polyB0 * k.rsB[L.LB] : 1.0) * ipow(k.pBm, L.LB) * L.lb_scale;
   return bw * bt;
+}
+
+// Spline, revised K-matrix and triangle-cusp Pc lineshapes (GetAmp2s / TemplateGetAmp2s cases,
+// kernel_calEva.cu:404-425, 708-730), out of line.
+static __host__ __device__ __noinline__ cplx pc_general(const PointTable& T, const PcEntry& Z, double mz) {
+  if (Z.type == LT_SPLINE) return spline_wave(T.spl + Z.aux, SPL_KNOTS_Z, SPL_Z_LO, SPL_Z_HI, mz);
+  if (Z.type == LT_RKM) return rkm_lineshape(T, 1, Z.aux, mz);
+  return cusp_lineshape(Z.m_r, Z.g_r, mz);
 }
 
 // Lambda_b -> Pc K barrier (BTermZ, cu_DPFPropogator.cu:183-203).
@@ -224,7 +247,10 @@ __host__ __device__ inline void pc_group_exact(const PointTable& T, int g, const
   if (gr.km >= 0) km_solve(T.G[gr.km], k.mz, T.ffb, kmo);
   for (int q = 0; q < gr.count; ++q) {
     const PcEntry& Z = T.Z[T.order[gr.first + q]];
-    const cplx v = (Z.type == LT_KM) ? kmo[Z.slot] : (Z.type == LT_BW) ? pc_bw(Z, k) : mk(1, 0);
+    const cplx v = (Z.type == LT_KM)   ? kmo[Z.slot]
+                   : (Z.type == LT_BW) ? pc_bw(Z, k)
+                   : (Z.type == LT_NR) ? mk(1, 0)
+                                       : pc_general(T, Z, k.mz);
     raw[q] = v * pc_barrier(Z, k);
   }
 }

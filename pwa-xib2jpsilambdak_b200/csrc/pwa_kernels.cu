@@ -35,7 +35,7 @@ namespace pwa {
 // masses exactly (out of line); it runs over the deferred list (events [0, *n_list) of list) or,
 // without tables, over the whole segment.  Keeping the exact path out of the main kernel keeps its
 // register allocation free of the call's save/restore.
-template <bool FIX, bool ZCS>
+template <bool FIX, bool ZCS, bool GEN>
 __global__ void __launch_bounds__(EV_THREADS, 2)
     k_unsmeared(EventSet ev, int64_t begin, int64_t end, const int32_t* list, const int* n_list,
                 const PointTable* __restrict__ gtab, Partial* parts, double* fx_out, int mode, int32_t* defer,
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(EV_THREADS, 2)
       const LstarKin lk = lstar_kin(T, mkp);
       for (int r0 = 0; r0 < T.NR; r0 += 2) {
         const int rm = r0 + k;
-        const cplx mine = (rm < T.NR) ? lstar_lineshape(T.L[rm], lk) : mk(0, 0);
+        const cplx mine = (rm < T.NR) ? lstar_lineshape<GEN>(T, rm, lk) : mk(0, 0);
         const cplx other = shfl_xor(mine, 16);
 #pragma unroll
         for (int d = 0; d < 2; ++d) {
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(EV_THREADS, 3)
     const double mkp = E.mkp(), mz = E.mz();
     // Lambda*: lane r evaluates lineshape r; lane (h, part) sums the resonances r = part mod 4
     cplx qmine = mk(0, 0);
-    if (lane < T.NR) qmine = lstar_lineshape(T.L[lane], lstar_kin(T, mkp));
+    if (lane < T.NR) qmine = lstar_lineshape(T, lane, lstar_kin(T, mkp));
     cplx hl = mk(0, 0);
     for (int r0 = 0; r0 < T.NR; r0 += 4) {
       const int r = r0 + part;
@@ -567,8 +567,12 @@ static void launch_kind_t(const EventSet& ev, int kind, int64_t begin, int64_t e
                           cudaStream_t st) {
   switch (kind) {
     case SMEAR_NONE:
-      k_unsmeared<FIX, ZCS><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
-                                                                     fx_out, mode, defer, defer_count);
+      if (ev.lgen)
+        k_unsmeared<FIX, ZCS, true><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table,
+                                                                           out, fx_out, mode, defer, defer_count);
+      else
+        k_unsmeared<FIX, ZCS, false><<<nb, EV_THREADS, UNSMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table,
+                                                                            out, fx_out, mode, defer, defer_count);
       break;
     case SMEAR_20:
       k_smeared<20, FIX, ZCS><<<nb, EV_THREADS, SMEARED_SMEM, st>>>(ev, begin, end, list, n_list, d_table, out,
@@ -644,8 +648,10 @@ template <bool ZCS>
 static cudaError_t configure_variant(int* occ) {
   cudaError_t e;
   int unused = 0;
-  if ((e = configure_one(k_unsmeared<false, ZCS>, UNSMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_NONE]))) return e;
-  if ((e = configure_one(k_unsmeared<true, ZCS>, UNSMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_unsmeared<false, ZCS, false>, UNSMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_NONE]))) return e;
+  if ((e = configure_one(k_unsmeared<true, ZCS, false>, UNSMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_unsmeared<false, ZCS, true>, UNSMEARED_SMEM, &unused))) return e;
+  if ((e = configure_one(k_unsmeared<true, ZCS, true>, UNSMEARED_SMEM, &unused))) return e;
   if ((e = configure_one(k_smeared<20, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_20]))) return e;
   if ((e = configure_one(k_smeared<30, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_30]))) return e;
   if ((e = configure_one(k_smeared<150, false, ZCS>, SMEARED_SMEM, ZCS ? &unused : &occ[SMEAR_150]))) return e;
@@ -759,6 +765,47 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
   const double thr_pk = (double)(float)(M_P + M_K);
   const double thr_pz = (double)(float)(M_P + M_JPSI);
   int cnt = para_size;
+  // spline blocks follow the couplings, Lambda* waves first (cuda_configure_splcount,
+  // kernel_calEva.cu:1100-1135)
+  int splcount = para_size + vamp_size, spl_used = 0;
+  const int spl_end = para_size + vamp_size + spline_size;
+  auto take_spline = [&](int knots, int* aux) -> int {
+    const int nf = 9 * knots;
+    if (splcount + nf > spl_end) return 3;  // PWA_E_LAYOUT
+    if (spl_used + nf > SPL_FLOATS) return 4;
+    std::memcpy(T->spl + spl_used, pl + splcount, nf * sizeof(float));
+    *aux = spl_used;
+    spl_used += nf;
+    splcount += nf;
+    return 0;
+  };
+  // revised K-matrix entry of chain c: own-term constants in the chain's two-body system (threshold
+  // thr, upper edge hi) and the p K constants of its KMatrixTerm
+  auto take_rkm = [&](int c, const float* q, int* aux) -> int {
+    if (T->nrkm[c] >= MAX_RKM) return 4;
+    RkmEntry& R = T->rkm[c][T->nrkm[c]];
+    *aux = T->nrkm[c]++;
+    R.m = q[0];
+    R.g = q[1];
+    R.LR = (int)q[3];
+    if (R.LR < 0 || R.LR > 5) return 5;
+    R.set = (int)q[2] * 2 + ((int)q[5] > 0 ? 1 : 0);
+    const double m1 = c ? M_JPSI : M_P, m2 = c ? M_P : M_K, m3 = c ? M_K : M_JPSI;
+    const double thr = c ? (double)(float)(M_JPSI + M_P) : (double)(float)(M_P + M_K);
+    const double lo = m1 + m2, hi = M_LB - m3;
+    const double mc = (R.m > thr) ? R.m : (R.m >= 0) ? tanh_eff_mass(R.m, lo, hi) : (lo + hi) / 2.0;
+    const double pc = two_body_p(mc, m1, m2);
+    R.inv_pR0c = 1.0 / pc;
+    R.polyR0c = bw_poly(R.LR, sq(T->ffr * pc));
+    R.branch = (R.m <= 0) ? 3 : (R.m > thr) ? 0 : (R.m < thr) ? 1 : 2;
+    if (R.branch == 1) R.inv_pR0sp = 1.0 / two_body_p(R.m, PWA_F(1.18937f), PWA_F(0.13957018f));
+    R.factor = (R.m > 0) ? bw_norm(R.m, R.g) : 1.0;
+    const double mk_ = (R.m > thr_pk) ? R.m : (R.m >= 0) ? tanh_eff_mass(R.m, mmin, mmax) : (mmin + mmax) / 2.0;
+    const double pk = two_body_p(mk_, M_P, M_K);
+    R.inv_pR0k = 1.0 / pk;
+    R.polyR0k = bw_poly(R.LR, sq(T->ffr * pk));
+    return 0;
+  };
   auto coupling = [&](int idx) -> cplx {
     const float a = pl[idx], b = pl[idx + 1];
     // the reference skips couplings with float |c| < 1e-10 (kernel_calEva.cu:174,481)
@@ -775,12 +822,19 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     if (S2 < 1 || S2 > 9 || (S2 % 2) == 0) return 6;  // PWA_E_PARAM
     L.sidx = (S2 - 1) / 2;
     L.ncm = (S2 == 1) ? 4 : 6;
-    if (type == REF_BREITWIGNER)
+    if (type == REF_BREITWIGNER) {
       L.type = LT_BW;
-    else if (type == REF_NONRESONANT)
+    } else if (type == REF_NONRESONANT) {
       L.type = LT_NR;
-    else
+    } else if (type == REF_MODELINDEPENDENT) {
+      L.type = LT_SPLINE;
+      if (int e = take_spline(SPL_KNOTS_L, &L.aux)) return e;
+    } else if (type == REF_REVISEDKMATRIX) {
+      L.type = LT_RKM;
+      if (int e = take_rkm(0, q, &L.aux)) return e;
+    } else {
       return 5;
+    }
     const double m_r = L.m_r;
     if (m_r < 0) {
       L.branch = 2;
@@ -805,13 +859,14 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     if (L.type == LT_BW && (L.branch == 0 || L.branch == 3) && L.LR >= 1 && L.LR <= 5) T->lmask_lstar_R |= 1 << L.LR;
     if (L.type == LT_BW && L.branch == 1) T->needs_sigma_pi = 1;
     if (L.LR > 5) return 5;
-    // Lambda_b barrier constants (BTerm)
+    // Lambda_b barrier constants (BTerm; a spline wave passes mass -0.5, kernel_calEva.cu:143)
     const double J = 0.5 * S2;
     L.LB = (J <= 1) ? 0 : (int)(J - 1.5);
+    const double mb = (L.type == LT_SPLINE) ? -0.5 : m_r;
     double pB0 = -1;
-    if (m_r < 0) pB0 = two_body_p(M_LB, M_JPSI, (mmin + mmax) / 2.0);
-    if (m_r > 1e-10 && m_r + M_JPSI < M_LB) pB0 = two_body_p(M_LB, M_JPSI, m_r);
-    if (m_r + M_JPSI > M_LB) pB0 = two_body_p(M_LB, M_JPSI, tanh_eff_mass(m_r, mmin, mmax));
+    if (mb < 0) pB0 = two_body_p(M_LB, M_JPSI, (mmin + mmax) / 2.0);
+    if (mb > 1e-10 && mb + M_JPSI < M_LB) pB0 = two_body_p(M_LB, M_JPSI, mb);
+    if (mb + M_JPSI > M_LB) pB0 = two_body_p(M_LB, M_JPSI, tanh_eff_mass(mb, mmin, mmax));
     if (pB0 < 0) return 6;  // resonance mass in [0, 1e-10]: barrier momentum undefined
     L.pB0 = pB0;
     L.polyB0 = bw_poly(L.LB, sq(T->ffb * pB0));
@@ -837,14 +892,23 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     Z.g_r = q[1];
     if (S2 < 1 || S2 > 7 || (S2 % 2) == 0) return 6;
     Z.sidx = (S2 - 1) / 2;
-    if (type == REF_BREITWIGNER)
+    if (type == REF_BREITWIGNER) {
       Z.type = LT_BW;
-    else if (type == REF_KMATRIX)
+    } else if (type == REF_KMATRIX) {
       Z.type = LT_KM;
-    else if (type == REF_NONRESONANT)
+    } else if (type == REF_NONRESONANT) {
       Z.type = LT_NR;
-    else
+    } else if (type == REF_MODELINDEPENDENT) {
+      Z.type = LT_SPLINE;
+      if (int e = take_spline(SPL_KNOTS_Z, &Z.aux)) return e;
+    } else if (type == REF_REVISEDKMATRIX) {
+      Z.type = LT_RKM;
+      if (int e = take_rkm(1, q, &Z.aux)) return e;
+    } else if (type == REF_TRIANGLE) {
+      Z.type = LT_CUSP;
+    } else {
       return 5;
+    }
     if (Z.type == LT_KM) {
       Z.group = (Z.LR > 0) ? ((S2 == 3) ? 3 : 2) : ((S2 == 3) ? 1 : 0);
       if (S2 > 3) return 5;
@@ -863,9 +927,10 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     }
     const double J = 0.5 * S2;
     Z.LB = (int)(J - 0.5);
+    const double mbz = (Z.type == LT_SPLINE) ? -0.5 : Z.m_r;  // BTermZ mass (kernel_calEva.cu:408)
     double pB0 = -1;
-    if (Z.m_r < 0) pB0 = two_body_p(M_LB, M_K, (M_JPSI + M_P + M_LB - M_K) / 2.0);
-    if (Z.m_r > 1e-10 && Z.m_r + M_K < M_LB) pB0 = two_body_p(M_LB, M_K, Z.m_r);
+    if (mbz < 0) pB0 = two_body_p(M_LB, M_K, (M_JPSI + M_P + M_LB - M_K) / 2.0);
+    if (mbz > 1e-10 && mbz + M_K < M_LB) pB0 = two_body_p(M_LB, M_K, mbz);
     Z.pB0_event = (pB0 < 0);
     Z.pB0 = pB0;
     Z.polyB0 = bw_poly(Z.LB, sq(T->ffb * pB0));
@@ -951,6 +1016,7 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
         if (nonzero_host(X.c[k * 12 + m])) T->x_mmask[k] |= 1 << m;
   }
   if (cnt != para_size + vamp_size) return 3;
+  if (splcount != spl_end) return 3;  // the spline blocks must fill spline_size exactly
   // K-matrix groups (Default_KMatrix pole scan and near-threshold mass shift, :674-746)
   const int kmcount = para_size + vamp_size + spline_size;
   for (int ik = 0; ik < 4; ++ik) {
@@ -1012,6 +1078,21 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
           if (++g.count > MAX_GROUP_ENTRIES) return 4;
         }
       if (G_valid_check(T->G[Z.group]) != 0) return 6;
+    } else if (Z.type == LT_RKM) {  // a revised K-matrix set: its entries' lineshapes depend on each other
+      const int set = T->rkm[1][Z.aux].set;
+      bool seen = false;
+      for (int j = 0; j < i; ++j) seen |= (T->Z[j].type == LT_RKM && T->rkm[1][T->Z[j].aux].set == set);
+      if (seen) continue;
+      PcGroup& g = T->grp[ng++];
+      g.km = -1;
+      g.sidx = Z.sidx;
+      g.first = pos;
+      g.count = 0;
+      for (int j = i; j < NZ; ++j)
+        if (T->Z[j].type == LT_RKM && T->rkm[1][T->Z[j].aux].set == set) {
+          T->order[pos++] = j;
+          ++g.count;
+        }
     } else {
       PcGroup& g = T->grp[ng++];
       g.km = -1;
@@ -1115,6 +1196,13 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
   }
   if (neg_parity)
     for (double m : complex_branch_masses()) guard(m, step);
+  // spline waves drop to zero outside their domain
+  bool pc_spline = false;
+  for (int i = 0; i < NZ; ++i) pc_spline |= (T->Z[i].type == LT_SPLINE);
+  if (pc_spline) {
+    guard(SPL_Z_LO, cusp);
+    guard(SPL_Z_HI, cusp);
+  }
   if (tb.nguard >= MAX_GUARDS) return 4;
   return 0;
 }
@@ -1125,7 +1213,7 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
 void host_lineshapes(const PointTable& T, double mkp, double mz, cplx* lstar, cplx* pc) {
   const LstarKin lk = lstar_kin(T, mkp);
   const PcKin pk = pc_kin(T, mz);
-  for (int r = 0; r < T.NR; ++r) lstar[r] = lstar_lineshape(T.L[r], lk);
+  for (int r = 0; r < T.NR; ++r) lstar[r] = lstar_lineshape(T, r, lk);
   cplx raw[MAX_PC];
   for (int g = 0; g < T.ngroups; ++g) pc_group_exact(T, g, pk, raw + T.grp[g].first);
   for (int q = 0; q < T.NZ; ++q) pc[T.order[q]] = raw[q];

@@ -39,7 +39,16 @@ struct EventSet {
   // pp4 96 planes (DX)
   const float* pp3 = nullptr;
   const float* pp4 = nullptr;
+  // the model has spline or revised K-matrix Lambda* entries: selects the unsmeared-event kernel that
+  // evaluates those lineshapes (the Breit-Wigner-only variant keeps its register allocation)
+  int lgen = 0;
 };
+
+inline int lstar_has_general(const PointTable& T) {
+  for (int r = 0; r < T.NR; ++r)
+    if (T.L[r].type == LT_SPLINE || T.L[r].type == LT_RKM) return 1;
+  return 0;
+}
 
 // Event classes: unsmeared, the reference's three quantile schemes (offsets in units of the mass
 // resolution, equal weights), and a weighted grid of absolute offsets (fixed-width Gaussian).

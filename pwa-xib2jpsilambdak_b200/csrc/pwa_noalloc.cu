@@ -199,7 +199,8 @@ extern "C" int pwa_eval_nll_noalloc(int device, const float* d_pp, const float* 
     tot += segment_blocks(segs[i], sm_count);
   }
   if (tot > kMaxParts) return finish(PWA_E_SIZE);
-  const EventSet ev{d_pp, d_pp1, d_pp2, d_sw, n_size, n, nda};
+  EventSet ev{d_pp, d_pp1, d_pp2, d_sw, n_size, n, nda};
+  ev.lgen = lstar_has_general(table);
   for (int i = 0; i < nseg; ++i)
     if ((e = launch_segment(ev, segs[i], d_table, d_parts + offs[i], nullptr, nullptr, nullptr, sm_count, st)) !=
         cudaSuccess)

@@ -15,14 +15,41 @@ constexpr int MAX_ZCS = 4;
 constexpr int MAX_GROUPS = MAX_PC + 4;  // K-matrix J^P groups + one group per non-K-matrix Pc entry
 constexpr int NSET = 6;
 
-enum LineType : int { LT_BW = 1, LT_NR = 2, LT_KM = 3 };
-// Lineshape type codes of the parameter block (Resonances.h:97-108).
+// Lineshapes: Breit-Wigner, constant (non-resonant), coupled-channel K-matrix, spline
+// (model-independent wave), revised K-matrix, triangle cusp.
+enum LineType : int { LT_BW = 1, LT_NR = 2, LT_KM = 3, LT_SPLINE = 4, LT_RKM = 5, LT_CUSP = 6 };
+// Lineshape type codes of the parameter block (Resonances.h:108-120).
 constexpr int REF_BREITWIGNER = 1;
+constexpr int REF_MODELINDEPENDENT = 3;
+constexpr int REF_TRIANGLE = 7;
 constexpr int REF_KMATRIX = 240;
+constexpr int REF_REVISEDKMATRIX = 360;
 constexpr int REF_NONRESONANT = 361;
+// Spline knots of the Lambda* and Pc model-independent waves (Resonances.h:5-6); a spline block holds
+// the knots, (y, b, c, d) per knot of the real part, then of the imaginary part: 9 floats per knot.
+constexpr int SPL_KNOTS_L = 24, SPL_KNOTS_Z = 11;
+constexpr int SPL_FLOATS = 2 * 9 * SPL_KNOTS_L + 2 * 9 * SPL_KNOTS_Z;  // two waves of each chain
+// Entries of revised K-matrices per chain (all spin-parity sets together).
+constexpr int MAX_RKM = 6;
+
+// Revised K-matrix entry (Revised_KMAMP, cu_DPFPropogator.cu:825-926): the constants of its own term
+// (chain two-body system) and of the term it adds to the other entries of its set (KMatrixTerm,
+// :928-972, always in the p K system).  Entries with equal spin and parity form one set.
+struct RkmEntry {
+  int set;     // 2J * 2 + (P > 0): entries with equal set are coupled
+  int LR;
+  int branch;  // own term: 0 mass above the chain threshold, 1 below it (Sigma pi channel),
+               // 2 at it, 3 non-resonant (mass <= 0)
+  int pad;
+  double m, g;
+  double inv_pR0c, polyR0c;  // own term: 1 / reference momentum, Blatt-Weisskopf polynomial there
+  double inv_pR0sp;          // branch 1: 1 / Sigma pi momentum at the mass
+  double factor;             // 0.948850 m sqrt(g kr / sqrt(m (m + kr))) for m > 0, else 1
+  double inv_pR0k, polyR0k;  // KMatrixTerm: p K reference momentum and polynomial
+};
 
 struct LstarEntry {
-  int type;   // LT_BW or LT_NR
+  int type;   // LT_BW, LT_NR, LT_SPLINE, LT_RKM
   int sidx;   // d-function spin index (2J-1)/2
   int LR, LB;
   int branch;  // 0: m_r above pK threshold, 1: below threshold (Sigma pi channel), 2: m_r < 0
@@ -31,10 +58,11 @@ struct LstarEntry {
   double pB0, polyB0, lb_scale;                // Lambda_b barrier: F ratio * (pB/mLb)^LB * lb_scale
   double inv_pR0, sqrt_polyR0, inv_pR0_sp, sqrt_polyB0;  // the same constants in the form the kernels use
   cplx c[12];                                  // c[k*6+m]; |c| < 1e-10 stored as 0
+  int aux;  // LT_SPLINE: first float of its block in PointTable::spl; LT_RKM: index in PointTable::rkm[0]
 };
 
 struct PcEntry {
-  int type;  // LT_BW, LT_NR, LT_KM
+  int type;  // LT_BW, LT_NR, LT_KM, LT_SPLINE, LT_RKM, LT_CUSP
   int sidx, LR, LB;
   int group, slot;  // K-matrix J^P group and P-vector output slot
   int bw_above;     // Breit-Wigner mass above J/psi p threshold
@@ -43,6 +71,7 @@ struct PcEntry {
   double pB0, polyB0;
   double inv_pR0, sqrt_polyR0, sqrt_polyB0;
   cplx c[24];  // c[k*12+m], 12 helicity slots per proton helicity (disallowed slots are 0)
+  int aux;     // LT_SPLINE: first float of its block in PointTable::spl; LT_RKM: index in PointTable::rkm[1]
 };
 
 // Zcs -> J/psi K entry (Breit-Wigner BW_AMPX with production barrier BTermX,
@@ -145,6 +174,10 @@ struct alignas(16) PointTable {
   // the plane slots this point's amplitude reads (kernels that stage an event copy only these)
   int nstage;
   short stage[SLOT_ALL];
+  // revised K-matrix entries per chain (0 Lambda*, 1 Pc) in resonance order, and spline blocks
+  int nrkm[2];
+  RkmEntry rkm[2][MAX_RKM];
+  float spl[SPL_FLOATS];
 };
 
 }  // namespace pwa

@@ -19,7 +19,7 @@ EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_c
             "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing", "pwa_ctx_select_data",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
-            "pwa_host_lineshapes", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
+            "pwa_host_lineshapes", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
 
 _fp = C.POINTER(C.c_float)
@@ -94,6 +94,8 @@ def load() -> C.CDLL:
         L.pwa_ctx_stream.argtypes = [C.c_void_p]
         L.pwa_host_lineshapes.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                           C.c_float, C.c_double, C.c_double, _dp, _dp]
+        L.pwa_lineshapes_lstar_km.argtypes = [C.c_int, _fp, C.c_int, C.c_int, C.c_float, _fp, C.c_int, _dp, _dp,
+                                              _dp, _dp]
         L.pwa_generate_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
                                           C.c_uint64, C.c_uint64, C.c_float, C.c_float, C.c_int, C.c_void_p]
         L.pwa_basis_from_angles.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
@@ -306,3 +308,17 @@ def host_lineshapes(block, mkp: float, mz: float):
                                 block.NX, block.ffr, block.ffb, mkp, mz, ls.ctypes.data_as(_dp),
                                 pc.ctypes.data_as(_dp)), "pwa_host_lineshapes")
     return ls[0::2][:block.NR] + 1j * ls[1::2][:block.NR], pc[0::2][:block.NZ] + 1j * pc[1::2][:block.NZ]
+
+
+def lineshapes_lstar_km(block, mkp, device: int = 0) -> tuple:
+    """pwa_lineshapes_lstar_km (the reference's host_store_lineshapeLsKM on the device): revised K-matrix
+    and Breit-Wigner lineshape of every Lambda* entry, each times the Lambda_b barrier with radius FFR,
+    as complex [NR, n] arrays."""
+    L = load()
+    m = np.ascontiguousarray(mkp, np.float32)
+    n, nr = len(m), block.NR
+    out = [np.zeros(n * nr) for _ in range(4)]
+    pl = np.ascontiguousarray(block.data, np.float32)
+    check(L.pwa_lineshapes_lstar_km(device, _f(m), n, nr, block.ffr, _f(pl), block.para_size,
+                                    *[o.ctypes.data_as(_dp) for o in out]), "pwa_lineshapes_lstar_km")
+    return (out[0] + 1j * out[1]).reshape(nr, n), (out[2] + 1j * out[3]).reshape(nr, n)

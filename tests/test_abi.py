@@ -26,7 +26,8 @@ def test_exports_every_declared_symbol():
     for mangled in ("_Z13host_store_fxSt6vectorIPfSaIS0_EES2_S2_S2_S2_S2_S0_iiiPdiiiiiiiiRdddffb",
                     "_Z14cu_malloc_h_ppPfRS_ii", "_Z10cu_Free_ppSt6vectorIPfSaIS0_EES2_S2_S2_S2_",
                     "_Z25cuda_configure_Pc_KMatrixPKf", "_Z23cuda_configure_ampcountPKfi", "_Z20cuda_configure_smearv",
-                    "_Z16host_store_amp2sSt6vectorIPfSaIS0_EES2_S2_S2_S2_S0_iiiPdiiiiiff"):
+                    "_Z16host_store_amp2sSt6vectorIPfSaIS0_EES2_S2_S2_S2_S0_iiiPdiiiiiff",
+                    "_Z24host_store_lineshapeLsKMPKfPfS1_S1_S1_iiifS1_iii"):
         assert mangled in out, mangled
 
 
@@ -72,9 +73,12 @@ def test_error_codes():
     args = (b.para_size, b.vamp_size, 0, b.NR, b.NZ)
     f = lib._f(pl)
     bad = pl.copy()
-    bad[4] = 360  # revised K-matrix Lambda* lineshape: not built
+    bad[4] = 2  # Flatte Lambda* lineshape: the reference kernels have no case for it
     assert L.pwa_host_lineshapes(lib._f(bad), *args, 0, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
                                  d.ctypes.data_as(dp)) == 5
+    bad[4] = 3  # a spline wave without its spline block
+    assert L.pwa_host_lineshapes(lib._f(bad), *args, 0, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
+                                 d.ctypes.data_as(dp)) == 3
     assert L.pwa_host_lineshapes(f, *args, 1, b.ffr, b.ffb, 1.5, 4.4, d.ctypes.data_as(dp),
                                  d.ctypes.data_as(dp)) == 3  # a Zcs entry without its table row
     mz_, vz = configs.small_zcs()
@@ -102,3 +106,17 @@ def test_band_order_matches_reorder_semantics():
     assert np.array_equal(order, ref)
     b = B.band_of(mz)
     assert n1 == int(np.sum(b == 1)) and n2 == int(np.sum(b == 2))
+
+
+def test_decoded_lineshapes_of_every_type_match_oracle(oracle_mod):
+    """The decoded point table's lineshapes (spline waves, revised K-matrices, the triangle cusp, next to
+    Breit-Wigners), evaluated on the host by the same functions the kernels use, against the FP64
+    oracle over the kinematic ranges (cusp masses away from its branch jumps: both are FP64, so they
+    only differ where one side rounds across a jump, which a scan does not hit)."""
+    mdl, vals = configs.lineshapes()
+    b = M.build_param_block(mdl, vals)
+    for mkp, mz in zip(np.linspace(1.433, 2.52, 97), np.linspace(4.036, 5.125, 97)):
+        ls, pc = lib.host_lineshapes(b, float(mkp), float(mz))
+        ols, opc = oracle_mod.lineshapes(b, float(mkp), float(mz))
+        assert np.allclose(ls, ols, rtol=1e-12, atol=1e-300), (mkp, ls, ols)
+        assert np.allclose(pc, opc, rtol=1e-11, atol=1e-300), (mz, pc, opc)
