@@ -221,6 +221,45 @@ int pwa_basis_from_angles(const double* d_angles, int64_t n, float* d_pp, float*
  * px py pz E) into device [15][n] (the first 15 rows of the layout above). */
 int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles, void* stream);
 
+/* ---- Learned proposal density (no counterpart in the reference, whose toys are flat hit-or-miss,
+ * gen_toys/create_efficiency/hit_and_reject.py:40-50; the exact amplitude reweights every event).
+ *
+ * Unit coordinates x in [0,1]^7 of the phase space: x0, x1 the Dalitz point (m^2(Kp) linear in x0, then
+ * m^2(J/psi p) linear in x1 across the Dalitz row), x2..x4 the decay's orientation in the Lambda_b rest
+ * frame (cos of the J/psi angle to the flight axis, its azimuth, the roll of the decay plane), x5, x6 the
+ * mu+ direction in the J/psi frame.  Arrays of x are device doubles [7][ldx] (coordinate-major). */
+
+/* Events at unit coordinates into columns [col0, col0 + n) of device planes (reference layout, as
+ * pwa_generate_events writes them; data != 0 writes the data weight sentinel, else weight w), and
+ * (d_flat, optional) the flat phase-space density of each x. */
+int pwa_events_from_unit(const double* d_x, int64_t ldx, int64_t n, float* d_pp, float* d_pp1, float* d_pp2,
+                         int64_t n_size, int64_t col0, float w, int data, double* d_flat, void* stream);
+/* n flat phase-space events in unit coordinates (counter-based: event i is a function of (seed, first_id + i)). */
+int pwa_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* d_x, int64_t ldx, void* stream);
+
+/* The proposal network: autoregressive 4 x 256 SiLU MLP over x (masked), 64 bins per coordinate,
+ * q(x) = prod_d 64 p_d(bin(x_d) | x_<d).  Kernels: BF16 tcgen05 GEMMs with FP32 accumulation in TMEM,
+ * fused epilogues; Adam on FP32 master weights.  max_batch: a multiple of 128 (rows per step / chunk). */
+typedef struct pwa_flow pwa_flow;
+int pwa_flow_create(int device, int max_batch, uint64_t seed, pwa_flow** out);
+int pwa_flow_destroy(pwa_flow* flow);
+/* Parameters (FP32, layer by layer: weights [out x in] row-major then biases; layers 256 x 64,
+ * 3 x 256 x 256, 512 x 256). */
+int64_t pwa_flow_param_count(void);
+int pwa_flow_get_params(pwa_flow* flow, float* h_params);
+int pwa_flow_set_params(pwa_flow* flow, const float* h_params);
+/* One Adam step (learning rate lr) on the loss -sum_i w_i log q(x_i) / sum_i w_i of n events (n a multiple
+ * of 128, at most max_batch; d_w device doubles); *loss: the loss before the step. */
+int pwa_flow_train_step(pwa_flow* flow, const double* d_x, int64_t ldx, const double* d_w, int n, float lr,
+                        double* loss);
+/* The same loss and its gradients (h_grad: pwa_flow_param_count floats, parameter layout) without an update. */
+int pwa_flow_gradients(pwa_flow* flow, const double* d_x, int64_t ldx, const double* d_w, int n, double* loss,
+                       float* h_grad);
+/* log q(x) of n events into device floats. */
+int pwa_flow_log_density(pwa_flow* flow, const double* d_x, int64_t ldx, int64_t n, float* d_logq);
+/* n events drawn from q (counter-based on seed): x into device doubles [7][ldx], log q(x) into d_logq. */
+int pwa_flow_sample(pwa_flow* flow, int64_t n, uint64_t seed, double* d_x, int64_t ldx, float* d_logq);
+
 /* Allocation-free likelihood evaluation.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory while they evaluate the likelihood -- for

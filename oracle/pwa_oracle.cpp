@@ -411,7 +411,7 @@ cd revised_km_refactor(const float* pl, double mpp, int nr, int irst, int ired, 
 // from acos(Re / |z|), negative for Im < 0; atan(z) = -i/2 log((1 + i z) / (1 - i z)).
 cd clog_ref(cd x) {
   const double r = std::sqrt(x.real() * x.real() + x.imag() * x.imag());
-  double th = std::acos(x.real() / r);
+  double th = std::acos(std::min(1.0, std::max(-1.0, x.real() / r)));  // clamped against rounding
   if (x.imag() < 0) th = -th;
   return cd(std::log(r), th);
 }

@@ -375,6 +375,112 @@ int init_tables() {
   return 0;
 }
 
+// ------------------------------------------------------------------ unit coordinates
+// The phase space as a map from x in [0,1]^7 (the coordinates of the learned proposal density):
+// s1 = m^2(Kp) linear in x0 over [(m_p + m_K)^2, (m_Lb - m_J/psi)^2], s2 = m^2(J/psi p) linear in x1
+// over the Dalitz row at s1; the decay's orientation in the Lambda_b rest frame from the J/psi
+// direction (cos theta = 2 x2 - 1 to the flight axis, azimuth 2 pi x3) and the roll 2 pi x4 of the decay
+// plane about it (together a uniform rotation); the mu+ direction in the J/psi rest frame
+// (cos = 2 x5 - 1, phi = 2 pi x6 - pi), as the flat generator above draws it.  Flat phase space has
+// density (s1 range) (row length at s1) / (Dalitz area) in these coordinates.
+__host__ __device__ inline void dalitz_row(double s1, double& lo, double& hi) {
+  const double M = M_LB, m1 = sqrt(s1);
+  const double ep = (s1 - M_K * M_K + M_P * M_P) / (2 * m1);
+  const double epsi = (M * M - s1 - M_JPSI * M_JPSI) / (2 * m1);
+  const double qp = sqrt(fmax(ep * ep - M_P * M_P, 0.0)), qpsi = sqrt(fmax(epsi * epsi - M_JPSI * M_JPSI, 0.0));
+  lo = sq(ep + epsi) - sq(qp + qpsi);
+  hi = sq(ep + epsi) - sq(qp - qpsi);
+}
+constexpr double S1_LO = (M_P + M_K) * (M_P + M_K), S1_HI = (M_LB - M_JPSI) * (M_LB - M_JPSI);
+
+__device__ void event_from_unit(const double* x, V4& p, V4& k, V4& mup, V4& mum, double& row_len) {
+  const double M = M_LB;
+  const double s1 = S1_LO + (S1_HI - S1_LO) * x[0];
+  double lo, hi;
+  dalitz_row(s1, lo, hi);
+  row_len = hi - lo;
+  const double s2 = lo + (hi - lo) * x[1];
+  const double s3 = M * M + M_JPSI * M_JPSI + M_P * M_P + M_K * M_K - s1 - s2;
+  const double Epsi = (M * M + M_JPSI * M_JPSI - s1) / (2 * M);
+  const double Ek = (M * M + M_K * M_K - s2) / (2 * M);
+  const double Ep = (M * M + M_P * M_P - s3) / (2 * M);
+  const double qpsi = sqrt(fmax(Epsi * Epsi - M_JPSI * M_JPSI, 0.0));
+  const double qk = sqrt(fmax(Ek * Ek - M_K * M_K, 0.0));
+  const double qp = sqrt(fmax(Ep * Ep - M_P * M_P, 0.0));
+  const double ca = clamp1((qpsi * qpsi + qp * qp - qk * qk) / (2 * qpsi * qp));
+  const double sa = sqrt(fmax(1 - ca * ca, 0.0));
+  const V3 psi3{qpsi, 0, 0}, p3{-qp * ca, qp * sa, 0};
+  const V3 k3 = -(psi3 + p3);
+  const double ct = 2 * x[2] - 1, st = sqrt(fmax(1 - ct * ct, 0.0));
+  const double ph = 2 * M_PI * x[3], chi = 2 * M_PI * x[4];
+  const V3 e1{st * cos(ph), st * sin(ph), ct};
+  const V3 e2{-sin(ph), cos(ph), 0.0};
+  const V3 e3{-ct * cos(ph), -ct * sin(ph), st};
+  const V3 f2 = cos(chi) * e2 + sin(chi) * e3, f3 = cos(chi) * e3 - sin(chi) * e2;
+  auto rot = [&](V3 v) { return v.x * e1 + v.y * f2 + v.z * f3; };
+  const V4 psi{rot(psi3), Epsi};
+  p = V4{rot(p3), Ep};
+  k = V4{rot(k3), Ek};
+  const double qmu = two_body_p(M_JPSI, MU, MU);
+  const double c = 2 * x[5] - 1, phm = 2 * M_PI * x[6] - M_PI;
+  const double sn = sqrt(fmax(1 - c * c, 0.0));
+  const V3 mu3{qmu * sn * cos(phm), qmu * sn * sin(phm), qmu * c};
+  const double emu = sqrt(qmu * qmu + MU * MU);
+  const V3 bpsi = (1.0 / psi.e) * psi.p;
+  mup = boost(V4{mu3, emu}, bpsi);
+  mum = boost(V4{-mu3, emu}, bpsi);
+}
+
+__global__ void k_events_from_unit(const double* __restrict__ x, int64_t ldx, int64_t n, float* pp, float* pp1,
+                                   float* pp2, int64_t ns, int64_t col0, float w, int data, double* flat,
+                                   double norm) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double u[7];
+  for (int d = 0; d < 7; ++d) u[d] = x[d * ldx + t];
+  V4 p, k, mup, mum;
+  double row_len;
+  event_from_unit(u, p, k, mup, mum, row_len);
+  write_basis(helicity_angles(p, k, mup, mum), pp, pp1, pp2, ns, col0 + t, data ? -1001.f : w);
+  if (flat) flat[t] = row_len * norm;
+}
+
+// Flat phase space in unit coordinates: x0 by rejection against the Dalitz row length (max_len
+// bounds it), the other coordinates uniform.
+__global__ void k_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* x, int64_t ldx, double max_len) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  Rng R;
+  R.id = first_id + (uint64_t)t;
+  R.k0 = (uint32_t)seed ^ 0x75u;
+  R.k1 = (uint32_t)(seed >> 32);
+  double x0 = R.uni();
+  for (int it = 0; it < 1000; ++it) {  // acceptance is above one half: 1000 tries never run out in practice
+    double lo, hi;
+    dalitz_row(S1_LO + (S1_HI - S1_LO) * x0, lo, hi);
+    if (R.uni() * max_len < hi - lo) break;
+    x0 = R.uni();
+  }
+  x[t] = x0;
+  for (int d = 1; d < 7; ++d) x[d * ldx + t] = R.uni();
+}
+
+// Dalitz area in (s1, s2) and the largest row length (Simpson's rule on the row length).
+static void dalitz_area(double* area, double* max_len) {
+  const int n = 20000;
+  const double h = (S1_HI - S1_LO) / n;
+  double a = 0, mx = 0;
+  for (int i = 0; i <= n; ++i) {
+    double lo, hi;
+    dalitz_row(S1_LO + i * h, lo, hi);
+    const double len = hi - lo;
+    a += len * ((i == 0 || i == n) ? 1 : (i % 2 ? 4 : 2));
+    mx = fmax(mx, len);
+  }
+  *area = a * h / 3;
+  *max_len = mx * 1.001;
+}
+
 }  // namespace gen
 }  // namespace pwa
 
@@ -415,6 +521,28 @@ int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles
   if (n == 0) return PWA_OK;
   cudaStream_t st = (cudaStream_t)stream;
   pwa::gen::k_angles_from_vectors<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(d_vectors, n, d_angles);
+  return cudaStreamSynchronize(st) == cudaSuccess ? PWA_OK : PWA_E_CUDA;
+}
+int pwa_events_from_unit(const double* d_x, int64_t ldx, int64_t n, float* d_pp, float* d_pp1, float* d_pp2,
+                         int64_t n_size, int64_t col0, float w, int data, double* d_flat, void* stream) {
+  if (!d_x || !d_pp || !d_pp1 || !d_pp2 || n < 0 || ldx < n || col0 < 0 || col0 + n > n_size) return PWA_E_ARG;
+  if (n == 0) return PWA_OK;
+  if (pwa::gen::init_tables()) return PWA_E_CUDA;
+  double area, max_len;
+  pwa::gen::dalitz_area(&area, &max_len);
+  cudaStream_t st = (cudaStream_t)stream;
+  pwa::gen::k_events_from_unit<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+      d_x, ldx, n, d_pp, d_pp1, d_pp2, n_size, col0, w, data, d_flat, (pwa::gen::S1_HI - pwa::gen::S1_LO) / area);
+  return cudaStreamSynchronize(st) == cudaSuccess ? PWA_OK : PWA_E_CUDA;
+}
+
+int pwa_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* d_x, int64_t ldx, void* stream) {
+  if (!d_x || n < 0 || ldx < n) return PWA_E_ARG;
+  if (n == 0) return PWA_OK;
+  double area, max_len;
+  pwa::gen::dalitz_area(&area, &max_len);
+  cudaStream_t st = (cudaStream_t)stream;
+  pwa::gen::k_unit_flat<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, seed, first_id, d_x, ldx, max_len);
   return cudaStreamSynchronize(st) == cudaSuccess ? PWA_OK : PWA_E_CUDA;
 }
 }

@@ -387,8 +387,10 @@ __device__ bool interval_ok(const PointTable& T, const cplx* base, int stride, d
       for (int q = 0; q < gr.count; ++q) {
         cplx acc = mk(0, 0);
         for (int n = 0; n < 6; ++n) acc += base[n * stride + gr.first + q] * w[n];
-        emax = fmax(emax, sqrt(norm2(acc - ex[q])));
-        vmax = fmax(vmax, sqrt(norm2(ex[q])));
+        // written so that a non-finite node or exact value propagates (fmax would drop a NaN)
+        const double e = sqrt(norm2(acc - ex[q])), v = sqrt(norm2(ex[q]));
+        if (!(e <= emax)) emax = e;
+        if (!(v <= vmax)) vmax = v;
       }
       if (!(isfinite(emax) && emax <= TAB_CHECK_TOL * vmax)) return false;
     }

@@ -89,13 +89,15 @@ __host__ __device__ inline cplx rkm_lineshape(const PointTable& T, int c, int i,
 
 // Complex division and the reference's complex logarithm and arctangent (RooTDalitz/cuComplex.h:
 // 660-676): the argument from acos(Re / |z|), negated for Im < 0; atan(z) = -i/2 log((1 + i z) / (1 - i z)).
+// Re / |z| is clamped to [-1, 1]: rounding can push it just outside for a nearly real z, where acos
+// would return NaN (the reference's float code has the same hazard).
 __host__ __device__ inline cplx cdiv(cplx a, cplx b) {
   const double d = 1.0 / (b.re * b.re + b.im * b.im);
   return mk((a.re * b.re + a.im * b.im) * d, (a.im * b.re - a.re * b.im) * d);
 }
 __host__ __device__ inline cplx clog_ref(cplx x) {
   const double r = sqrt(x.re * x.re + x.im * x.im);
-  double th = acos(x.re / r);
+  double th = acos(fmin(1.0, fmax(-1.0, x.re / r)));
   if (x.im < 0) th = -th;
   return mk(log(r), th);
 }

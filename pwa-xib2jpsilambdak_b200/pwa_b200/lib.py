@@ -19,7 +19,10 @@ EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_c
             "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing", "pwa_ctx_select_data",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
             "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
-            "pwa_host_lineshapes", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_basis_from_angles", "pwa_angles_from_vectors",
+            "pwa_host_lineshapes", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_events_from_unit",
+            "pwa_unit_flat", "pwa_flow_create", "pwa_flow_destroy", "pwa_flow_param_count", "pwa_flow_get_params",
+            "pwa_flow_set_params", "pwa_flow_train_step", "pwa_flow_gradients", "pwa_flow_log_density",
+            "pwa_flow_sample", "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
 
 _fp = C.POINTER(C.c_float)
