@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--small", action="store_true", help="1/10 of the workload (for profiling captures)")
     ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
+    ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
     ap.add_argument("--no-full-parity", action="store_true",
                     help="skip the FP64 oracle check of the whole sample (centre and one point per batch kind)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
@@ -255,6 +256,94 @@ def full_size_parity(dsample, block, ctx, labels, gblocks, bres, probe) -> dict:
     worst = max(max(abs(r["dnll_plain"]), abs(r["dnll_batched"] or 0.0)) for r in rows)
     return {"sample_events": dsample.n, "points": rows, "max_abs_dnll": worst,
             "oracle_threads": os.cpu_count(), "seconds": round(time.perf_counter() - t0, 1)}
+
+
+# ------------------------------------------------------------------------------ learned proposal
+PROPOSAL = {"model": "full_bw", "n_train": 10_000_000, "n_toy": 10_000_000, "n_norm": 5_000_000, "batch": 65536,
+            "epochs": 4, "lr": 3e-3, "chunk": 1 << 20}
+# FLOPs per event of one training step: forward (64x256 + 3 x 256^2 + 256x512), backward through the
+# activations (512x256 + 3 x 256^2) and the weight gradients (512x256 + 3 x 256^2 + 256x64), 2 per MAC
+PROPOSAL_FLOP_PER_ROW = 2.0 * ((64 * 256 + 3 * 256 ** 2 + 256 * 512) + (512 * 256 + 3 * 256 ** 2)
+                               + (512 * 256 + 3 * 256 ** 2 + 256 * 64))
+
+
+def _amp2_unit(ctx, block, x, chunk):
+    """|A|^2 and the flat phase-space density at unit coordinates x (torch [7, n] on the device)."""
+    import torch
+    from pwa_b200 import flow
+    a2, fl = [], []
+    for c0 in range(0, x.shape[1], chunk):
+        xs = x[:, c0:c0 + chunk].contiguous()
+        (pp, pp1, pp2, ns), f = flow.events_from_unit(xs)
+        sw = torch.zeros(ns, dtype=torch.float32, device=x.device)
+        ctx.bind_planes(pp, pp1, pp2, sw, xs.shape[1], ns)
+        a2.append(torch.as_tensor(ctx.amp2(block), device=x.device))
+        fl.append(f)
+        del pp, pp1, pp2
+    return torch.cat(a2), torch.cat(fl)
+
+
+def proposal_bench(device: int, bf16_peak: float) -> dict:
+    """The learned proposal (trained on the GPU, BF16 tcgen05 GEMMs) against flat hit-or-miss on the
+    full Breit-Wigner model: amplitude evaluations per accepted toy event (acceptance against 1.05 x the
+    largest weight, as the hit-or-miss toy maker does with its global maximum), and amplitude evaluations
+    for equal statistical error of the normalisation integral (importance sampling, weights |A|^2 flat / q)."""
+    import torch
+    from pwa_b200 import configs, flow, lib, model as M
+    P = PROPOSAL
+    mdl, vals = configs.MODELS[P["model"]]()
+    block = M.build_param_block(mdl, vals)
+    ctx = lib.Context(device)
+    t0 = time.perf_counter()
+    xt = flow.flat_unit(P["n_train"], seed=501, device=device)
+    a2t, _ = _amp2_unit(ctx, block, xt, P["chunk"])
+    t_data = time.perf_counter() - t0
+    f = flow.Flow(device, max_batch=P["batch"], seed=11)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    hist = f.train(xt, a2t, epochs=P["epochs"], batch=P["batch"], lr=P["lr"])
+    torch.cuda.synchronize(device)
+    t_train = time.perf_counter() - t0
+    steps = len(hist)
+    del xt, a2t
+    # toys: candidates from q vs flat candidates
+    xq, lq = f.sample(P["n_toy"], seed=502)
+    a2q, flq = _amp2_unit(ctx, block, xq, P["chunk"])
+    wq = a2q * flq / torch.exp(lq.double())
+    xf = flow.flat_unit(P["n_toy"], seed=503, device=device)
+    a2f, _ = _amp2_unit(ctx, block, xf, P["chunk"])
+    g = torch.Generator(device=f"cuda:{device}").manual_seed(504)
+
+    def accepted(w):
+        mx = 1.05 * float(w.max())
+        return int((torch.rand(w.numel(), generator=g, device=w.device, dtype=torch.float64) * mx < w).sum())
+
+    acc_q, acc_f = accepted(wq), accepted(a2f)
+    evals_q, evals_f = P["n_toy"] / max(acc_q, 1), P["n_toy"] / max(acc_f, 1)
+    # normalisation integral on the first n_norm events of each
+    nn = P["n_norm"]
+    wn, fn = wq[:nn], a2f[:nn]
+    i_q, i_f = float(wn.mean()), float(fn.mean())
+    rv_q, rv_f = float(wn.var()) / i_q ** 2, float(fn.var()) / i_f ** 2
+    ctx.close()
+    f.close()
+    gain = evals_f / evals_q
+    tflops = PROPOSAL_FLOP_PER_ROW * P["batch"] * steps / t_train / 1e12
+    return {
+        "model": "full_bw (14 Lambda* BW up to J = 7/2, 3 narrow Pc BW): the batched-gradient config's model",
+        "network": "autoregressive 4 x 256 SiLU MLP, 64 bins per coordinate, BF16 tcgen05 GEMMs, FP32 accumulation",
+        "train_events": P["n_train"], "epochs": P["epochs"], "steps": steps, "batch": P["batch"],
+        "train_s": round(t_train, 3), "data_s": round(t_data, 3), "loss_first": hist[0], "loss_last": hist[-1],
+        "train_tflops": round(tflops, 2),
+        "train_frac_of_bf16_peak": round(tflops / bf16_peak, 4),
+        "toy_candidates": P["n_toy"], "accepted_flat": acc_f, "accepted_learned": acc_q,
+        "evals_per_accepted_flat": round(evals_f, 3), "evals_per_accepted_learned": round(evals_q, 3),
+        "evals_per_accepted_gain": round(gain, 3), "target_gain": 10.0, "target_met": bool(gain >= 10.0),
+        "norm_events": nn, "norm_integral_flat": i_f, "norm_integral_learned": i_q,
+        "norm_rel_diff": (i_q - i_f) / i_f,
+        "norm_rel_diff_in_sigma": (i_q - i_f) / np.sqrt(float(wn.var()) / nn + float(fn.var()) / nn),
+        "norm_evals_gain_equal_error": round(rv_f / rv_q, 3),
+    }
 
 
 # ------------------------------------------------------------------------------ GPU arm
@@ -467,6 +556,11 @@ def main():
                                                   probe)
         except Exception as ex:
             out["parity_full"] = {"failed": str(ex)}
+    if world == 1 and not args.no_proposal:
+        try:
+            out["proposal"] = proposal_bench(local, bf16)
+        except Exception as ex:
+            out["proposal"] = {"failed": str(ex)}
     if bat:
         out = batched_line(out, bat, args, world, sample, req_b, hbm, peak_kind)
     print(json.dumps(out))

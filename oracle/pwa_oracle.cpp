@@ -415,9 +415,15 @@ cd clog_ref(cd x) {
   if (x.imag() < 0) th = -th;
   return cd(std::log(r), th);
 }
+// complex division as a / b = a conj(b) / |b|^2 (the reference's own algorithm scales instead; the
+// two agree to rounding, and this form is the one the device code uses)
+cd cdiv(cd a, cd b) {
+  const double d = 1.0 / (b.real() * b.real() + b.imag() * b.imag());
+  return cd((a.real() * b.real() + a.imag() * b.imag()) * d, (a.imag() * b.real() - a.real() * b.imag()) * d);
+}
 cd catan_ref(cd x) {
   const cd ii(0, 1);
-  return -0.5 * (ii * clog_ref((1.0 + ii * x) / (1.0 - ii * x)));
+  return -0.5 * (ii * clog_ref(cdiv(1.0 + ii * x, 1.0 - ii * x)));
 }
 
 cd cusp_amp(double m_r, double gamma, double mpp) {  // GetCusp_AMP
@@ -434,9 +440,9 @@ cd cusp_amp(double m_r, double gamma, double mpp) {  // GetCusp_AMP
     const cd b = (alpha * (p12 * p12 - p13 * p13 - p23 * p23) + m3 * m3 - m2 * m2) / p23 / p23 + 1.0 - 0.001 * ii;
     const cd c = (alpha * (m1 * m1 - m3 * m3) + m3 * m3 - alpha * (1.0 - alpha) * p13 * p13) / (p23 * p23);
     const cd sv = csqrt_branch(4.0 * c - b * b);
-    const cd t1 = catan_ref(b / sv);
-    const cd t2 = catan_ref((b + 2.0 * (alpha - 1.0)) / sv);
-    integral += dx * ((1.0 / sv) * (t1 - t2));
+    const cd t1 = catan_ref(cdiv(b, sv));
+    const cd t2 = catan_ref(cdiv(b + 2.0 * (alpha - 1.0), sv));
+    integral += dx * cdiv(t1 - t2, sv);
   }
   return integral * (1.0 / mpp / mpp);
 }

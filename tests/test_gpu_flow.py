@@ -26,8 +26,10 @@ def test_log_density_matches_float32_reference():
     x = torch.rand((7, 1024), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
     lq = f.log_density(x).cpu().numpy()
     ref, _ = R.log_q(params, x.cpu().numpy(), torch.float32, emulate_bf16=True)
-    # BF16 operands with FP32 accumulation on both sides; only summation order differs
-    assert np.max(np.abs(lq - ref.numpy())) < 2e-3, np.max(np.abs(lq - ref.numpy()))
+    # BF16 operands with FP32 accumulation on both sides: summation order differs, and now and then an
+    # activation rounds to the other neighbouring BF16 value
+    d = np.abs(lq - ref.numpy())
+    assert np.median(d) < 1e-5 and np.max(d) < 1e-2, (np.median(d), np.max(d))
     f.close()
 
 
@@ -84,11 +86,11 @@ def test_trained_proposal_is_unbiased_and_beats_hit_or_miss():
     blk = M.build_param_block(mdl, vals)
     ctx = lib.Context(0)
     n = 1 << 18
-    xt = flow.flat_unit(n, seed=21)
+    xt = flow.flat_unit(1 << 21, seed=21)
     a2t, _ = _amp2_at(ctx, blk, xt)
-    f = flow.Flow(0, max_batch=65536, seed=7)
-    hist = f.train(xt, a2t, epochs=6, batch=65536, lr=3e-3)
-    assert hist[-1] < hist[0]
+    f = flow.Flow(0, max_batch=16384, seed=7)
+    hist = f.train(xt, a2t, epochs=6, batch=16384, lr=3e-3)
+    assert np.mean(hist[-20:]) < np.mean(hist[:20])
     # flat hit-or-miss vs the learned proposal on fresh events
     xf = flow.flat_unit(n, seed=22)
     a2f, _ = _amp2_at(ctx, blk, xf)
@@ -98,8 +100,11 @@ def test_trained_proposal_is_unbiased_and_beats_hit_or_miss():
     i_f, s_f = float(a2f.mean()), float(a2f.std()) / np.sqrt(n)
     i_q, s_q = float(wq.mean()), float(wq.std()) / np.sqrt(n)
     assert abs(i_q - i_f) < 5 * np.hypot(s_f, s_q), (i_f, s_f, i_q, s_q)
-    evals_flat = float(a2f.max()) / i_f
-    evals_q = float(wq.max()) / i_q
-    assert evals_q < evals_flat / 2, (evals_flat, evals_q)
+    # amplitude evaluations per accepted toy event (hit-or-miss against the largest weight) and per
+    # effective event of a weighted sample
+    evals_flat, evals_q = float(a2f.max()) / i_f, float(wq.max()) / i_q
+    ess_flat = i_f ** 2 / float((a2f ** 2).mean())
+    ess_q = i_q ** 2 / float((wq ** 2).mean())
+    assert ess_q > 2 * ess_flat and evals_q < evals_flat / 2, (evals_flat, evals_q, ess_flat, ess_q)
     ctx.close()
     f.close()
