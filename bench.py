@@ -260,7 +260,7 @@ def full_size_parity(dsample, block, ctx, labels, gblocks, bres, probe) -> dict:
 
 # ------------------------------------------------------------------------------ learned proposal
 PROPOSAL = {"model": "full_bw", "n_train": 10_000_000, "n_toy": 10_000_000, "n_norm": 5_000_000, "batch": 65536,
-            "epochs": 4, "lr": 3e-3, "chunk": 1 << 20}
+            "epochs": 4, "lr": 3e-3, "chunk": 1 << 20, "premap_mix": 0.1}
 # FLOPs per event of one training step: forward (64x256 + 3 x 256^2 + 256x512), backward through the
 # activations (512x256 + 3 x 256^2) and the weight gradients (512x256 + 3 x 256^2 + 256x64), 2 per MAC
 PROPOSAL_FLOP_PER_ROW = 2.0 * ((64 * 256 + 3 * 256 ** 2 + 256 * 512) + (512 * 256 + 3 * 256 ** 2)
@@ -301,6 +301,7 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
     f = flow.Flow(device, max_batch=P["batch"], seed=11)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
+    f.fit_premap(xt, a2t, mix=P["premap_mix"])
     hist = f.train(xt, a2t, epochs=P["epochs"], batch=P["batch"], lr=P["lr"])
     torch.cuda.synchronize(device)
     t_train = time.perf_counter() - t0
@@ -309,7 +310,9 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
     # toys: candidates from q vs flat candidates
     xq, lq = f.sample(P["n_toy"], seed=502)
     a2q, flq = _amp2_unit(ctx, block, xq, P["chunk"])
-    wq = a2q * flq / torch.exp(lq.double())
+    inside = flq > 0  # candidates outside the Dalitz region: weight 0, no amplitude to evaluate
+    n_inside = int(inside.sum())
+    wq = torch.where(inside, a2q * flq / torch.exp(lq.double()), torch.zeros_like(a2q))
     xf = flow.flat_unit(P["n_toy"], seed=503, device=device)
     a2f, _ = _amp2_unit(ctx, block, xf, P["chunk"])
     g = torch.Generator(device=f"cuda:{device}").manual_seed(504)
@@ -319,7 +322,11 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
         return int((torch.rand(w.numel(), generator=g, device=w.device, dtype=torch.float64) * mx < w).sum())
 
     acc_q, acc_f = accepted(wq), accepted(a2f)
-    evals_q, evals_f = P["n_toy"] / max(acc_q, 1), P["n_toy"] / max(acc_f, 1)
+    evals_q, evals_f = n_inside / max(acc_q, 1), P["n_toy"] / max(acc_f, 1)
+    # the same in expectation: (amplitude evaluations per candidate) x max weight / mean weight
+    exp_q = n_inside / P["n_toy"] * 1.05 * float(wq.max()) / float(wq.mean())
+    exp_f = 1.05 * float(a2f.max()) / float(a2f.mean())
+    q999 = float(torch.quantile(wq[inside][:1 << 24].float(), 0.999)) / float(wq.mean())
     # normalisation integral on the first n_norm events of each
     nn = P["n_norm"]
     wn, fn = wq[:nn], a2f[:nn]
@@ -336,7 +343,11 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
         "train_s": round(t_train, 3), "data_s": round(t_data, 3), "loss_first": hist[0], "loss_last": hist[-1],
         "train_tflops": round(tflops, 2),
         "train_frac_of_bf16_peak": round(tflops / bf16_peak, 4),
-        "toy_candidates": P["n_toy"], "accepted_flat": acc_f, "accepted_learned": acc_q,
+        "premap": f"per-coordinate piecewise-linear CDF on 1024 cells, uniform floor {P['premap_mix']}",
+        "toy_candidates": P["n_toy"], "candidates_inside_dalitz": n_inside,
+        "accepted_flat": acc_f, "accepted_learned": acc_q,
+        "evals_per_accepted_expected_flat": round(exp_f, 3), "evals_per_accepted_expected_learned": round(exp_q, 3),
+        "learned_weight_q999_over_mean": round(q999, 3),
         "evals_per_accepted_flat": round(evals_f, 3), "evals_per_accepted_learned": round(evals_q, 3),
         "evals_per_accepted_gain": round(gain, 3), "target_gain": 10.0, "target_met": bool(gain >= 10.0),
         "norm_events": nn, "norm_integral_flat": i_f, "norm_integral_learned": i_q,

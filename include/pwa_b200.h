@@ -224,14 +224,16 @@ int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles
 /* ---- Learned proposal density (no counterpart in the reference, whose toys are flat hit-or-miss,
  * gen_toys/create_efficiency/hit_and_reject.py:40-50; the exact amplitude reweights every event).
  *
- * Unit coordinates x in [0,1]^7 of the phase space: x0, x1 the Dalitz point (m^2(Kp) linear in x0, then
- * m^2(J/psi p) linear in x1 across the Dalitz row), x2..x4 the decay's orientation in the Lambda_b rest
- * frame (cos of the J/psi angle to the flight axis, its azimuth, the roll of the decay plane), x5, x6 the
- * mu+ direction in the J/psi frame.  Arrays of x are device doubles [7][ldx] (coordinate-major). */
+ * Unit coordinates x in [0,1]^7 of the phase space: x0, x1 the Dalitz point (m^2(Kp) linear in x0 and
+ * m^2(J/psi p) linear in x1, each over its full range: the rectangle around the Dalitz region, 70 % of
+ * which is inside), x2..x4 the decay's orientation in the Lambda_b rest frame (cos of the J/psi angle to
+ * the flight axis, its azimuth, the roll of the decay plane), x5, x6 the mu+ direction in the J/psi
+ * frame.  Arrays of x are device doubles [7][ldx] (coordinate-major). */
 
 /* Events at unit coordinates into columns [col0, col0 + n) of device planes (reference layout, as
  * pwa_generate_events writes them; data != 0 writes the data weight sentinel, else weight w), and
- * (d_flat, optional) the flat phase-space density of each x. */
+ * (d_flat, optional) the flat phase-space density of each x: a constant inside the Dalitz region, 0
+ * outside (where the column holds a valid stand-in event and the caller evaluates no amplitude). */
 int pwa_events_from_unit(const double* d_x, int64_t ldx, int64_t n, float* d_pp, float* d_pp1, float* d_pp2,
                          int64_t n_size, int64_t col0, float w, int data, double* d_flat, void* stream);
 /* n flat phase-space events in unit coordinates (counter-based: event i is a function of (seed, first_id + i)). */
@@ -259,6 +261,16 @@ int pwa_flow_gradients(pwa_flow* flow, const double* d_x, int64_t ldx, const dou
 int pwa_flow_log_density(pwa_flow* flow, const double* d_x, int64_t ldx, int64_t n, float* d_logq);
 /* n events drawn from q (counter-based on seed): x into device doubles [7][ldx], log q(x) into d_logq. */
 int pwa_flow_sample(pwa_flow* flow, int64_t n, uint64_t seed, double* d_x, int64_t ldx, float* d_logq);
+/* Pre-maps: before the network, each coordinate passes a fixed monotone map u = F(x), piecewise linear
+ * through PWA_FLOW_PREMAP_NODES nodes at x = k / (nodes - 1), and q(x) = q_net(F(x)) prod_d F_d'(x_d).
+ * Identity at creation.  fit: F_d' = (1 - mix) (weighted histogram of x_d, normalised) + mix, from n
+ * events with weights w >= 0 (device doubles), 0 < mix <= 1; fit before training, as the network's
+ * input changes with them.  get/set: host doubles [7][PWA_FLOW_PREMAP_NODES] (set refuses rows that do
+ * not run strictly upward from 0 to 1). */
+#define PWA_FLOW_PREMAP_NODES 1025
+int pwa_flow_fit_premap(pwa_flow* flow, const double* d_x, int64_t ldx, const double* d_w, int64_t n, double mix);
+int pwa_flow_get_premap(pwa_flow* flow, double* h_cdf);
+int pwa_flow_set_premap(pwa_flow* flow, const double* h_cdf);
 
 /* Allocation-free likelihood evaluation.  No counterpart in the reference.
  *

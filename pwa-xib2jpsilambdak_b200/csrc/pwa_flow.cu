@@ -29,19 +29,24 @@ namespace pwa {
 namespace flow {
 
 // ------------------------------------------------------------------ element-wise kernels
-// Network input of n events: 2 x - 1 in columns 0..6 (row-major and feature-major), the target bins,
-// and the weights normalised by their sum (*wsum).
-__global__ void k_pack(const double* __restrict__ x, int64_t ldx, const double* __restrict__ w, const double* wsum,
-                       int n, int ldT, bf16* xin, bf16* xinT, uint8_t* bins, float* wn) {
+// Network input of n events: u = F(x) through the pre-maps, 2 u - 1 in columns 0..6 (row-major and
+// feature-major), the target bins of u, the weights normalised by their sum (*wsum), and (lq0) the
+// pre-maps' log Jacobian sum_d log F_d'(x_d), the part of log q(x) outside the network.
+__global__ void k_pack(const double* __restrict__ x, int64_t ldx, const double* __restrict__ pm,
+                       const double* __restrict__ w, const double* wsum, int n, int ldT, bf16* xin, bf16* xinT,
+                       uint8_t* bins, float* wn, float* lq0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   alignas(16) bf16 row[FLOW_IN];
 #pragma unroll
   for (int c = 0; c < FLOW_IN; ++c) row[c] = __float2bfloat16(0.0f);
+  double lpm = 0;
   for (int d = 0; d < FLOW_D; ++d) {
-    const double xd = x[(size_t)d * ldx + i];
-    row[d] = __float2bfloat16((float)(2.0 * xd - 1.0));
-    bins[(size_t)i * 8 + d] = (uint8_t)min(FLOW_BINS - 1, max(0, (int)floor(xd * FLOW_BINS)));
+    double logf;
+    const double ud = pm_forward(pm + d * PM_NODES, x[(size_t)d * ldx + i], &logf);
+    lpm += logf;
+    row[d] = __float2bfloat16((float)(2.0 * ud - 1.0));
+    bins[(size_t)i * 8 + d] = (uint8_t)min(FLOW_BINS - 1, max(0, (int)floor(ud * FLOW_BINS)));
   }
   bins[(size_t)i * 8 + 7] = 0;
   for (int c = 0; c < FLOW_IN; ++c) xinT[(size_t)c * ldT + i] = row[c];
@@ -50,6 +55,26 @@ __global__ void k_pack(const double* __restrict__ x, int64_t ldx, const double* 
 #pragma unroll
   for (int q = 0; q < FLOW_IN / 8; ++q) d[q] = s[q];
   if (wn) wn[i] = (float)(w[i] / *wsum);
+  if (lq0) lq0[i] = (float)lpm;
+}
+
+// Weighted histograms of the n events' coordinates on the pre-map cells (hist [D][PM_BINS], added
+// to): per block in shared memory, then once into global memory.
+__global__ void k_hist(const double* __restrict__ x, int64_t ldx, const double* __restrict__ w, int64_t n,
+                       double* hist) {
+  extern __shared__ double sh[];  // [D][PM_BINS]
+  for (int j = threadIdx.x; j < FLOW_D * PM_BINS; j += blockDim.x) sh[j] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double wi = w[i];
+    for (int d = 0; d < FLOW_D; ++d) {
+      const int k = min(PM_BINS - 1, max(0, (int)floor(x[(size_t)d * ldx + i] * PM_BINS)));
+      atomicAdd(&sh[d * PM_BINS + k], wi);
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < FLOW_D * PM_BINS; j += blockDim.x)
+    if (sh[j] != 0) atomicAdd(&hist[j], sh[j]);
 }
 
 __global__ void k_sum(const double* __restrict__ a, int n, double* out) {
@@ -165,6 +190,7 @@ struct pwa_flow {
   uint8_t* bins = nullptr;
   float *wn = nullptr, *logq = nullptr;
   double *acc = nullptr, *xs = nullptr;  // acc[0] weight sum, acc[1] loss
+  double* pm = nullptr;                  // pre-maps [D][PM_NODES]
   int* err = nullptr;
   CUtensorMap mxin, mxinT, mh[4], mhT[4], mdlog, mdlogT, mdz[2], mdzT;
   int64_t step = 0;
@@ -229,9 +255,9 @@ cudaError_t loss_and_grads(pwa_flow* f, const double* d_x, int64_t ldx, const do
   cudaError_t e;
   if ((e = cudaMemsetAsync(f->acc, 0, 2 * sizeof(double), f->st))) return e;
   k_sum<<<64, 256, 0, f->st>>>(d_w, n, f->acc);
-  k_pack<<<(n + 255) / 256, 256, 0, f->st>>>(d_x, ldx, d_w, f->acc, n, f->max_batch, f->xin, f->xinT, f->bins, f->wn);
+  k_pack<<<(n + 255) / 256, 256, 0, f->st>>>(d_x, ldx, f->pm, d_w, f->acc, n, f->max_batch, f->xin, f->xinT,
+                                              f->bins, f->wn, f->logq);
   if ((e = forward_hidden(f, n, true))) return e;
-  if ((e = cudaMemsetAsync(f->logq, 0, n * sizeof(float), f->st))) return e;
   EpiOutput out{f->L[4].b, f->bins, f->wn, f->dlog, f->dlogT, f->logq, n, f->max_batch, 1};
   if ((e = gemm<256>(f, f->mh[3], f->L[4].mapW, n, 2, FLOW_H, 1, out))) return e;
   k_loss<<<64, 256, 0, f->st>>>(f->wn, f->logq, n, f->acc + 1);
@@ -353,8 +379,16 @@ extern "C" int pwa_flow_create(int device, int max_batch, uint64_t seed, pwa_flo
       (e = dalloc(f, &f->dlog, B * FLOW_OUT)) || (e = dalloc(f, &f->dlogT, (size_t)FLOW_OUT * B)) ||
       (e = dalloc(f, &f->dzT, (size_t)FLOW_H * B)) || (e = dalloc(f, &f->bins, B * 8)) ||
       (e = dalloc(f, &f->wn, B)) || (e = dalloc(f, &f->logq, B)) || (e = dalloc(f, &f->acc, 2)) ||
-      (e = dalloc(f, &f->err, 1)))
+      (e = dalloc(f, &f->err, 1)) || (e = dalloc(f, &f->pm, (size_t)FLOW_D * PM_NODES)))
     return fail(e);
+  {  // identity pre-maps
+    std::vector<double> id((size_t)FLOW_D * PM_NODES);
+    for (int d = 0; d < FLOW_D; ++d)
+      for (int k = 0; k < PM_NODES; ++k) id[(size_t)d * PM_NODES + k] = (double)k / PM_BINS;
+    if ((e = cudaMemcpyAsync(f->pm, id.data(), id.size() * sizeof(double), cudaMemcpyHostToDevice, f->st)) ||
+        (e = cudaStreamSynchronize(f->st)))
+      return fail(e);
+  }
   for (int l = 0; l < 4; ++l)
     if ((e = dalloc(f, &f->z[l], B * FLOW_H)) || (e = dalloc(f, &f->h[l], B * FLOW_H)) ||
         (e = dalloc(f, &f->hT[l], (size_t)FLOW_H * B)))
@@ -423,10 +457,9 @@ extern "C" int pwa_flow_log_density(pwa_flow* f, const double* d_x, int64_t ldx,
   for (int64_t c0 = 0; c0 < n; c0 += f->max_batch) {
     const int m = (int)std::min<int64_t>(f->max_batch, n - c0);
     const int mp = (m + 127) / 128 * 128;
-    k_pack<<<(m + 255) / 256, 256, 0, f->st>>>(d_x + c0, ldx, nullptr, nullptr, m, f->max_batch, f->xin, f->xinT,
-                                                f->bins, nullptr);
+    k_pack<<<(m + 255) / 256, 256, 0, f->st>>>(d_x + c0, ldx, f->pm, nullptr, nullptr, m, f->max_batch, f->xin,
+                                                f->xinT, f->bins, nullptr, d_logq + c0);
     if ((e = forward_hidden(f, mp, false))) return cuda_fail(e);
-    if ((e = cudaMemsetAsync(d_logq + c0, 0, m * sizeof(float), f->st))) return cuda_fail(e);
     EpiOutput out{f->L[4].b, f->bins, nullptr, nullptr, nullptr, d_logq + c0, m, f->max_batch, 0};
     if ((e = gemm<256>(f, f->mh[3], f->L[4].mapW, mp, 2, FLOW_H, 1, out))) return cuda_fail(e);
   }
@@ -447,7 +480,7 @@ extern "C" int pwa_flow_sample(pwa_flow* f, int64_t n, uint64_t seed, double* d_
       return cuda_fail(e);
     for (int d = 0; d < FLOW_D; ++d) {
       if ((e = forward_hidden(f, mp, false))) return cuda_fail(e);
-      EpiSample smp{f->L[4].b, d_x + c0, f->xin, f->bins, d_logq + c0, seed, c0, m, (int)ldx, d};
+      EpiSample smp{f->L[4].b, d_x + c0, f->xin, f->bins, d_logq + c0, f->pm, seed, c0, m, (int)ldx, d};
       if ((e = gemm<256>(f, f->mh[3], f->L[4].mapW, mp, 1, FLOW_H, 1, smp, d / 4))) return cuda_fail(e);
     }
   }
@@ -483,6 +516,73 @@ extern "C" int pwa_flow_set_params(pwa_flow* f, const float* h_params) {
     o += nw + LAYER_OUT[l];
   }
   if (e == cudaSuccess) e = repack(f);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->st);
+  return e == cudaSuccess ? PWA_OK : cuda_fail(e);
+}
+
+// Fits the pre-maps to the weighted marginals of n events (x: device doubles [7][ldx], w: device
+// doubles [n], w >= 0): F_d' = (1 - mix) x (the weighted histogram of x_d on PM_BINS cells, normalised)
+// + mix (a uniform floor that keeps F strictly increasing).  The network's input changes with the
+// pre-maps: fit them before training.
+extern "C" int pwa_flow_fit_premap(pwa_flow* f, const double* d_x, int64_t ldx, const double* d_w, int64_t n,
+                                   double mix) {
+  if (!f || !d_x || !d_w || n < 1 || ldx < n || !(mix > 0.0 && mix <= 1.0)) return PWA_E_ARG;
+  cudaError_t e = cudaSetDevice(f->device);
+  if (e) return cuda_fail(e);
+  const size_t cells = (size_t)FLOW_D * PM_BINS;
+  double* d_hist = nullptr;
+  if ((e = cudaMalloc(&d_hist, cells * sizeof(double)))) return cuda_fail(e);
+  std::vector<double> hist(cells), cdf((size_t)FLOW_D * PM_NODES);
+  const int smem = (int)(cells * sizeof(double));
+  e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, cells * sizeof(double), f->st);
+  if (e == cudaSuccess) {
+    k_hist<<<296, 512, smem, f->st>>>(d_x, ldx, d_w, n, d_hist);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hist.data(), d_hist, cells * sizeof(double), cudaMemcpyDeviceToHost, f->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->st);
+  cudaFree(d_hist);
+  if (e) return cuda_fail(e);
+  for (int d = 0; d < FLOW_D; ++d) {
+    const double* h = hist.data() + (size_t)d * PM_BINS;
+    double tot = 0;
+    for (int k = 0; k < PM_BINS; ++k) tot += h[k];
+    if (!(tot > 0) || !std::isfinite(tot)) return PWA_E_ARG;
+    double* c = cdf.data() + (size_t)d * PM_NODES;
+    c[0] = 0;
+    for (int k = 0; k < PM_BINS; ++k) c[k + 1] = c[k] + (1.0 - mix) * h[k] / tot + mix / PM_BINS;
+    for (int k = 1; k < PM_BINS; ++k) c[k] /= c[PM_BINS];
+    c[PM_BINS] = 1.0;
+  }
+  if ((e = cudaMemcpyAsync(f->pm, cdf.data(), cdf.size() * sizeof(double), cudaMemcpyHostToDevice, f->st)) ||
+      (e = cudaStreamSynchronize(f->st)))
+    return cuda_fail(e);
+  return PWA_OK;
+}
+
+// The pre-maps' nodes (host doubles [7][PWA_FLOW_PREMAP_NODES]).
+extern "C" int pwa_flow_get_premap(pwa_flow* f, double* h_cdf) {
+  if (!f || !h_cdf) return PWA_E_ARG;
+  cudaError_t e = cudaSetDevice(f->device);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h_cdf, f->pm, (size_t)FLOW_D * PM_NODES * sizeof(double), cudaMemcpyDeviceToHost, f->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->st);
+  return e == cudaSuccess ? PWA_OK : cuda_fail(e);
+}
+
+// Sets them (each row: 0 first, 1 last, strictly increasing; anything else is refused).
+extern "C" int pwa_flow_set_premap(pwa_flow* f, const double* h_cdf) {
+  if (!f || !h_cdf) return PWA_E_ARG;
+  for (int d = 0; d < FLOW_D; ++d) {
+    const double* c = h_cdf + (size_t)d * PM_NODES;
+    if (c[0] != 0.0 || c[PM_BINS] != 1.0) return PWA_E_ARG;
+    for (int k = 0; k < PM_BINS; ++k)
+      if (!(c[k + 1] > c[k])) return PWA_E_ARG;
+  }
+  cudaError_t e = cudaSetDevice(f->device);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(f->pm, h_cdf, (size_t)FLOW_D * PM_NODES * sizeof(double), cudaMemcpyHostToDevice, f->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(f->st);
   return e == cudaSuccess ? PWA_OK : cuda_fail(e);
 }

@@ -1,9 +1,12 @@
 // Epilogues of the proposal network's GEMMs and the network's element-wise kernels.
 //
-// The network is an autoregressive density over x in [0,1]^7 (MADE masks): input 2x - 1 padded to 64
+// The network is an autoregressive density over u in [0,1]^7 (MADE masks): input 2u - 1 padded to 64
 // columns, four hidden layers of 256 SiLU units, and 8 x 64 output logits (dimension d's 64 logits
-// give the bin probabilities of x_d given x_<d; the eighth block is padding).  q(x) =
-// prod_d 64 softmax(logits_d)[floor(64 x_d)], a piecewise-constant conditional per dimension.
+// give the bin probabilities of u_d given u_<d; the eighth block is padding).  q_u(u) =
+// prod_d 64 softmax(logits_d)[floor(64 u_d)], a piecewise-constant conditional per dimension.
+// Each coordinate first passes a fixed monotone pre-map u_d = F_d(x_d), a piecewise-linear CDF on
+// PM_BINS equal cells fitted to the target's marginal (identity until fitted), so that the 64 bins
+// are narrow where the marginal is peaked; q(x) = q_u(F(x)) prod_d F_d'(x_d).
 #pragma once
 #include <cuda_bf16.h>
 
@@ -19,6 +22,8 @@ constexpr int FLOW_H = 256;     // hidden width
 constexpr int FLOW_OUT = 512;   // 8 blocks of 64 logits (the last is padding)
 constexpr int FLOW_LAYERS = 5;  // 4 hidden + output
 constexpr float LOG_BINS = 4.1588830833596715f;  // log(64)
+constexpr int PM_BINS = 1024;   // cells of each coordinate's pre-map
+constexpr int PM_NODES = PM_BINS + 1;
 
 using bf16 = __nv_bfloat16;
 
@@ -45,6 +50,32 @@ __device__ __forceinline__ double hash_uniform(uint64_t key, uint64_t ctr) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   z ^= z >> 31;
   return ((z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// Pre-map of one coordinate: u = F(x) with F piecewise linear through cdf[k] at x = k / PM_BINS
+// (cdf[0] = 0, cdf[PM_BINS] = 1, strictly increasing); *logf = log F'(x).
+__device__ __forceinline__ double pm_forward(const double* __restrict__ cdf, double x, double* logf) {
+  double t = x * PM_BINS;
+  const int k = min(PM_BINS - 1, max(0, (int)floor(t)));
+  t -= k;
+  const double a = cdf[k], b = cdf[k + 1];
+  *logf = log((b - a) * PM_BINS);
+  return a + t * (b - a);
+}
+
+// Its inverse: x = F^-1(u) by bisection over the nodes; *logf = log F'(x).
+__device__ __forceinline__ double pm_inverse(const double* __restrict__ cdf, double u, double* logf) {
+  int lo = 0, hi = PM_BINS;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (cdf[mid] <= u)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const double a = cdf[lo], b = cdf[lo + 1];
+  *logf = log((b - a) * PM_BINS);
+  return (lo + (u - a) / (b - a)) * (1.0 / PM_BINS);
 }
 
 struct NoState {};
@@ -134,8 +165,8 @@ struct EpiOutput {
 };
 
 // Sampling pass of dimension d: bin from the conditional (inverse CDF on a counter-based uniform),
-// x_d uniform inside the bin; writes x_d (double [D][ldx]), the network input 2 x_d - 1 of later
-// passes, the bin, and adds log(64 p_bin) to logq.
+// u_d uniform inside the bin and x_d = F_d^-1(u_d); writes x_d (double [D][ldx]), the network input
+// 2 u_d - 1 of later passes, the bin, and adds log(64 p_bin) + log F_d'(x_d) to logq.
 struct EpiSample {
   static constexpr int CHUNK = 64;
   using State = NoState;
@@ -144,6 +175,7 @@ struct EpiSample {
   bf16* xin;      // [M][FLOW_IN]
   uint8_t* bins;  // [M][8]
   float* logq;
+  const double* pm;  // pre-maps [D][PM_NODES]
   uint64_t key;
   int64_t row0;   // global index of row 0 (counter base)
   int M, ldx, d;
@@ -173,11 +205,12 @@ struct EpiSample {
         break;
       }
     }
-    const double xd = (b + hash_uniform(key, ctr + 1)) / FLOW_BINS;
-    x[(size_t)d * ldx + row] = xd;
-    xin[(size_t)row * FLOW_IN + d] = __float2bfloat16((float)(2.0 * xd - 1.0));
+    const double ud = (b + hash_uniform(key, ctr + 1)) / FLOW_BINS;
+    double logf;
+    x[(size_t)d * ldx + row] = pm_inverse(pm + d * PM_NODES, ud, &logf);
+    xin[(size_t)row * FLOW_IN + d] = __float2bfloat16((float)(2.0 * ud - 1.0));
     bins[(size_t)row * 8 + d] = (uint8_t)b;
-    logq[row] += LOG_BINS + __logf(v[b] / s);
+    logq[row] += LOG_BINS + __logf(v[b] / s) + (float)logf;
   }
   __device__ void finish(State&, int) const {}
 };

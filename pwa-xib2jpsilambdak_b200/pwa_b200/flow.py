@@ -3,17 +3,22 @@
 The density q(x) lives on unit coordinates x in [0,1]^7 of the Lambda_b -> J/psi(-> mu mu) p K-
 phase space (`pwa_events_from_unit` turns x into an event):
 
-* x1, x2: the Dalitz point, m^2(Kp) linear in x1 over its range and m^2(J/psi p) linear in x2 over
-  its range at that m^2(Kp);
+* x1, x2: the Dalitz point, m^2(Kp) linear in x1 and m^2(J/psi p) linear in x2, each over its full
+  range (the rectangle around the Dalitz region, so that Lambda* bands lie at fixed x1 and Pc bands at
+  fixed x2; 30 % of the rectangle is outside the region and holds no event);
 * x3, x4, x5: the orientation of the decay in the Lambda_b rest frame (cos of the J/psi polar angle
   to the Lambda_b flight axis, its azimuth, the roll of the decay plane about the J/psi direction);
 * x6, x7: the mu+ direction in the J/psi rest frame (cos theta, phi).
 
-Flat phase space has the density `flat_density(x)` (the Dalitz-row length only).  The network is an
-autoregressive 4 x 256 SiLU MLP (MADE masks) giving, per dimension, 64 bin probabilities conditional
-on the earlier dimensions: q(x) = prod_d 64 p_d(bin(x_d) | x_<d), normalised and sampled exactly.  It
-is trained by weighted maximum likelihood on flat phase-space events weighted by |A|^2 (the target
-density is |A|^2 times flat phase space), with BF16 tcgen05 GEMMs and FP32 accumulation.
+Flat phase space has a constant density inside the Dalitz region and 0 outside (`events_from_unit`
+returns it).  Each coordinate first passes a fixed monotone pre-map u = F(x) fitted to the target's
+weighted marginal (`fit_premap`: a piecewise-linear CDF on 1024 cells with a uniform floor), which
+stretches the narrow resonance bands over many of the network's bins.  The network is an
+autoregressive 4 x 256 SiLU MLP (MADE masks) giving, per dimension, 64 bin probabilities of u_d
+conditional on the earlier dimensions: q(x) = prod_d 64 p_d(bin(u_d) | u_<d) F_d'(x_d), normalised
+and sampled exactly.  It is trained by weighted maximum likelihood on flat phase-space events
+weighted by |A|^2 (the target density is |A|^2 times flat phase space), with BF16 tcgen05 GEMMs and
+FP32 accumulation.
 
 Used (i) for toys: candidates drawn from q, each weighted by |A|^2 flat / q and accepted against the
 largest weight (hit-or-miss on the weights), and (ii) for normalisation integrals: the mean of
@@ -30,6 +35,7 @@ import numpy as np
 from . import lib
 
 D, BINS, IN, H, OUT = 7, 64, 64, 256, 512
+PREMAP_NODES = 1025
 LAYERS = [(H, IN), (H, H), (H, H), (H, H), (OUT, H)]  # (out, in)
 
 
@@ -72,6 +78,9 @@ def _bind(L):
     L.pwa_flow_sample.argtypes = [vp, i64, C.c_uint64, vp, i64, vp]
     L.pwa_flow_get_params.argtypes = [vp, fp]
     L.pwa_flow_set_params.argtypes = [vp, fp]
+    L.pwa_flow_fit_premap.argtypes = [vp, vp, i64, vp, i64, C.c_double]
+    L.pwa_flow_get_premap.argtypes = [vp, dp]
+    L.pwa_flow_set_premap.argtypes = [vp, dp]
     L.pwa_events_from_unit.argtypes = [vp, i64, i64, vp, vp, vp, i64, i64, C.c_float, C.c_int, vp, vp]
     L.pwa_unit_flat.argtypes = [i64, C.c_uint64, C.c_uint64, vp, i64, vp]
     L._flow_bound = True
@@ -124,6 +133,21 @@ class Flow:
     def set_params(self, params: list):
         p = np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in params]).astype(np.float32)
         lib.check(self.L.pwa_flow_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))), "pwa_flow_set_params")
+
+    def fit_premap(self, x, w, mix: float = 0.1):
+        """Fit the coordinates' pre-maps to the weighted marginals of events x [7, n] (weights w [n])."""
+        lib.check(self.L.pwa_flow_fit_premap(self.h, _ptr(x), x.stride(0), _ptr(w), x.shape[1], mix),
+                  "pwa_flow_fit_premap")
+
+    def premap(self) -> np.ndarray:
+        """The pre-maps' nodes [7, PREMAP_NODES] (F_d at x = k / (PREMAP_NODES - 1))."""
+        c = np.zeros((D, PREMAP_NODES), np.float64)
+        lib.check(self.L.pwa_flow_get_premap(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "pwa_flow_get_premap")
+        return c
+
+    def set_premap(self, cdf: np.ndarray):
+        c = np.ascontiguousarray(cdf, np.float64)
+        lib.check(self.L.pwa_flow_set_premap(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "pwa_flow_set_premap")
 
     def log_density(self, x):
         import torch
@@ -178,7 +202,8 @@ def flat_unit(n: int, seed: int, device: int = 0, first_id: int = 0):
 
 def events_from_unit(x, data: bool = False, weight: float = 1.0):
     """Device planes (pp, pp1, pp2 torch tensors, n_size) of the events at unit coordinates x, and the
-    flat phase-space density of x (torch float64 [n])."""
+    flat phase-space density of x (torch float64 [n]; 0 outside the Dalitz region, where the planes
+    hold a stand-in event whose amplitude the caller need not evaluate)."""
     import torch
     from . import basis as B
     L = _bind(lib.load())

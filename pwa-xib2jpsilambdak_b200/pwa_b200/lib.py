@@ -22,7 +22,8 @@ EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_c
             "pwa_host_lineshapes", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_events_from_unit",
             "pwa_unit_flat", "pwa_flow_create", "pwa_flow_destroy", "pwa_flow_param_count", "pwa_flow_get_params",
             "pwa_flow_set_params", "pwa_flow_train_step", "pwa_flow_gradients", "pwa_flow_log_density",
-            "pwa_flow_sample", "pwa_basis_from_angles", "pwa_angles_from_vectors",
+            "pwa_flow_sample", "pwa_flow_fit_premap", "pwa_flow_get_premap", "pwa_flow_set_premap",
+            "pwa_basis_from_angles", "pwa_angles_from_vectors",
             "pwa_error_string", "pwa_last_cuda_error"]
 
 _fp = C.POINTER(C.c_float)

@@ -33,6 +33,54 @@ def test_log_density_matches_float32_reference():
     f.close()
 
 
+def _random_premap(seed):
+    """Strictly increasing pre-map nodes with cells of widths varying over two decades."""
+    from pwa_b200 import flow
+    rng = np.random.default_rng(seed)
+    dens = np.exp(rng.normal(0, 1.2, (flow.D, flow.PREMAP_NODES - 1)))
+    cdf = np.concatenate([np.zeros((flow.D, 1)), np.cumsum(dens, axis=1)], axis=1)
+    cdf /= cdf[:, -1:]
+    cdf[:, -1] = 1.0
+    return cdf
+
+
+def test_log_density_with_premap_matches_reference():
+    import torch
+    f, params = _flow(seed=5)
+    cdf = _random_premap(6)
+    f.set_premap(cdf)
+    assert np.array_equal(f.premap(), cdf)
+    x = torch.rand((7, 1024), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+    lq = f.log_density(x).cpu().numpy()
+    ref, _ = R.log_q(params, x.cpu().numpy(), torch.float32, emulate_bf16=True, cdf=cdf)
+    d = np.abs(lq - ref.numpy())
+    assert np.median(d) < 1e-5 and np.max(d) < 1e-2, (np.median(d), np.max(d))
+    f.close()
+
+
+def test_premap_fit_follows_the_marginals():
+    """A weighted sample whose coordinate 0 piles up near 0.3: the fitted map's density there is the
+    weighted histogram's (mixed with the uniform floor)."""
+    import torch
+    from pwa_b200 import flow
+    f, _ = _flow()
+    g = torch.Generator("cuda").manual_seed(8)
+    x = torch.rand((7, 1 << 20), dtype=torch.float64, device="cuda", generator=g)
+    w = 1.0 + 50.0 * torch.exp(-0.5 * ((x[0] - 0.3) / 0.01) ** 2)
+    f.fit_premap(x, w, mix=0.1)
+    c = f.premap()
+    cells = flow.PREMAP_NODES - 1
+    h = np.histogram(x[0].cpu().numpy(), bins=cells, range=(0, 1), weights=w.cpu().numpy())[0]
+    want = 0.9 * h / h.sum() + 0.1 / cells
+    assert np.allclose(np.diff(c[0]), want, rtol=1e-9, atol=1e-15)
+    assert np.all(np.diff(c, axis=1) > 0) and np.all(c[:, 0] == 0) and np.all(c[:, -1] == 1)
+    bad = c.copy()
+    bad[3, 10] = bad[3, 9]
+    with pytest.raises(Exception):
+        f.set_premap(bad)
+    f.close()
+
+
 def test_gradients_match_cpu_float64():
     import torch
     f, params = _flow()
@@ -56,9 +104,12 @@ def test_gradients_match_cpu_float64():
     f.close()
 
 
-def test_sampling_matches_density_and_is_normalised():
+@pytest.mark.parametrize("premap", [False, True])
+def test_sampling_matches_density_and_is_normalised(premap):
     import torch
     f, _ = _flow(max_batch=16384, seed=4)
+    if premap:
+        f.set_premap(_random_premap(10))
     x, lq = f.sample(65536, seed=9)
     assert float(x.min()) >= 0.0 and float(x.max()) < 1.0
     lq2 = f.log_density(x)
@@ -89,6 +140,7 @@ def test_trained_proposal_is_unbiased_and_beats_hit_or_miss():
     xt = flow.flat_unit(1 << 21, seed=21)
     a2t, _ = _amp2_at(ctx, blk, xt)
     f = flow.Flow(0, max_batch=16384, seed=7)
+    f.fit_premap(xt, a2t)
     hist = f.train(xt, a2t, epochs=6, batch=16384, lr=3e-3)
     assert np.mean(hist[-20:]) < np.mean(hist[:20])
     # flat hit-or-miss vs the learned proposal on fresh events
@@ -96,13 +148,15 @@ def test_trained_proposal_is_unbiased_and_beats_hit_or_miss():
     a2f, _ = _amp2_at(ctx, blk, xf)
     xq, lq = f.sample(n, seed=23)
     a2q, flat = _amp2_at(ctx, blk, xq)
-    wq = a2q * flat / torch.exp(lq.double())
+    inside = flat > 0
+    wq = torch.where(inside, a2q * flat / torch.exp(lq.double()), torch.zeros_like(a2q))
     i_f, s_f = float(a2f.mean()), float(a2f.std()) / np.sqrt(n)
     i_q, s_q = float(wq.mean()), float(wq.std()) / np.sqrt(n)
     assert abs(i_q - i_f) < 5 * np.hypot(s_f, s_q), (i_f, s_f, i_q, s_q)
-    # amplitude evaluations per accepted toy event (hit-or-miss against the largest weight) and per
-    # effective event of a weighted sample
-    evals_flat, evals_q = float(a2f.max()) / i_f, float(wq.max()) / i_q
+    # amplitude evaluations per accepted toy event (hit-or-miss against the largest weight; candidates
+    # outside the Dalitz region cost no amplitude) and per effective event of a weighted sample
+    evals_flat = float(a2f.max()) / i_f
+    evals_q = float(inside.double().mean()) * float(wq.max()) / i_q
     ess_flat = i_f ** 2 / float((a2f ** 2).mean())
     ess_q = i_q ** 2 / float((wq ** 2).mean())
     assert ess_q > 2 * ess_flat and evals_q < evals_flat / 2, (evals_flat, evals_q, ess_flat, ess_q)
