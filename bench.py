@@ -310,9 +310,7 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
     # toys: candidates from q vs flat candidates
     xq, lq = f.sample(P["n_toy"], seed=502)
     a2q, flq = _amp2_unit(ctx, block, xq, P["chunk"])
-    inside = flq > 0  # candidates outside the Dalitz region: weight 0, no amplitude to evaluate
-    n_inside = int(inside.sum())
-    wq = torch.where(inside, a2q * flq / torch.exp(lq.double()), torch.zeros_like(a2q))
+    wq = a2q * flq / torch.exp(lq.double())
     xf = flow.flat_unit(P["n_toy"], seed=503, device=device)
     a2f, _ = _amp2_unit(ctx, block, xf, P["chunk"])
     g = torch.Generator(device=f"cuda:{device}").manual_seed(504)
@@ -322,11 +320,15 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
         return int((torch.rand(w.numel(), generator=g, device=w.device, dtype=torch.float64) * mx < w).sum())
 
     acc_q, acc_f = accepted(wq), accepted(a2f)
-    evals_q, evals_f = n_inside / max(acc_q, 1), P["n_toy"] / max(acc_f, 1)
-    # the same in expectation: (amplitude evaluations per candidate) x max weight / mean weight
-    exp_q = n_inside / P["n_toy"] * 1.05 * float(wq.max()) / float(wq.mean())
+    evals_q, evals_f = P["n_toy"] / max(acc_q, 1), P["n_toy"] / max(acc_f, 1)
+    # the same in expectation: 1.05 x max weight / mean weight
+    exp_q = 1.05 * float(wq.max()) / float(wq.mean())
     exp_f = 1.05 * float(a2f.max()) / float(a2f.mean())
-    q999 = float(torch.quantile(wq[inside][:1 << 24].float(), 0.999)) / float(wq.mean())
+    q999 = float(torch.quantile(wq[:1 << 24].float(), 0.999)) / float(wq.mean())
+    # weighted toys (every candidate kept with weight |A|^2 flat / q, the exact amplitude as judge): the
+    # amplitude evaluations per effective event, n / ESS = mean(w^2) / mean(w)^2, against the
+    # evaluations per accepted event of flat hit-or-miss at the same statistical power
+    per_eff_q = float((wq ** 2).mean()) / float(wq.mean()) ** 2
     # normalisation integral on the first n_norm events of each
     nn = P["n_norm"]
     wn, fn = wq[:nn], a2f[:nn]
@@ -344,10 +346,11 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
         "train_tflops": round(tflops, 2),
         "train_frac_of_bf16_peak": round(tflops / bf16_peak, 4),
         "premap": f"per-coordinate piecewise-linear CDF on 1024 cells, uniform floor {P['premap_mix']}",
-        "toy_candidates": P["n_toy"], "candidates_inside_dalitz": n_inside,
-        "accepted_flat": acc_f, "accepted_learned": acc_q,
+        "toy_candidates": P["n_toy"], "accepted_flat": acc_f, "accepted_learned": acc_q,
         "evals_per_accepted_expected_flat": round(exp_f, 3), "evals_per_accepted_expected_learned": round(exp_q, 3),
         "learned_weight_q999_over_mean": round(q999, 3),
+        "weighted_toys_evals_per_effective_event": round(per_eff_q, 3),
+        "weighted_toys_gain_vs_hit_or_miss": round(exp_f / per_eff_q, 3),
         "evals_per_accepted_flat": round(evals_f, 3), "evals_per_accepted_learned": round(evals_q, 3),
         "evals_per_accepted_gain": round(gain, 3), "target_gain": 10.0, "target_met": bool(gain >= 10.0),
         "norm_events": nn, "norm_integral_flat": i_f, "norm_integral_learned": i_q,

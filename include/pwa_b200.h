@@ -60,6 +60,9 @@ typedef struct {
 
 /* Context on CUDA device `device` (its own stream and buffers).  Replaces the file-scope state of
  * kernel_calEva.cu:76-80. */
+/* A context owns a blocking CUDA stream (pwa_ctx_stream): its work is ordered with the legacy default
+ * stream, so device inputs written there before a call are complete when the call reads them; inputs
+ * written on other streams must be complete before the call. */
 int pwa_ctx_create(int device, pwa_ctx** out);
 int pwa_ctx_destroy(pwa_ctx* ctx);
 
@@ -224,16 +227,15 @@ int pwa_angles_from_vectors(const double* d_vectors, int64_t n, double* d_angles
 /* ---- Learned proposal density (no counterpart in the reference, whose toys are flat hit-or-miss,
  * gen_toys/create_efficiency/hit_and_reject.py:40-50; the exact amplitude reweights every event).
  *
- * Unit coordinates x in [0,1]^7 of the phase space: x0, x1 the Dalitz point (m^2(Kp) linear in x0 and
- * m^2(J/psi p) linear in x1, each over its full range: the rectangle around the Dalitz region, 70 % of
- * which is inside), x2..x4 the decay's orientation in the Lambda_b rest frame (cos of the J/psi angle to
- * the flight axis, its azimuth, the roll of the decay plane), x5, x6 the mu+ direction in the J/psi
- * frame.  Arrays of x are device doubles [7][ldx] (coordinate-major). */
+ * Unit coordinates x in [0,1]^7 of the phase space: x0, x1 the Dalitz point (m^2(J/psi p) linear in x0
+ * over its range, then m^2(Kp) linear in x1 across the Dalitz row: Pc bands at fixed x0, the region's
+ * boundary at x1 = 0 and 1), x2..x4 the decay's orientation in the Lambda_b rest frame (cos of the
+ * J/psi angle to the flight axis, its azimuth, the roll of the decay plane), x5, x6 the mu+ direction in
+ * the J/psi frame.  Arrays of x are device doubles [7][ldx] (coordinate-major). */
 
 /* Events at unit coordinates into columns [col0, col0 + n) of device planes (reference layout, as
  * pwa_generate_events writes them; data != 0 writes the data weight sentinel, else weight w), and
- * (d_flat, optional) the flat phase-space density of each x: a constant inside the Dalitz region, 0
- * outside (where the column holds a valid stand-in event and the caller evaluates no amplitude). */
+ * (d_flat, optional) the flat phase-space density of each x. */
 int pwa_events_from_unit(const double* d_x, int64_t ldx, int64_t n, float* d_pp, float* d_pp1, float* d_pp2,
                          int64_t n_size, int64_t col0, float w, int data, double* d_flat, void* stream);
 /* n flat phase-space events in unit coordinates (counter-based: event i is a function of (seed, first_id + i)). */
@@ -243,6 +245,8 @@ int pwa_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* d_x, int6
  * q(x) = prod_d 64 p_d(bin(x_d) | x_<d).  Kernels: BF16 tcgen05 GEMMs with FP32 accumulation in TMEM,
  * fused epilogues; Adam on FP32 master weights.  max_batch: a multiple of 128 (rows per step / chunk). */
 typedef struct pwa_flow pwa_flow;
+/* Calls run on the handle's own blocking stream (ordered with the legacy default stream, as for a
+ * context) and return when their work is done. */
 int pwa_flow_create(int device, int max_batch, uint64_t seed, pwa_flow** out);
 int pwa_flow_destroy(pwa_flow* flow);
 /* Parameters (FP32, layer by layer: weights [out x in] row-major then biases; layers 256 x 64,

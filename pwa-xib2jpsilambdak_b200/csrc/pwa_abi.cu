@@ -261,7 +261,9 @@ int pwa_ctx_create(int device, pwa_ctx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = configure_kernels();
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  // a blocking stream: ordered with the legacy default stream, on which callers (torch by default)
+  // write the device events a context borrows and free the memory it reads
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamDefault);
   if (e == cudaSuccess) e = cudaEventCreate(&c->e0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->e1);
   if (e == cudaSuccess) e = cudaMalloc(&c->d_table, sizeof(PointTable));

@@ -325,7 +325,9 @@ extern "C" int pwa_flow_create(int device, int max_batch, uint64_t seed, pwa_flo
   f->device = device;
   f->max_batch = max_batch;
   cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->st, cudaStreamNonBlocking);
+  // a blocking stream: ordered with the legacy default stream, on which callers (torch by default)
+  // write the events and weights a call reads and free its inputs afterwards
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->st, cudaStreamDefault);
   const size_t B = (size_t)max_batch;
   auto fail = [&](cudaError_t err) {
     pwa_flow_destroy(f);

@@ -377,42 +377,33 @@ int init_tables() {
 
 // ------------------------------------------------------------------ unit coordinates
 // The phase space as a map from x in [0,1]^7 (the coordinates of the learned proposal density):
-// s1 = m^2(Kp) linear in x0 over [(m_p + m_K)^2, (m_Lb - m_J/psi)^2] and s2 = m^2(J/psi p) linear in x1
-// over [(m_J/psi + m_p)^2, (m_Lb - m_K)^2] (the rectangle around the Dalitz region, so that the
-// Lambda* bands lie at fixed x0 and the Pc bands at fixed x1; points outside the Dalitz region, 30 %
-// of the rectangle, are no event); the decay's orientation in the Lambda_b rest frame from the J/psi
+// s2 = m^2(J/psi p) linear in x0 over [(m_J/psi + m_p)^2, (m_Lb - m_K)^2] (so that the Pc bands lie at
+// fixed x0) and s1 = m^2(Kp) linear in x1 across the Dalitz row at that s2 (so that the region's
+// boundary is x1 = 0 and x1 = 1); the decay's orientation in the Lambda_b rest frame from the J/psi
 // direction (cos theta = 2 x2 - 1 to the flight axis, azimuth 2 pi x3) and the roll 2 pi x4 of the
 // decay plane about it (together a uniform rotation); the mu+ direction in the J/psi rest frame
 // (cos = 2 x5 - 1, phi = 2 pi x6 - pi), as the flat generator above draws it.  Flat phase space has
-// the density (s1 range) (s2 range) / (Dalitz area) inside the Dalitz region and 0 outside.
-__host__ __device__ inline void dalitz_row(double s1, double& lo, double& hi) {
-  const double M = M_LB, m1 = sqrt(s1);
-  const double ep = (s1 - M_K * M_K + M_P * M_P) / (2 * m1);
-  const double epsi = (M * M - s1 - M_JPSI * M_JPSI) / (2 * m1);
-  const double qp = sqrt(fmax(ep * ep - M_P * M_P, 0.0)), qpsi = sqrt(fmax(epsi * epsi - M_JPSI * M_JPSI, 0.0));
-  lo = sq(ep + epsi) - sq(qp + qpsi);
-  hi = sq(ep + epsi) - sq(qp - qpsi);
+// density (s2 range) (row length at s2) / (Dalitz area) in these coordinates.
+//
+// Range of s1 = m^2(Kp) at s2 = m^2(J/psi p): the p and K- energies and momenta in the J/psi p rest
+// frame give the extremes (E_p + E_K)^2 - (q_p -+ q_K)^2.
+__host__ __device__ inline void dalitz_row(double s2, double& lo, double& hi) {
+  const double M = M_LB, m2 = sqrt(s2);
+  const double ep = (s2 - M_JPSI * M_JPSI + M_P * M_P) / (2 * m2);
+  const double ek = (M * M - s2 - M_K * M_K) / (2 * m2);
+  const double qp = sqrt(fmax(ep * ep - M_P * M_P, 0.0)), qk = sqrt(fmax(ek * ek - M_K * M_K, 0.0));
+  lo = sq(ep + ek) - sq(qp + qk);
+  hi = sq(ep + ek) - sq(qp - qk);
 }
-constexpr double S1_LO = (M_P + M_K) * (M_P + M_K), S1_HI = (M_LB - M_JPSI) * (M_LB - M_JPSI);
 constexpr double S2_LO = (M_JPSI + M_P) * (M_JPSI + M_P), S2_HI = (M_LB - M_K) * (M_LB - M_K);
 
-__host__ __device__ inline bool dalitz_inside(double x0, double x1) {
-  double lo, hi;
-  dalitz_row(S1_LO + (S1_HI - S1_LO) * x0, lo, hi);
-  const double s2 = S2_LO + (S2_HI - S2_LO) * x1;
-  return s2 >= lo && s2 <= hi && hi > lo;
-}
-
-// The event at x; false (and the event at the row's middle) where (x0, x1) lies outside the Dalitz
-// region.
-__device__ bool event_from_unit(const double* x, V4& p, V4& k, V4& mup, V4& mum) {
+__device__ void event_from_unit(const double* x, V4& p, V4& k, V4& mup, V4& mum, double& row_len) {
   const double M = M_LB;
-  const double s1 = S1_LO + (S1_HI - S1_LO) * x[0];
+  const double s2 = S2_LO + (S2_HI - S2_LO) * x[0];
   double lo, hi;
-  dalitz_row(s1, lo, hi);
-  double s2 = S2_LO + (S2_HI - S2_LO) * x[1];
-  const bool inside = s2 >= lo && s2 <= hi && hi > lo;
-  if (!inside) s2 = 0.5 * (lo + hi);
+  dalitz_row(s2, lo, hi);
+  row_len = hi - lo;
+  const double s1 = lo + (hi - lo) * x[1];
   const double s3 = M * M + M_JPSI * M_JPSI + M_P * M_P + M_K * M_K - s1 - s2;
   const double Epsi = (M * M + M_JPSI * M_JPSI - s1) / (2 * M);
   const double Ek = (M * M + M_K * M_K - s2) / (2 * M);
@@ -442,7 +433,6 @@ __device__ bool event_from_unit(const double* x, V4& p, V4& k, V4& mup, V4& mum)
   const V3 bpsi = (1.0 / psi.e) * psi.p;
   mup = boost(V4{mu3, emu}, bpsi);
   mum = boost(V4{-mu3, emu}, bpsi);
-  return inside;
 }
 
 __global__ void k_events_from_unit(const double* __restrict__ x, int64_t ldx, int64_t n, float* pp, float* pp1,
@@ -453,41 +443,46 @@ __global__ void k_events_from_unit(const double* __restrict__ x, int64_t ldx, in
   double u[7];
   for (int d = 0; d < 7; ++d) u[d] = x[d * ldx + t];
   V4 p, k, mup, mum;
-  const bool inside = event_from_unit(u, p, k, mup, mum);
+  double row_len;
+  event_from_unit(u, p, k, mup, mum, row_len);
   write_basis(helicity_angles(p, k, mup, mum), pp, pp1, pp2, ns, col0 + t, data ? -1001.f : w);
-  if (flat) flat[t] = inside ? norm : 0.0;
+  if (flat) flat[t] = row_len * norm;
 }
 
-// Flat phase space in unit coordinates: (x0, x1) uniform in the rectangle by rejection against the
-// Dalitz region (acceptance 0.70), the other coordinates uniform.
-__global__ void k_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* x, int64_t ldx) {
+// Flat phase space in unit coordinates: x0 by rejection against the Dalitz row length (max_len
+// bounds it), the other coordinates uniform.
+__global__ void k_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* x, int64_t ldx, double max_len) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   Rng R;
   R.id = first_id + (uint64_t)t;
   R.k0 = (uint32_t)seed ^ 0x75u;
   R.k1 = (uint32_t)(seed >> 32);
-  double x0 = R.uni(), x1 = R.uni();
-  for (int it = 0; it < 1000 && !dalitz_inside(x0, x1); ++it) {  // 1000 tries never run out in practice
+  double x0 = R.uni();
+  for (int it = 0; it < 1000; ++it) {  // acceptance is above one half: 1000 tries never run out in practice
+    double lo, hi;
+    dalitz_row(S2_LO + (S2_HI - S2_LO) * x0, lo, hi);
+    if (R.uni() * max_len < hi - lo) break;
     x0 = R.uni();
-    x1 = R.uni();
   }
   x[t] = x0;
-  x[ldx + t] = x1;
-  for (int d = 2; d < 7; ++d) x[d * ldx + t] = R.uni();
+  for (int d = 1; d < 7; ++d) x[d * ldx + t] = R.uni();
 }
 
-// Dalitz area in (s1, s2) (Simpson's rule on the row length).
-static double dalitz_area() {
+// Dalitz area in (s1, s2) (Simpson's rule on the row length over s2) and the largest row length.
+static void dalitz_area(double* area, double* max_len) {
   const int n = 20000;
-  const double h = (S1_HI - S1_LO) / n;
-  double a = 0;
+  const double h = (S2_HI - S2_LO) / n;
+  double a = 0, mx = 0;
   for (int i = 0; i <= n; ++i) {
     double lo, hi;
-    dalitz_row(S1_LO + i * h, lo, hi);
-    a += (hi - lo) * ((i == 0 || i == n) ? 1 : (i % 2 ? 4 : 2));
+    dalitz_row(S2_LO + i * h, lo, hi);
+    const double len = hi - lo;
+    a += len * ((i == 0 || i == n) ? 1 : (i % 2 ? 4 : 2));
+    mx = fmax(mx, len);
   }
-  return a * h / 3;
+  *area = a * h / 3;
+  *max_len = mx * 1.001;
 }
 
 }  // namespace gen
@@ -537,19 +532,21 @@ int pwa_events_from_unit(const double* d_x, int64_t ldx, int64_t n, float* d_pp,
   if (!d_x || !d_pp || !d_pp1 || !d_pp2 || n < 0 || ldx < n || col0 < 0 || col0 + n > n_size) return PWA_E_ARG;
   if (n == 0) return PWA_OK;
   if (pwa::gen::init_tables()) return PWA_E_CUDA;
-  const double area = pwa::gen::dalitz_area();
+  double area, max_len;
+  pwa::gen::dalitz_area(&area, &max_len);
   cudaStream_t st = (cudaStream_t)stream;
   pwa::gen::k_events_from_unit<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
-      d_x, ldx, n, d_pp, d_pp1, d_pp2, n_size, col0, w, data, d_flat,
-      (pwa::gen::S1_HI - pwa::gen::S1_LO) * (pwa::gen::S2_HI - pwa::gen::S2_LO) / area);
+      d_x, ldx, n, d_pp, d_pp1, d_pp2, n_size, col0, w, data, d_flat, (pwa::gen::S2_HI - pwa::gen::S2_LO) / area);
   return cudaStreamSynchronize(st) == cudaSuccess ? PWA_OK : PWA_E_CUDA;
 }
 
 int pwa_unit_flat(int64_t n, uint64_t seed, uint64_t first_id, double* d_x, int64_t ldx, void* stream) {
   if (!d_x || n < 0 || ldx < n) return PWA_E_ARG;
   if (n == 0) return PWA_OK;
+  double area, max_len;
+  pwa::gen::dalitz_area(&area, &max_len);
   cudaStream_t st = (cudaStream_t)stream;
-  pwa::gen::k_unit_flat<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, seed, first_id, d_x, ldx);
+  pwa::gen::k_unit_flat<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, seed, first_id, d_x, ldx, max_len);
   return cudaStreamSynchronize(st) == cudaSuccess ? PWA_OK : PWA_E_CUDA;
 }
 }

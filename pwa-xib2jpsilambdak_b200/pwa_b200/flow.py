@@ -3,15 +3,14 @@
 The density q(x) lives on unit coordinates x in [0,1]^7 of the Lambda_b -> J/psi(-> mu mu) p K-
 phase space (`pwa_events_from_unit` turns x into an event):
 
-* x1, x2: the Dalitz point, m^2(Kp) linear in x1 and m^2(J/psi p) linear in x2, each over its full
-  range (the rectangle around the Dalitz region, so that Lambda* bands lie at fixed x1 and Pc bands at
-  fixed x2; 30 % of the rectangle is outside the region and holds no event);
+* x1, x2: the Dalitz point, m^2(J/psi p) linear in x1 over its range (the narrow Pc bands lie at
+  fixed x1) and m^2(Kp) linear in x2 across the Dalitz row at that m^2(J/psi p) (the region's
+  boundary lies at x2 = 0 and 1, so no bin of the network straddles it);
 * x3, x4, x5: the orientation of the decay in the Lambda_b rest frame (cos of the J/psi polar angle
   to the Lambda_b flight axis, its azimuth, the roll of the decay plane about the J/psi direction);
 * x6, x7: the mu+ direction in the J/psi rest frame (cos theta, phi).
 
-Flat phase space has a constant density inside the Dalitz region and 0 outside (`events_from_unit`
-returns it).  Each coordinate first passes a fixed monotone pre-map u = F(x) fitted to the target's
+Flat phase space has the density `events_from_unit` returns (the Dalitz-row length only).  Each coordinate first passes a fixed monotone pre-map u = F(x) fitted to the target's
 weighted marginal (`fit_premap`: a piecewise-linear CDF on 1024 cells with a uniform floor), which
 stretches the narrow resonance bands over many of the network's bins.  The network is an
 autoregressive 4 x 256 SiLU MLP (MADE masks) giving, per dimension, 64 bin probabilities of u_d
@@ -202,8 +201,7 @@ def flat_unit(n: int, seed: int, device: int = 0, first_id: int = 0):
 
 def events_from_unit(x, data: bool = False, weight: float = 1.0):
     """Device planes (pp, pp1, pp2 torch tensors, n_size) of the events at unit coordinates x, and the
-    flat phase-space density of x (torch float64 [n]; 0 outside the Dalitz region, where the planes
-    hold a stand-in event whose amplitude the caller need not evaluate)."""
+    flat phase-space density of x (torch float64 [n])."""
     import torch
     from . import basis as B
     L = _bind(lib.load())
