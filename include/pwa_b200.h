@@ -276,6 +276,50 @@ int pwa_flow_fit_premap(pwa_flow* flow, const double* d_x, int64_t ldx, const do
 int pwa_flow_get_premap(pwa_flow* flow, double* h_cdf);
 int pwa_flow_set_premap(pwa_flow* flow, const double* h_cdf);
 
+/* ---- Toy ensembles fitted together (no counterpart in the reference, which builds one PDF per toy and
+ * integrates the MC anew at every call: src/RooDalitzAmplitude.cxx:1293-1628, gen_toys/).
+ *
+ * For fits that float the helicity couplings with the lineshape parameters held where the ensemble is
+ * set up.  |A|^2 of an event is then a Hermitian form in the coupling "slots": c_{r,k,m} of Lambda* r
+ * (slot k NS + 6 r + m) and c_{q,k,m} of the Pc entry at group-order position q (slot k NS + 6 NR +
+ * 12 q + m), NS = 6 NR + 12 NZ, proton helicity k, helicity index m as in the parameter block.  The MC
+ * normalisation of any toy is c^H M c (M: FP64 Gram matrix over the shared MC, built at creation), and
+ * one call evaluates every toy's data term over its own window with its gradient.
+ *
+ * create: over the context's events (borrowed: keep them uploaded, unchanged), the lineshape part of the
+ * model from the block (its couplings are not used), toy t = data events [first[t], first[t] + count[t])
+ * with the band arguments nda_smr[t], nda_fine[t] that pwa_ctx_select_data takes for it, sum_w_data[t]
+ * its data weight sum and sum_w_mc that of the MC; active (optional, one byte per slot): slots that can
+ * be non-zero in the fit (the Gram matrix is accumulated for those only; null: all).  Models with Zcs
+ * entries: PWA_E_UNSUPPORTED.  Memory: (2 NR + 2 NZ + NZ (NZ + 1)) doubles per data event. */
+typedef struct pwa_ens pwa_ens;
+int pwa_ens_create(pwa_ctx* ctx, const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR,
+                   int NZ, int NX, float FFR, float FFB, int n_toys, const int64_t* first, const int64_t* count,
+                   const int64_t* nda_smr, const int64_t* nda_fine, const double* sum_w_data, double sum_w_mc,
+                   const uint8_t* active, pwa_ens** out);
+int pwa_ens_destroy(pwa_ens* ens);
+/* Number of slots (2 NS). */
+int pwa_ens_slot_count(const pwa_ens* ens);
+/* The slot values (Re, Im doubles, 2 (6 NR + 12 NZ) slots) of a parameter block. */
+int pwa_ens_slots(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                  float FFR, float FFB, double* h_slots);
+/* The Gram matrices M and Mn (non-interference sum), row-major slot x slot complex (Re, Im doubles). */
+int pwa_ens_gram(const pwa_ens* ens, double* h_M, double* h_Mn);
+/* Launch shape of the per-call kernel: warps per block (4 or 8) and events per work item; the
+ * project's autotuner (pwa_b200.ensemble.autotune) picks them by timing. */
+int pwa_ens_set_launch(pwa_ens* ens, int warps, int tile_events);
+/* One evaluation of every toy t with on[t] != 0 (on null: all) at its slot vector h_slots[t] ([n_toys]
+ * [slots] x (Re, Im)), as one CUDA-graph launch (captured at the first call and after a launch-shape or
+ * nll_shift change): h_out[4 t ..] = NLL (nll_shift + W_t ln(I / W_mc) - D_t, +1000 under the reference's
+ * non-interference guard), D_t = sum sw ln|A|^2 over its data, I = c^H M c, In = c^H Mn c;
+ * h_grad[t] (optional) = dNLL / d conj(c), slot-wise (Re, Im); h_bad[t] (optional): data events with
+ * |A|^2 <= 0 or not finite.  Rows of toys that are off are left as they were. */
+int pwa_ens_eval(pwa_ens* ens, const double* h_slots, const int* h_on, double nll_shift, double* h_out,
+                 double* h_grad, int64_t* h_bad);
+/* Device time of the last pwa_ens_eval (ms) and of the set-up passes (factor rows, Gram matrices). */
+double pwa_ens_last_ms(const pwa_ens* ens);
+int pwa_ens_setup_ms(const pwa_ens* ens, double* factors_ms, double* gram_ms);
+
 /* Allocation-free likelihood evaluation.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory while they evaluate the likelihood -- for

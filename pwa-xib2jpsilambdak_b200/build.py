@@ -12,6 +12,7 @@ OUT = HERE / "pwa_b200" / "libpwa_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["pwa_kernels.cu", "pwa_batch.cu", "pwa_batch_s20.cu", "pwa_batch_s30.cu", "pwa_batch_s150.cu",
            "pwa_batch_grid.cu", "pwa_abi.cu", "pwa_generate.cu", "pwa_noalloc.cu", "pwa_lineshape_diag.cu", "pwa_flow.cu",
+           "pwa_ensemble.cu",
            "kernel_calEva_compat.cpp"]
 
 

@@ -227,6 +227,17 @@ int build_reference_segments(pwa_ctx* c, const float* h_mz) {
   return PWA_OK;
 }
 
+}  // namespace
+
+int pwa::ctx_view(const pwa_ctx* c, CtxView* v) {
+  if (!c || !v) return PWA_E_ARG;
+  *v = CtxView{c->device, c->sm_count, c->st, c->pp, c->pp1, c->pp2, c->sw, c->pp3, c->pp4, c->n, c->n_size,
+               c->nda, c->smear_mode == PWA_SMEAR_GAUSS ? 1 : 0, c->d_grid, c->grid_nb, c->use_tables};
+  return c->pp ? PWA_OK : PWA_E_STATE;
+}
+
+namespace {
+
 int check_events(int64_t n, int64_t n_size, int64_t nda) {
   if (n < 0 || nda < 0 || nda > n || n_size < n || n > INT32_MAX) return PWA_E_ARG;
   return PWA_OK;

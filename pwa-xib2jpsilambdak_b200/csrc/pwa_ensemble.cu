@@ -237,9 +237,9 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_ens_gram(const PointTable* __r
     acc[j] = mk(0, 0);
   }
   const int64_t per = (count + gridDim.x - 1) / gridDim.x;
-  const int64_t i_begin = (int64_t)blockIdx.x * per, i_end = min(count, i_begin + per);
+  const int64_t i_begin = (int64_t)blockIdx.x * per, i_end = count < i_begin + per ? count : i_begin + per;
   for (int64_t i0 = i_begin; i0 < i_end; i0 += GRAM_EB) {
-    const int ne = (int)min<int64_t>(GRAM_EB, i_end - i0);
+    const int ne = (int)(i_end - i0 < GRAM_EB ? i_end - i0 : GRAM_EB);
     __syncthreads();
     gram_stage(T, ev, chunk_begin, i0, ne, fac, ld, buf, bsize);
     __syncthreads();
@@ -264,3 +264,738 @@ __global__ void k_ens_sum_rows(const cplx* __restrict__ part, int rows, int n, c
   for (int r = 0; r < rows; ++r) s += part[(size_t)r * n + j];
   out[j] += s;
 }
+
+// ------------------------------------------------------------------ data terms of all toys
+constexpr int ENS_MAX_SLOTS = 2 * (6 * MAX_LSTAR + 12 * MAX_PC);
+constexpr int ENS_SPL = (ENS_MAX_SLOTS + 31) / 32;  // slots per lane
+
+// A work item: events [e0, e1) of toy t.
+struct Tile {
+  int64_t e0, e1;
+  int t, pad;
+};
+
+// Per-warp scratch of the data kernel.
+struct EnsWarp {
+  double pl[SLOT_ALL];                                   // the event's plane slots
+  double fac[2 * MAX_LSTAR + 2 * MAX_PC + MAX_PC * (MAX_PC + 1)];  // its factor row
+  cplx hz[MAX_PC][8];  // HZ_q[h]
+  cplx z[MAX_PC][8];   // d v / d conj(HZ_q[h])
+  cplx x[8];           // d v / d conj(H_L[h])
+  cplx yl[12];         // sum_ij conj(A_ijm) x[k, ij]
+  cplx yz[2 * MAX_PC * 12];
+};
+
+template <int WARPS>
+constexpr size_t ens_data_smem() {
+  return ((sizeof(PointTable) + 15) & ~size_t(15)) + (size_t)ENS_MAX_SLOTS * sizeof(cplx) + WARPS * sizeof(EnsWarp);
+}
+
+// Persistent blocks take tiles from *next; per tile the block loads the toy's slot couplings and each
+// warp evaluates one event at a time.  Per toy: val[t] += sum sw ln v (-1e12 for v <= 0, as the
+// reference), bad[t] counts events with v <= 0 or not finite, grad[t][s] += sum (sw / v) dv/dconj(c_s).
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __restrict__ gtab, EventSet ev,
+                                                         const double* __restrict__ fac, int64_t ld,
+                                                         const Tile* __restrict__ tiles, int n_tiles, int* next,
+                                                         const cplx* __restrict__ coup, const int* __restrict__ on,
+                                                         int n_slot, double* val, cplx* grad,
+                                                         unsigned long long* bad) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  PointTable& T = *reinterpret_cast<PointTable*>(sm);
+  load_table<WARPS * 32>(gtab, &T);
+  cplx* c = reinterpret_cast<cplx*>(sm + ((sizeof(PointTable) + 15) & ~size_t(15)));
+  EnsWarp& W = reinterpret_cast<EnsWarp*>(c + ENS_MAX_SLOTS)[threadIdx.x / 32];
+  __shared__ int tile_id;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
+  const int h = lane & 7, part = lane >> 3;
+  const int hi = h >> 2, hj = (h >> 1) & 1, hk = h & 1;
+  const int NR = T.NR, NZ = T.NZ, NS = 6 * NR + 12 * NZ;
+  const FactorLayout F{NR, NZ};
+  const int nf = F.size(false);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) tile_id = atomicAdd(next, 1);
+    __syncthreads();
+    const int ti = tile_id;
+    if (ti >= n_tiles) break;
+    const Tile tl = tiles[ti];
+    if (!on[tl.t]) continue;
+    for (int s = threadIdx.x; s < n_slot; s += WARPS * 32) c[s] = coup[(size_t)tl.t * n_slot + s];
+    __syncthreads();
+    cplx acc[ENS_SPL];
+#pragma unroll
+    for (int j = 0; j < ENS_SPL; ++j) acc[j] = mk(0, 0);
+    double value = 0;
+    unsigned long long nbad = 0;
+    for (int64_t e = tl.e0 + warp; e < tl.e1; e += WARPS) {
+      stage_event(T, ev, e, W.pl, lane);
+      for (int f = lane; f < nf; f += 32) W.fac[f] = fac[(size_t)f * ld + e];
+      __syncwarp();
+      const EvS E{W.pl};
+      // H_L[h]: lane (h, part) sums the Lambda* r = part mod 4
+      cplx hl = mk(0, 0);
+      for (int r = part; r < NR; r += 4) {
+        const int sidx = T.L[r].sidx;
+        const cplx* cr = c + hk * NS + r * 6;
+        cplx f = mk(0, 0);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) cmac(f, cr[m], E.A(hi, hj, m) * E.DL(sidx, hk, m));
+        cmac(hl, mk(W.fac[F.l() + 2 * r], W.fac[F.l() + 2 * r + 1]), f);
+      }
+      hl += shfl_xor(hl, 8);
+      hl += shfl_xor(hl, 16);
+      for (int q = part; q < NZ; q += 4) {
+        const int sidx = T.Z[T.order[q]].sidx;
+        const cplx* cq = c + hk * NS + 6 * NR + q * 12;
+        cplx f = mk(0, 0);
+#pragma unroll
+        for (int m = 0; m < 12; ++m) cmac(f, cq[m], E.AZ(hi, hj, m) * E.DZ(sidx, hk, m));
+        W.hz[q][h] = f;
+      }
+      __syncwarp();
+      double vp = 0;
+      if (part == 0) {
+        cplx sx = mk(0, 0);
+        for (int q = 0; q < NZ; ++q) cmac(sx, mk(W.fac[F.s1() + 2 * q], W.fac[F.s1() + 2 * q + 1]), W.hz[q][h]);
+        vp = norm2(hl) + 2.0 * (hl.re * sx.re + hl.im * sx.im);
+        W.x[h] = hl + sx;
+      }
+      for (int q = part; q < NZ; q += 4) {
+        cplx tq = mk(0, 0);
+        for (int p = 0; p < NZ; ++p) {
+          const int o = F.s2() + 2 * (q <= p ? tri(q, p, NZ) : tri(p, q, NZ));
+          const cplx s2 = q <= p ? mk(W.fac[o], W.fac[o + 1]) : mk(W.fac[o], -W.fac[o + 1]);
+          cmac(tq, s2, W.hz[p][h]);
+        }
+        const cplx hz = W.hz[q][h];
+        vp += hz.re * tq.re + hz.im * tq.im;
+        W.z[q][h] = conj(mk(W.fac[F.s1() + 2 * q], W.fac[F.s1() + 2 * q + 1])) * hl + tq;
+      }
+      const double v = warp_sum(vp);
+      __syncwarp();
+      for (int t = lane; t < 12 + 24 * NZ; t += 32) {
+        cplx y = mk(0, 0);
+        if (t < 12) {
+          const int k = t / 6, m = t % 6;
+#pragma unroll
+          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.A(ij >> 1, ij & 1, m)), W.x[(ij << 1) | k]);
+          W.yl[t] = y;
+        } else {
+          const int u = t - 12, k = u / (12 * NZ), q = (u / 12) % NZ, m = u % 12;
+#pragma unroll
+          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.AZ(ij >> 1, ij & 1, m)), W.z[q][(ij << 1) | k]);
+          W.yz[u] = y;
+        }
+      }
+      __syncwarp();
+      const double sw = (double)__ldg(ev.sw + e);
+      const bool good = v > 0 && isfinite(v);
+      const double scale = good ? sw / v : 0.0;
+#pragma unroll
+      for (int j = 0; j < ENS_SPL; ++j) {
+        const int s = lane + 32 * j;
+        if (s >= n_slot) break;
+        const int k = s / NS, u = s % NS;
+        cplx g;
+        if (u < 6 * NR) {
+          const int r = u / 6, m = u % 6;
+          const cplx L = mk(W.fac[F.l() + 2 * r], W.fac[F.l() + 2 * r + 1]);
+          g = conj(L * E.DL(T.L[r].sidx, k, m)) * W.yl[k * 6 + m];
+        } else {
+          const int q = (u - 6 * NR) / 12, m = (u - 6 * NR) % 12;
+          g = W.yz[(k * NZ + q) * 12 + m] * E.DZ(T.Z[T.order[q]].sidx, k, m);
+        }
+        cmac(acc[j], mk(scale, 0), g);
+      }
+      if (lane == 0) {
+        value += v > 0 ? log(v) * sw : -1e12;
+        nbad += good ? 0 : 1;
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int j = 0; j < ENS_SPL; ++j) {
+      const int s = lane + 32 * j;
+      if (s >= n_slot) break;
+      atomicAdd(&grad[(size_t)tl.t * n_slot + s].re, acc[j].re);
+      atomicAdd(&grad[(size_t)tl.t * n_slot + s].im, acc[j].im);
+    }
+    if (lane == 0) {
+      atomicAdd(val + tl.t, value);
+      if (nbad) atomicAdd(bad + tl.t, nbad);
+    }
+  }
+}
+
+// Per toy (one block each): I = c^H M c, In = c^H Mn c, and the NLL with its gradient in the slots,
+//   nll = shift + W_t ln(I / W_mc) - D_t (+1000 when |In / I - 1| > 0.3, as the reference's guard),
+//   d nll / d conj(c) = W_t (M c) / I - sum (sw / v) dv / dconj(c).
+// out[t]: nll, D_t, I, In; gout[t][s] (optional): the gradient.
+__global__ void k_ens_finish(int n_slot, const cplx* __restrict__ M, const cplx* __restrict__ Mn,
+                             const cplx* __restrict__ coup, const int* __restrict__ on, const double* __restrict__ val,
+                             const cplx* __restrict__ grad, const double* __restrict__ wdata, double w_mc,
+                             double shift, double* out, cplx* gout) {
+  const int t = blockIdx.x;
+  if (!on[t]) return;
+  const cplx* c = coup + (size_t)t * n_slot;
+  __shared__ double red[2][32];
+  double I = 0, In = 0;
+  for (int a = threadIdx.x; a < n_slot; a += blockDim.x) {
+    cplx mc = mk(0, 0), mnc = mk(0, 0);
+    for (int b = 0; b < n_slot; ++b) {
+      cmac(mc, M[(size_t)a * n_slot + b], c[b]);
+      cmac(mnc, Mn[(size_t)a * n_slot + b], c[b]);
+    }
+    I += c[a].re * mc.re + c[a].im * mc.im;
+    In += c[a].re * mnc.re + c[a].im * mnc.im;
+    if (gout) gout[(size_t)t * n_slot + a] = mc;  // M c for now
+  }
+  I = warp_sum(I);
+  In = warp_sum(In);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x / 32] = I;
+    red[1][threadIdx.x / 32] = In;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x / 32;
+    I = threadIdx.x < nw ? red[0][threadIdx.x] : 0.0;
+    In = threadIdx.x < nw ? red[1][threadIdx.x] : 0.0;
+    I = warp_sum(I);
+    In = warp_sum(In);
+    if (threadIdx.x == 0) {
+      red[0][0] = I;
+      red[1][0] = In;
+    }
+  }
+  __syncthreads();
+  I = red[0][0];
+  In = red[1][0];
+  const double W = wdata[t];
+  if (gout) {
+    for (int a = threadIdx.x; a < n_slot; a += blockDim.x) {
+      const size_t o = (size_t)t * n_slot + a;
+      gout[o] = gout[o] * (W / I) - grad[o];
+    }
+  }
+  if (threadIdx.x == 0) {
+    double nll = shift + W * log(I / w_mc) - val[t];
+    if (fabs(In / I - 1.0) > (double)0.3f) nll += 1000.0;
+    out[4 * t] = nll;
+    out[4 * t + 1] = val[t];
+    out[4 * t + 2] = I;
+    out[4 * t + 3] = In;
+  }
+}
+
+}  // namespace ens
+}  // namespace pwa
+
+// ------------------------------------------------------------------ host side
+using namespace pwa;
+using namespace pwa::ens;
+
+struct pwa_ens {
+  CtxView cv;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  PointTable* h_T = nullptr;
+  PointTable* d_T = nullptr;
+  void* d_tab = nullptr;
+  int NR = 0, NZ = 0, NS = 0, n_slot = 0;
+  int n_toys = 0;
+  std::vector<int64_t> first, count;
+  std::vector<double> wdata;
+  double w_mc = 0;
+  uint8_t* d_kind = nullptr;
+  double* d_fac = nullptr;  // factor rows of the data events, [F][nda]
+  int64_t ld = 0;
+  std::vector<cplx> M, Mn;  // Gram matrices (host copies)
+  cplx *d_M = nullptr, *d_Mn = nullptr;
+  // launch shape and work list
+  int warps = 8, tile_events = 1024, blocks = 0;
+  Tile* d_tiles = nullptr;
+  int n_tiles = 0;
+  // per-call buffers: device and pinned host mirrors
+  cplx *d_coup = nullptr, *d_grad = nullptr, *d_gout = nullptr;
+  int* d_on = nullptr;
+  int* d_next = nullptr;
+  double *d_val = nullptr, *d_wdata = nullptr, *d_out = nullptr;
+  unsigned long long* d_bad = nullptr;
+  cplx *h_coup = nullptr, *h_gout = nullptr;
+  int* h_on = nullptr;
+  double* h_out = nullptr;
+  unsigned long long* h_bad = nullptr;
+  double* d_shift = nullptr;
+  double shift = 0;
+  cudaGraphExec_t graph = nullptr;
+  double last_ms = 0, factors_ms = 0, gram_ms = 0;
+  std::vector<void*> owned;
+};
+
+namespace {
+
+int ens_fail(pwa_ens* s, cudaError_t e);
+
+template <class T>
+cudaError_t ens_alloc(pwa_ens* s, T** p, size_t count) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
+  if (e == cudaSuccess) s->owned.push_back(*p);
+  return e;
+}
+
+void ens_free(pwa_ens* s) {
+  if (!s) return;
+  cudaSetDevice(s->cv.device);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (void* p : s->owned) cudaFree(p);
+  cudaFree(s->d_tiles);
+  cudaFreeHost(s->h_T);
+  cudaFreeHost(s->h_coup);
+  cudaFreeHost(s->h_gout);
+  cudaFreeHost(s->h_on);
+  cudaFreeHost(s->h_out);
+  cudaFreeHost(s->h_bad);
+  if (s->e0) cudaEventDestroy(s->e0);
+  if (s->e1) cudaEventDestroy(s->e1);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+// m(J/psi p) windows of the 20-offset smearing, on the float mass as the reference tests them.
+inline bool in_window(float mz) { return (mz > 4.4 && mz < 4.48) || (mz > 4.27 && mz < 4.34); }
+
+// Event classes as the single-point evaluator's segments give them for toy windows and the MC.
+std::vector<uint8_t> event_kinds(const pwa_ens* s, const std::vector<float>& mz, const std::vector<int64_t>& band1,
+                                 const std::vector<int64_t>& band2) {
+  const int64_t n = s->cv.n, nda = s->cv.nda;
+  std::vector<uint8_t> k(n, EK_NONE);
+  if (s->cv.gauss) {
+    std::fill(k.begin(), k.end(), (uint8_t)EK_GRID);
+    return k;
+  }
+  for (int t = 0; t < s->n_toys; ++t) {
+    const int64_t f = s->first[t], wn = s->count[t], a = band1[t], b = band2[t];
+    const int64_t b1e = f + std::max<int64_t>(0, std::min(wn, a));
+    const int64_t b2e = std::max(b1e, f + std::min(wn, a + b));
+    const int64_t r0 = f + std::min(wn, std::max<int64_t>(0, a + b));
+    for (int64_t e = f; e < b1e; ++e) k[e] = EK_S30;
+    for (int64_t e = b1e; e < b2e; ++e) k[e] = EK_S150;
+    for (int64_t e = r0; e < f + wn; ++e) k[e] = in_window(mz[e]) ? EK_S20 : EK_NONE;
+  }
+  for (int64_t e = nda; e < n; ++e) k[e] = in_window(mz[e]) ? EK_S20 : EK_NONE;
+  return k;
+}
+
+// Slot index of Lambda* (r, k, m) and of Pc entry at order position q (q, k, m).
+inline int slot_l(const pwa_ens* s, int k, int r, int m) { return k * s->NS + r * 6 + m; }
+inline int slot_z(const pwa_ens* s, int k, int q, int m) { return k * s->NS + 6 * s->NR + q * 12 + m; }
+
+void table_slots(const pwa_ens* s, const PointTable& T, double* out) {
+  for (int k = 0; k < 2; ++k) {
+    for (int r = 0; r < s->NR; ++r)
+      for (int m = 0; m < 6; ++m) {
+        const cplx c = T.L[r].c[k * 6 + m];
+        out[2 * slot_l(s, k, r, m)] = c.re;
+        out[2 * slot_l(s, k, r, m) + 1] = c.im;
+      }
+    for (int q = 0; q < s->NZ; ++q)
+      for (int m = 0; m < 12; ++m) {
+        const cplx c = T.Z[T.order[q]].c[k * 12 + m];
+        out[2 * slot_z(s, k, q, m)] = c.re;
+        out[2 * slot_z(s, k, q, m) + 1] = c.im;
+      }
+  }
+}
+
+// The Gram entries of active slot pairs a <= b (same proton helicity): kind 0 for M, 1 for the Pc
+// part of Mn.
+struct EntryRef {
+  int a, b, kind;
+};
+void gram_entries(const pwa_ens* s, const std::vector<uint8_t>& active, std::vector<GramEntry>* ent,
+                  std::vector<EntryRef>* ref) {
+  const GramBuf G{s->NR, s->NZ};
+  const int NR = s->NR, NZ = s->NZ;
+  auto add = [&](int a, int b, int kind, int o1, int o2, int o3, int o4) {
+    if (!active[a] || !active[b]) return;
+    ent->push_back(GramEntry{(int16_t)o1, (int16_t)o2, (int16_t)o3, (int16_t)o4});
+    ref->push_back(EntryRef{a, b, kind});
+  };
+  for (int k = 0; k < 2; ++k) {
+    for (int r = 0; r < NR; ++r)
+      for (int m = 0; m < 6; ++m) {
+        const int a = slot_l(s, k, r, m);
+        for (int r2 = 0; r2 < NR; ++r2)
+          for (int m2 = 0; m2 < 6; ++m2) {
+            const int b = slot_l(s, k, r2, m2);
+            if (b >= a) add(a, b, 0, G.ql(k, r, m), G.ql(k, r2, m2), G.pl(m, m2), G.one());
+          }
+        for (int q = 0; q < NZ; ++q)
+          for (int m2 = 0; m2 < 12; ++m2)
+            add(a, slot_z(s, k, q, m2), 0, G.ql(k, r, m), G.yz(k, q, m2), G.plz(m, m2), G.one());
+      }
+    for (int q = 0; q < NZ; ++q)
+      for (int m = 0; m < 12; ++m) {
+        const int a = slot_z(s, k, q, m);
+        for (int q2 = 0; q2 < NZ; ++q2)
+          for (int m2 = 0; m2 < 12; ++m2) {
+            const int b = slot_z(s, k, q2, m2);
+            if (b < a) continue;
+            add(a, b, 0, G.dz(k, q, m), G.dz(k, q2, m2), G.pz(m, m2), G.s2(q, q2));
+            add(a, b, 1, G.dz(k, q, m), G.dz(k, q2, m2), G.pz(m, m2), G.rn2(q, q2));
+          }
+      }
+  }
+}
+
+size_t gram_smem(const pwa_ens* s) {
+  return ((sizeof(PointTable) + 15) & ~size_t(15)) + (size_t)GRAM_EB * GramBuf{s->NR, s->NZ}.size() * sizeof(cplx);
+}
+
+// Factor rows of the data of every toy, then the Gram matrices over the MC in chunks.
+int ens_setup(pwa_ens* s, const std::vector<uint8_t>& active) {
+  const CtxView& cv = s->cv;
+  cudaError_t e;
+  EventSet ev{cv.pp, cv.pp1, cv.pp2, cv.sw, cv.n_size, cv.n, cv.nda};
+  const size_t tsm = (sizeof(PointTable) + 15) & ~size_t(15);
+  if ((e = cudaFuncSetAttribute(k_ens_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm)))
+    return ens_fail(s, e);
+  const FactorLayout F{s->NR, s->NZ};
+  s->ld = std::max<int64_t>(cv.nda, 1);
+  if ((e = ens_alloc(s, &s->d_fac, (size_t)F.size(false) * s->ld))) return ens_fail(s, e);
+  cudaEventRecord(s->e0, s->st);
+  for (int t = 0; t < s->n_toys; ++t) {
+    if (s->count[t] == 0) continue;
+    k_ens_factors<<<(unsigned)((s->count[t] + 127) / 128), 128, tsm, s->st>>>(
+        s->d_T, ev, s->d_kind, s->first[t], s->count[t], cv.grid, cv.grid_nb, s->d_fac + s->first[t], s->ld, 0);
+  }
+  cudaEventRecord(s->e1, s->st);
+  if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(s->st))) return ens_fail(s, e);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, s->e0, s->e1);
+  s->factors_ms = ms;
+  // Gram entries and the chunked accumulation over the MC
+  std::vector<GramEntry> ent;
+  std::vector<EntryRef> ref;
+  gram_entries(s, active, &ent, &ref);
+  const int n_ent = (int)ent.size();
+  const int64_t n_mc = cv.n - cv.nda;
+  s->M.assign((size_t)s->n_slot * s->n_slot, mk(0, 0));
+  s->Mn.assign((size_t)s->n_slot * s->n_slot, mk(0, 0));
+  if (n_ent > 0 && n_mc > 0) {
+    const int64_t CH = std::min<int64_t>(n_mc, 1 << 16);
+    const int tiles_y = (n_ent + GRAM_THREADS * GRAM_EPT - 1) / (GRAM_THREADS * GRAM_EPT);
+    const int gx = std::max(1, (2 * cv.sm_count + tiles_y - 1) / tiles_y);
+    GramEntry* d_ent = nullptr;
+    double* d_cf = nullptr;
+    cplx *d_part = nullptr, *d_acc = nullptr;
+    const size_t smem = gram_smem(s);
+    if ((e = cudaFuncSetAttribute(k_ens_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+        (e = cudaMalloc(&d_ent, n_ent * sizeof(GramEntry))) ||
+        (e = cudaMalloc(&d_cf, (size_t)F.size(true) * CH * sizeof(double))) ||
+        (e = cudaMalloc(&d_part, (size_t)gx * n_ent * sizeof(cplx))) || (e = cudaMalloc(&d_acc, n_ent * sizeof(cplx)))) {
+      cudaFree(d_ent);
+      cudaFree(d_cf);
+      cudaFree(d_part);
+      return ens_fail(s, e);
+    }
+    e = cudaMemcpyAsync(d_ent, ent.data(), n_ent * sizeof(GramEntry), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_acc, 0, n_ent * sizeof(cplx), s->st);
+    cudaEventRecord(s->e0, s->st);
+    for (int64_t c0 = cv.nda; c0 < cv.n && e == cudaSuccess; c0 += CH) {
+      const int64_t cnt = std::min<int64_t>(CH, cv.n - c0);
+      k_ens_factors<<<(unsigned)((cnt + 127) / 128), 128, tsm, s->st>>>(s->d_T, ev, s->d_kind, c0, cnt, cv.grid,
+                                                                         cv.grid_nb, d_cf, CH, 1);
+      k_ens_gram<<<dim3(gx, tiles_y), GRAM_THREADS, smem, s->st>>>(s->d_T, ev, c0, cnt, d_cf, CH, d_ent, n_ent,
+                                                                    d_part);
+      k_ens_sum_rows<<<(n_ent + 255) / 256, 256, 0, s->st>>>(d_part, gx, n_ent, d_acc);
+      e = cudaGetLastError();
+    }
+    cudaEventRecord(s->e1, s->st);
+    std::vector<cplx> acc(n_ent);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(acc.data(), d_acc, n_ent * sizeof(cplx), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d_ent);
+    cudaFree(d_cf);
+    cudaFree(d_part);
+    cudaFree(d_acc);
+    if (e) return ens_fail(s, e);
+    cudaEventElapsedTime(&ms, s->e0, s->e1);
+    s->gram_ms = ms;
+    const int n = s->n_slot;
+    for (int j = 0; j < n_ent; ++j) {
+      const EntryRef& r = ref[j];
+      std::vector<cplx>& dst = r.kind == 0 ? s->M : s->Mn;
+      dst[(size_t)r.a * n + r.b] = acc[j];
+      dst[(size_t)r.b * n + r.a] = conj(acc[j]);
+      // the Lambda* block of Mn is that of M (no Lambda* - Pc term without interference)
+      const bool both_l = (r.a % s->NS) < 6 * s->NR && (r.b % s->NS) < 6 * s->NR;
+      if (r.kind == 0 && both_l) {
+        s->Mn[(size_t)r.a * n + r.b] = acc[j];
+        s->Mn[(size_t)r.b * n + r.a] = conj(acc[j]);
+      }
+    }
+  }
+  if ((e = cudaMemcpyAsync(s->d_M, s->M.data(), s->M.size() * sizeof(cplx), cudaMemcpyHostToDevice, s->st)) ||
+      (e = cudaMemcpyAsync(s->d_Mn, s->Mn.data(), s->Mn.size() * sizeof(cplx), cudaMemcpyHostToDevice, s->st)) ||
+      (e = cudaStreamSynchronize(s->st)))
+    return ens_fail(s, e);
+  return PWA_OK;
+}
+
+int ens_fail(pwa_ens*, cudaError_t e) { return cuda_fail(e); }
+
+// The work list for the current tile size.
+int ens_tiles(pwa_ens* s) {
+  std::vector<Tile> tl;
+  for (int t = 0; t < s->n_toys; ++t)
+    for (int64_t e0 = s->first[t]; e0 < s->first[t] + s->count[t]; e0 += s->tile_events)
+      tl.push_back(Tile{e0, std::min(e0 + s->tile_events, s->first[t] + s->count[t]), t, 0});
+  cudaFree(s->d_tiles);
+  s->d_tiles = nullptr;
+  s->n_tiles = (int)tl.size();
+  cudaError_t e = cudaMalloc(&s->d_tiles, std::max<size_t>(tl.size(), 1) * sizeof(Tile));
+  if (e == cudaSuccess && !tl.empty())
+    e = cudaMemcpy(s->d_tiles, tl.data(), tl.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+  if (e) return cuda_fail(e);
+  return PWA_OK;
+}
+
+template <int W>
+cudaError_t launch_data(pwa_ens* s) {
+  const EventSet ev{s->cv.pp, s->cv.pp1, s->cv.pp2, s->cv.sw, s->cv.n_size, s->cv.n, s->cv.nda};
+  const size_t smem = ens_data_smem<W>();
+  k_ens_data<W><<<s->blocks, W * 32, smem, s->st>>>(s->d_T, ev, s->d_fac, s->ld, s->d_tiles, s->n_tiles, s->d_next,
+                                                    s->d_coup, s->d_on, s->n_slot, s->d_val, s->d_grad, s->d_bad);
+  return cudaGetLastError();
+}
+
+// Captures one ensemble step (inputs in, both kernels, results out) into a CUDA graph.
+int ens_capture(pwa_ens* s) {
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  const size_t nc = (size_t)s->n_toys * s->n_slot;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal);
+  if (e) return cuda_fail(e);
+  cudaMemcpyAsync(s->d_coup, s->h_coup, nc * sizeof(cplx), cudaMemcpyHostToDevice, s->st);
+  cudaMemcpyAsync(s->d_on, s->h_on, s->n_toys * sizeof(int), cudaMemcpyHostToDevice, s->st);
+  cudaMemsetAsync(s->d_val, 0, s->n_toys * sizeof(double), s->st);
+  cudaMemsetAsync(s->d_bad, 0, s->n_toys * sizeof(unsigned long long), s->st);
+  cudaMemsetAsync(s->d_grad, 0, nc * sizeof(cplx), s->st);
+  cudaMemsetAsync(s->d_next, 0, sizeof(int), s->st);
+  cudaError_t le = s->warps == 4 ? launch_data<4>(s) : launch_data<8>(s);
+  k_ens_finish<<<s->n_toys, 256, 0, s->st>>>(s->n_slot, s->d_M, s->d_Mn, s->d_coup, s->d_on, s->d_val, s->d_grad,
+                                             s->d_wdata, s->w_mc, s->shift, s->d_out, s->d_gout);
+  cudaMemcpyAsync(s->h_out, s->d_out, 4 * s->n_toys * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  cudaMemcpyAsync(s->h_gout, s->d_gout, nc * sizeof(cplx), cudaMemcpyDeviceToHost, s->st);
+  cudaMemcpyAsync(s->h_bad, s->d_bad, s->n_toys * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st);
+  e = cudaStreamEndCapture(s->st, &g);
+  if (le && !e) e = le;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e) {
+    s->graph = nullptr;
+    return cuda_fail(e);
+  }
+  return PWA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pwa_ens_set_launch(pwa_ens* s, int warps, int tile_events);
+
+int pwa_ens_create(pwa_ctx* ctx, const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                   int NX, float FFR, float FFB, int n_toys, const int64_t* first, const int64_t* count,
+                   const int64_t* nda_smr, const int64_t* nda_fine, const double* sum_w_data, double sum_w_mc,
+                   const uint8_t* active, pwa_ens** out) {
+  if (!ctx || !pl || !out || n_toys < 1 || !first || !count || !nda_smr || !nda_fine || !sum_w_data) return PWA_E_ARG;
+  *out = nullptr;
+  if (NX > 0) return PWA_E_UNSUPPORTED;
+  pwa_ens* s = new pwa_ens();
+  int rc = ctx_view(ctx, &s->cv);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  const CtxView& cv = s->cv;
+  for (int t = 0; t < n_toys; ++t)
+    if (first[t] < 0 || count[t] < 0 || first[t] + count[t] > cv.nda) {
+      delete s;
+      return PWA_E_ARG;
+    }
+  s->n_toys = n_toys;
+  s->first.assign(first, first + n_toys);
+  s->count.assign(count, count + n_toys);
+  s->wdata.assign(sum_w_data, sum_w_data + n_toys);
+  s->w_mc = sum_w_mc;
+  cudaError_t e = cudaSetDevice(cv.device);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cv.st);  // the context's work on its events is done
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_T, sizeof(PointTable));
+  if (e) {
+    ens_free(s);
+    return cuda_fail(e);
+  }
+  if ((rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, s->h_T))) {
+    ens_free(s);
+    return rc;
+  }
+  s->NR = NR;
+  s->NZ = NZ;
+  s->NS = 6 * NR + 12 * NZ;
+  s->n_slot = 2 * s->NS;
+  if ((e = ens_alloc(s, &s->d_T, 1))) {
+    ens_free(s);
+    return cuda_fail(e);
+  }
+  if (cv.use_tables) {
+    if ((e = ens_alloc(s, reinterpret_cast<uint8_t**>(&s->d_tab), TAB_BYTES))) {
+      ens_free(s);
+      return cuda_fail(e);
+    }
+    attach_tables(s->h_T, s->d_tab);
+  }
+  e = cudaMemcpyAsync(s->d_T, s->h_T, sizeof(PointTable), cudaMemcpyHostToDevice, s->st);
+  if (e == cudaSuccess && s->h_T->tab.enabled) e = launch_build_tables(s->d_T, TAB_NODES, cv.sm_count, s->st);
+  // event classes (the float m(J/psi p) plane decides the window, as in the reference)
+  std::vector<float> mz(cv.n);
+  if (e == cudaSuccess && cv.n)
+    e = cudaMemcpyAsync(mz.data(), cv.pp + cv.n_size, cv.n * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e) {
+    ens_free(s);
+    return cuda_fail(e);
+  }
+  const std::vector<uint8_t> kinds =
+      event_kinds(s, mz, std::vector<int64_t>(nda_smr, nda_smr + n_toys), std::vector<int64_t>(nda_fine, nda_fine + n_toys));
+  const size_t nc = (size_t)n_toys * s->n_slot;
+  if ((e = ens_alloc(s, &s->d_kind, cv.n)) ||
+      (e = cudaMemcpy(s->d_kind, kinds.data(), cv.n, cudaMemcpyHostToDevice)) ||
+      (e = ens_alloc(s, &s->d_M, (size_t)s->n_slot * s->n_slot)) ||
+      (e = ens_alloc(s, &s->d_Mn, (size_t)s->n_slot * s->n_slot)) || (e = ens_alloc(s, &s->d_coup, nc)) ||
+      (e = ens_alloc(s, &s->d_grad, nc)) || (e = ens_alloc(s, &s->d_gout, nc)) ||
+      (e = ens_alloc(s, &s->d_on, n_toys)) || (e = ens_alloc(s, &s->d_next, 1)) ||
+      (e = ens_alloc(s, &s->d_val, n_toys)) || (e = ens_alloc(s, &s->d_wdata, n_toys)) ||
+      (e = ens_alloc(s, &s->d_out, 4 * (size_t)n_toys)) || (e = ens_alloc(s, &s->d_bad, n_toys)) ||
+      (e = cudaMemcpy(s->d_wdata, sum_w_data, n_toys * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMallocHost(&s->h_coup, nc * sizeof(cplx))) || (e = cudaMallocHost(&s->h_gout, nc * sizeof(cplx))) ||
+      (e = cudaMallocHost(&s->h_on, n_toys * sizeof(int))) ||
+      (e = cudaMallocHost(&s->h_out, 4 * (size_t)n_toys * sizeof(double))) ||
+      (e = cudaMallocHost(&s->h_bad, n_toys * sizeof(unsigned long long)))) {
+    ens_free(s);
+    return cuda_fail(e);
+  }
+  std::vector<uint8_t> act(s->n_slot, 1);
+  if (active) act.assign(active, active + s->n_slot);
+  if ((rc = ens_setup(s, act))) {
+    ens_free(s);
+    return rc;
+  }
+  if ((rc = pwa_ens_set_launch(s, s->warps, s->tile_events))) {
+    ens_free(s);
+    return rc;
+  }
+  *out = s;
+  return PWA_OK;
+}
+
+int pwa_ens_destroy(pwa_ens* s) {
+  ens_free(s);
+  return PWA_OK;
+}
+
+int pwa_ens_slot_count(const pwa_ens* s) { return s ? s->n_slot : 0; }
+
+int pwa_ens_slots(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX, float FFR,
+                  float FFB, double* h_slots) {
+  if (!pl || !h_slots) return PWA_E_ARG;
+  if (NX != 0) return PWA_E_UNSUPPORTED;
+  PointTable* T = new PointTable();
+  const int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, T);
+  if (!rc) {
+    pwa_ens shape;
+    shape.NR = NR;
+    shape.NZ = NZ;
+    shape.NS = 6 * NR + 12 * NZ;
+    table_slots(&shape, *T, h_slots);
+  }
+  delete T;
+  return rc;
+}
+
+int pwa_ens_gram(const pwa_ens* s, double* h_M, double* h_Mn) {
+  if (!s) return PWA_E_ARG;
+  if (h_M) std::memcpy(h_M, s->M.data(), s->M.size() * sizeof(cplx));
+  if (h_Mn) std::memcpy(h_Mn, s->Mn.data(), s->Mn.size() * sizeof(cplx));
+  return PWA_OK;
+}
+
+int pwa_ens_set_launch(pwa_ens* s, int warps, int tile_events) {
+  if (!s || (warps != 4 && warps != 8) || tile_events < 32) return PWA_E_ARG;
+  cudaError_t e = cudaSetDevice(s->cv.device);
+  if (e) return cuda_fail(e);
+  s->warps = warps;
+  s->tile_events = tile_events;
+  const size_t smem = warps == 4 ? ens_data_smem<4>() : ens_data_smem<8>();
+  e = warps == 4 ? cudaFuncSetAttribute(k_ens_data<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                 : cudaFuncSetAttribute(k_ens_data<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 1;
+  if (e == cudaSuccess)
+    e = warps == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_data<4>, 128, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_data<8>, 256, smem);
+  if (e) return cuda_fail(e);
+  s->blocks = s->cv.sm_count * std::max(occ, 1);
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  return ens_tiles(s);
+}
+
+int pwa_ens_eval(pwa_ens* s, const double* h_slots, const int* h_on, double nll_shift, double* h_out, double* h_grad,
+                 int64_t* h_bad) {
+  if (!s || !h_slots || !h_out) return PWA_E_ARG;
+  cudaError_t e = cudaSetDevice(s->cv.device);
+  if (e) return cuda_fail(e);
+  if (!s->graph || nll_shift != s->shift) {
+    s->shift = nll_shift;
+    const int rc = ens_capture(s);
+    if (rc) return rc;
+  }
+  const size_t nc = (size_t)s->n_toys * s->n_slot;
+  std::memcpy(s->h_coup, h_slots, nc * sizeof(cplx));
+  for (int t = 0; t < s->n_toys; ++t) s->h_on[t] = h_on ? (h_on[t] != 0) : 1;
+  if ((e = cudaEventRecord(s->e0, s->st)) || (e = cudaGraphLaunch(s->graph, s->st)) ||
+      (e = cudaEventRecord(s->e1, s->st)) || (e = cudaStreamSynchronize(s->st)))
+    return cuda_fail(e);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, s->e0, s->e1);
+  s->last_ms = ms;
+  for (int t = 0; t < s->n_toys; ++t) {
+    if (!s->h_on[t]) continue;
+    for (int j = 0; j < 4; ++j) h_out[4 * t + j] = s->h_out[4 * t + j];
+    if (h_bad) h_bad[t] = (int64_t)s->h_bad[t];
+    if (h_grad) std::memcpy(h_grad + 2 * (size_t)t * s->n_slot, s->h_gout + (size_t)t * s->n_slot, s->n_slot * sizeof(cplx));
+  }
+  return PWA_OK;
+}
+
+double pwa_ens_last_ms(const pwa_ens* s) { return s ? s->last_ms : 0.0; }
+
+int pwa_ens_setup_ms(const pwa_ens* s, double* factors_ms, double* gram_ms) {
+  if (!s) return PWA_E_ARG;
+  if (factors_ms) *factors_ms = s->factors_ms;
+  if (gram_ms) *gram_ms = s->gram_ms;
+  return PWA_OK;
+}
+
+}  // extern "C"

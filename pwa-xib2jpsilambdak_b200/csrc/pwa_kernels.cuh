@@ -6,6 +6,8 @@
 
 #include "pwa_point.cuh"
 
+struct pwa_ctx;
+
 namespace pwa {
 
 // Per-block partial sums written by the event kernels and reduced by finalize.
@@ -73,6 +75,19 @@ int segment_parts(const Segment& s, int sm_count, bool deferred);
 // Records a failed CUDA call's message (pwa_last_cuda_error) and returns PWA_E_CUDA, or PWA_E_NOMEM
 // for a failed allocation.
 int cuda_fail(cudaError_t e);
+
+// What other parts of the library read of a context: its device, events and resolution model.
+struct CtxView {
+  int device, sm_count;
+  cudaStream_t st;
+  const float *pp, *pp1, *pp2, *sw, *pp3, *pp4;
+  int64_t n, n_size, nda;
+  int gauss;            // 1: Gaussian resolution on a weighted grid (d_grid, grid_nb)
+  const double* grid;
+  int grid_nb;
+  int use_tables;
+};
+int ctx_view(const pwa_ctx* c, CtxView* v);
 
 // Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,

@@ -24,6 +24,8 @@ EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_c
             "pwa_flow_set_params", "pwa_flow_train_step", "pwa_flow_gradients", "pwa_flow_log_density",
             "pwa_flow_sample", "pwa_flow_fit_premap", "pwa_flow_get_premap", "pwa_flow_set_premap",
             "pwa_basis_from_angles", "pwa_angles_from_vectors",
+            "pwa_ens_create", "pwa_ens_destroy", "pwa_ens_slot_count", "pwa_ens_slots", "pwa_ens_gram",
+            "pwa_ens_set_launch", "pwa_ens_eval", "pwa_ens_last_ms", "pwa_ens_setup_ms",
             "pwa_error_string", "pwa_last_cuda_error"]
 
 _fp = C.POINTER(C.c_float)
@@ -129,6 +131,7 @@ class Context:
         h = C.c_void_p()
         check(self.L.pwa_ctx_create(device, C.byref(h)), "pwa_ctx_create")
         self.h = h
+        self.device = device
         self.sample = None
         self.n = 0
 
