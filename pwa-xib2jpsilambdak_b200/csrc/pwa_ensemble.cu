@@ -329,7 +329,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
     double value = 0;
     unsigned long long nbad = 0;
     for (int64_t e = tl.e0 + warp; e < tl.e1; e += WARPS) {
-      stage_event(T, ev, e, W.pl, lane);
+      // every plane slot of pp, pp1, pp2: a fit moves couplings that are zero at the set-up point too,
+      // so the point table's own staging list (its non-zero helicity slots) is not enough here
+      for (int j = lane; j < SLOT_PP3; j += 32) {
+        const float* src = j < SLOT_PP1 ? ev.pp + (size_t)j * ev.n_size
+                                        : (j < SLOT_PP2 ? ev.pp1 + (size_t)(j - SLOT_PP1) * ev.n_size
+                                                        : ev.pp2 + (size_t)(j - SLOT_PP2) * ev.n_size);
+        W.pl[j] = (double)__ldg(src + e);
+      }
       for (int f = lane; f < nf; f += 32) W.fac[f] = fac[(size_t)f * ld + e];
       __syncwarp();
       const EvS E{W.pl};

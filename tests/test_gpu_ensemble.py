@@ -63,6 +63,29 @@ def test_nll_matches_single_point_per_toy(setup):
     toys.select_all(ctx, ens)
 
 
+def test_couplings_zero_at_the_set_up_point(setup):
+    """Couplings that are zero where the ensemble is set up (so the set-up point's helicity masks leave
+    their slots out) and move in the fit: still the single-point evaluator's NLL."""
+    from pwa_b200 import ensemble, toys
+    mode, mdl, vals, ens, ctx, E = setup
+    v0 = dict(vals)
+    zeroed = E.names[:4] + E.names[-4:]
+    for n in zeroed:
+        v0[n] = 0.0
+    E0 = ensemble.Ensemble(ctx, ens, mdl, v0, E.names)
+    try:
+        X = _random_points(E0, 0.2, 9)
+        out, _, bad = E0.eval_slots(np.stack([E0.exact_slots(x) for x in X]))
+        assert np.all(bad == 0)
+        for t in (1, 3):
+            toys.select(ctx, ens, t)
+            r = ctx.eval_nll(E0.builder.block(dict(zip(E0.names, X[t]))))
+            assert abs(out[t, 0] - r.nll) < NLL_TOL, (mode, t, out[t, 0], r.nll)
+        toys.select_all(ctx, ens)
+    finally:
+        E0.close()
+
+
 def test_nll_matches_oracle_on_toy_alone(setup, oracle_mod):
     from pwa_b200 import dataset as D
     mode, mdl, vals, ens, ctx, E = setup
@@ -70,7 +93,8 @@ def test_nll_matches_oracle_on_toy_alone(setup, oracle_mod):
         pytest.skip("the oracle takes the reference's resolution scheme")
     s = ens.sample
     X = _random_points(E, 0.2, 6)
-    out, _, _ = E.eval_slots(np.stack([E.exact_slots(x) for x in X]))
+    out, _, bad = E.eval_slots(np.stack([E.exact_slots(x) for x in X]))
+    assert np.all(bad == 0)
     for t in (0, 2):
         v = ens.view(t)
         cols = np.r_[v.first:v.first + v.nda, s.nda:s.n]
