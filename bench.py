@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--exact", action="store_true", help="solve the K-matrix for every lookup (no tables)")
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the toy-ensemble fit measurement")
     ap.add_argument("--no-full-parity", action="store_true",
                     help="skip the FP64 oracle check of the whole sample (centre and one point per batch kind)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
@@ -362,6 +363,92 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
     }
 
 
+# ------------------------------------------------------------------------------ toy ensemble
+ENSEMBLE = {"model": "full_bw", "n_toys": 256, "size_lo": 5e3, "size_hi": 2e5, "size_seed": 42, "n_mc": 1_000_000,
+            "w_range": (0.2, 1.0), "smearing": ("gauss", 0.0027, 0.0005, 17), "gen_seed": 11, "parity_toys": (0, 1, 2)}
+# bytes the ensemble kernel reads per data event: the pp / pp1 / pp2 plane slots (303 floats), the
+# data weight, and the cached lineshape factors (2 NR + 2 NZ + NZ (NZ + 1) doubles; NR = 14, NZ = 3)
+ENSEMBLE_BYTES_PER_EVENT = 303 * 4 + 4 + (2 * 14 + 2 * 3 + 3 * 4) * 8
+
+
+def ensemble_bench(device: int, hbm: float) -> dict:
+    """The batched-gradient config's toy study: 256 seeded toys of the full Breit-Wigner model with sizes
+    log-uniform in 5k-200k events and one 1M-event MC sample, all fitted together (every coupling but
+    the reference one free), against the toy-by-toy fit through the batched numerical gradient."""
+    import torch
+    from pwa_b200 import configs, ensemble, fit as F, lib, model as M, toys
+    P = ENSEMBLE
+    mdl, vals = configs.MODELS[P["model"]]()
+    block = M.build_param_block(mdl, vals)
+    sizes = toys.toy_sizes(P["n_toys"], P["size_lo"], P["size_hi"], P["size_seed"])
+    t0 = time.perf_counter()
+    ens = toys.make_ensemble_gpu(block, sizes, P["n_mc"], P["w_range"], seed=P["gen_seed"], device=device)
+    t_gen = time.perf_counter() - t0
+    ctx = lib.Context(device)
+    ctx.bind_device(ens.sample)
+    ctx.set_smearing(*P["smearing"])
+    names = ensemble.coupling_names(mdl)
+    t0 = time.perf_counter()
+    E = ensemble.Ensemble(ctx, ens, mdl, vals, names)
+    t_setup = time.perf_counter() - t0
+    fac_ms, gram_ms = E.setup_ms()
+    tune = ensemble.autotune(E)
+    S = np.repeat(E.s0[None, :], E.n_toys, axis=0)
+    ms = []
+    for _ in range(5):
+        E.eval_slots(S)
+        ms.append(E.last_ms())
+    step_ms = float(np.median(ms[1:]))
+    n_ev = int(sizes.sum())
+    gbs = ENSEMBLE_BYTES_PER_EVENT * n_ev / (step_ms / 1e3) / 1e9
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    fit = E.fit()
+    t_fit = time.perf_counter() - t0
+    # parity of the fitted points: the exact float blocks through the single-point evaluator
+    par = []
+    for t in P["parity_toys"]:
+        out, _, _ = E.eval_slots(np.repeat(E.exact_slots(fit.x[t])[None, :], E.n_toys, axis=0))
+        toys.select(ctx, ens, t)
+        r = ctx.eval_nll(E.builder.block(dict(zip(names, fit.x[t]))))
+        par.append(abs(out[t, 0] - r.nll))
+    # the toy-by-toy path: one batched numerical gradient (2N+1 points over the toy's data and the MC)
+    grad_s = []
+    for t in (int(np.argmin(sizes)), int(np.argmax(sizes))):
+        toys.select(ctx, ens, t)
+        f = F.gpu_fcn(ctx, mdl, vals, names)
+        X = F._grad_points(fit.x[t], np.full(len(names), 1e-3))
+        f(X)
+        t1 = time.perf_counter()
+        f(X)
+        grad_s.append(time.perf_counter() - t1)
+    toys.select_all(ctx, ens)
+    # Migrad-like toy-by-toy fits need at least one gradient per iteration: project with the ensemble's
+    # own iteration counts (a lower bound on the sequential cost)
+    seq_s = float(np.sum(fit.iterations + 1) * np.mean(grad_s))
+    E.close()
+    ctx.close()
+    del ens
+    return {
+        "model": "full_bw (14 Lambda* BW, 3 narrow Pc BW), Gaussian resolution 2.7 MeV on a 0.5 MeV grid",
+        "toys": P["n_toys"], "toy_sizes": "floor(exp U(ln 5e3, ln 2e5)), seed 42", "data_events": n_ev,
+        "mc_events": P["n_mc"], "free_parameters": len(names), "slots": E.n_slot,
+        "generate_s": round(t_gen, 3), "setup_s": round(t_setup, 3), "factor_cache_ms": round(fac_ms, 3),
+        "gram_ms": round(gram_ms, 3), "launch_shape": {k: tune[k] for k in ("warps", "tile_events", "cached")},
+        "step_ms": round(step_ms, 3), "step_gbs": round(gbs, 1), "step_frac_of_hbm": round(gbs / hbm, 4),
+        "step_bytes_per_event": ENSEMBLE_BYTES_PER_EVENT,
+        "fit_wall_s": round(t_fit, 3), "fit_calls": fit.calls, "fit_device_s": round(fit.device_ms / 1e3, 3),
+        "converged": int(fit.converged.sum()), "iterations_mean": float(fit.iterations.mean()),
+        "iterations_max": int(fit.iterations.max()),
+        "parity_fitted_points_max_dnll": float(max(par)),
+        "sequential_gradient_s": [round(x, 4) for x in grad_s],
+        "sequential_projection_s": round(seq_s, 1),
+        "speedup_vs_sequential_projection": round(seq_s / t_fit, 1),
+        "note": "sequential projection = sum over toys of (iterations + 1) x the measured time of one "
+                "batched numerical gradient (2N+1 points over the toy's window and the MC), a lower bound",
+    }
+
+
 # ------------------------------------------------------------------------------ GPU arm
 def main():
     args = parse()
@@ -577,6 +664,11 @@ def main():
             out["proposal"] = proposal_bench(local, bf16)
         except Exception as ex:
             out["proposal"] = {"failed": str(ex)}
+    if world == 1 and not args.no_ensemble:
+        try:
+            out["ensemble"] = ensemble_bench(local, hbm)
+        except Exception as ex:
+            out["ensemble"] = {"failed": str(ex)}
     if bat:
         out = batched_line(out, bat, args, world, sample, req_b, hbm, peak_kind)
     print(json.dumps(out))

@@ -132,9 +132,13 @@ def test_gram_matrices_are_hermitian_and_positive(setup):
     M, Mn = E.gram()
     assert np.allclose(M, M.conj().T, rtol=0, atol=1e-12 * np.abs(M).max())
     J = E.J
-    # restricted to the fit directions the normalisation is a positive quadratic form
+    # restricted to the fit directions the normalisation is a positive quadratic form; its null space is
+    # that of J (parameters, or combinations of them, that move no helicity coupling)
     H = np.real(J.conj().T @ M @ J)
-    assert np.linalg.eigvalsh(0.5 * (H + H.T)).min() > 0
+    ev = np.linalg.eigvalsh(0.5 * (H + H.T))
+    rank = np.linalg.matrix_rank(np.vstack([J.real, J.imag]))
+    assert ev.min() > -1e-12 * ev.max()
+    assert np.sum(ev > 1e-9 * ev.max()) == rank
     assert np.all(np.real(np.diag(Mn)) >= 0)
 
 
