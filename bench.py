@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the toy-ensemble fit measurement")
+    ap.add_argument("--profile-case", choices=["flow_small", "ensemble_small"],
+                    help="run one small case of a kernel for a profiler capture (no bench line)")
     ap.add_argument("--no-full-parity", action="store_true",
                     help="skip the FP64 oracle check of the whole sample (centre and one point per batch kind)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
@@ -449,9 +451,44 @@ def ensemble_bench(device: int, hbm: float) -> dict:
     }
 
 
+# ------------------------------------------------------------------------------ profiler cases
+def profile_case(name: str, device: int = 0) -> int:
+    """Small runs of one kernel family for ncu captures (inputs above L2, a few GB on the device at
+    most): flow_small = 12 training steps of the proposal network on 16,384-event batches (k_gemm);
+    ensemble_small = an 8-toy ensemble of the full BW model (8 x 40k data events, 100k MC) and three
+    ensemble steps (k_ens_data)."""
+    import torch
+    from pwa_b200 import configs, ensemble, flow, lib, model as M, toys
+    if name == "flow_small":
+        f = flow.Flow(device, max_batch=16384, seed=3)
+        x = flow.flat_unit(12 * 16384, seed=5, device=device)
+        w = torch.rand(x.shape[1], dtype=torch.float64, device=x.device, generator=torch.Generator(x.device).manual_seed(6))
+        f.fit_premap(x, w)
+        f.train(x, w, epochs=1, batch=16384, lr=1e-3)
+        f.close()
+    else:
+        mdl, vals = configs.MODELS["full_bw"]()
+        block = M.build_param_block(mdl, vals)
+        ens = toys.make_ensemble_gpu(block, np.full(8, 40_000), 100_000, (0.2, 1.0), seed=7, device=device)
+        ctx = lib.Context(device)
+        ctx.bind_device(ens.sample)
+        ctx.set_smearing("gauss", 0.0027, 0.0005, 17)
+        E = ensemble.Ensemble(ctx, ens, mdl, vals, ensemble.coupling_names(mdl))
+        S = np.repeat(E.s0[None, :], E.n_toys, axis=0)
+        for _ in range(3):
+            E.eval_slots(S)
+        print(json.dumps({"case": name, "step_ms": E.last_ms(), "events": int(ens.offsets[-1])}))
+        E.close()
+        ctx.close()
+    torch.cuda.synchronize(device)
+    return 0
+
+
 # ------------------------------------------------------------------------------ GPU arm
 def main():
     args = parse()
+    if args.profile_case:
+        return profile_case(args.profile_case)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
