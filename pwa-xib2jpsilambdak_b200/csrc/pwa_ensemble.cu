@@ -267,7 +267,6 @@ __global__ void k_ens_sum_rows(const cplx* __restrict__ part, int rows, int n, c
 
 // ------------------------------------------------------------------ data terms of all toys
 constexpr int ENS_MAX_SLOTS = 2 * (6 * MAX_LSTAR + 12 * MAX_PC);
-constexpr int ENS_SPL = (ENS_MAX_SLOTS + 31) / 32;  // slots per lane
 
 // A work item: events [e0, e1) of toy t.
 struct Tile {
@@ -275,37 +274,58 @@ struct Tile {
   int t, pad;
 };
 
-// Per-warp scratch of the data kernel.
-struct EnsWarp {
-  double pl[SLOT_ALL];                                   // the event's plane slots
-  double fac[2 * MAX_LSTAR + 2 * MAX_PC + MAX_PC * (MAX_PC + 1)];  // its factor row
-  cplx hz[MAX_PC][8];  // HZ_q[h]
-  cplx z[MAX_PC][8];   // d v / d conj(HZ_q[h])
-  cplx x[8];           // d v / d conj(H_L[h])
-  cplx yl[12];         // sum_ij conj(A_ijm) x[k, ij]
-  cplx yz[2 * MAX_PC * 12];
+// Per-warp scratch of the data kernel, laid out at run time for the model (offsets in doubles):
+// the event's plane slots pp / pp1 / pp2 (303), its factor row, HZ_q[h], d v / d conj(HZ_q[h]),
+// d v / d conj(H_L[h]), sum_ij conj(A_ijm) x[k, ij] (12 complex), sum_ij conj(AZ_ijm) z_q[k, ij].
+struct EnsScratch {
+  int pl, fac, hz, z, x, yl, yz, size;  // size: doubles per warp (a multiple of 2)
 };
+inline EnsScratch ens_scratch(int NR, int NZ) {
+  EnsScratch s;
+  const int nf = 2 * NR + 2 * NZ + NZ * (NZ + 1);
+  s.pl = 0;
+  s.fac = SLOT_PP3 + 1;  // 304: keeps the complex arrays 16-byte aligned
+  s.hz = s.fac + ((nf + 1) & ~1);
+  s.z = s.hz + 2 * 8 * NZ;
+  s.x = s.z + 2 * 8 * NZ;
+  s.yl = s.x + 16;
+  s.yz = s.yl + 24;
+  s.size = s.yz + 2 * 24 * NZ;
+  return s;
+}
 
-template <int WARPS>
-constexpr size_t ens_data_smem() {
-  return ((sizeof(PointTable) + 15) & ~size_t(15)) + (size_t)ENS_MAX_SLOTS * sizeof(cplx) + WARPS * sizeof(EnsWarp);
+constexpr int ENS_PV = (SLOT_PP3 + 31) / 32;  // plane values per lane (prefetch)
+constexpr int ENS_FV = (2 * MAX_LSTAR + 2 * MAX_PC + MAX_PC * (MAX_PC + 1) + 31) / 32;  // factor values per lane
+
+__host__ __device__ inline size_t ens_data_smem(int warps, int n_slot, const EnsScratch& sc) {
+  return ((sizeof(PointTable) + 15) & ~size_t(15)) + (size_t)n_slot * sizeof(cplx) +
+         (size_t)warps * sc.size * sizeof(double);
 }
 
 // Persistent blocks take tiles from *next; per tile the block loads the toy's slot couplings and each
-// warp evaluates one event at a time.  Per toy: val[t] += sum sw ln v (-1e12 for v <= 0, as the
-// reference), bad[t] counts events with v <= 0 or not finite, grad[t][s] += sum (sw / v) dv/dconj(c_s).
-template <int WARPS>
+// warp evaluates one event at a time, the next event's plane slots and factors already on their way
+// into registers.  Per toy: val[t] += sum sw ln v (-1e12 for v <= 0, as the reference), bad[t] counts
+// events with v <= 0 or not finite, grad[t][s] += sum (sw / v) dv/dconj(c_s).  SPL: slots per lane
+// (n_slot <= 32 SPL).
+template <int WARPS, int SPL>
 __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __restrict__ gtab, EventSet ev,
                                                          const double* __restrict__ fac, int64_t ld,
                                                          const Tile* __restrict__ tiles, int n_tiles, int* next,
                                                          const cplx* __restrict__ coup, const int* __restrict__ on,
-                                                         int n_slot, double* val, cplx* grad,
+                                                         int n_slot, EnsScratch sc, double* val, cplx* grad,
                                                          unsigned long long* bad) {
   extern __shared__ __align__(16) unsigned char sm[];
   PointTable& T = *reinterpret_cast<PointTable*>(sm);
   load_table<WARPS * 32>(gtab, &T);
   cplx* c = reinterpret_cast<cplx*>(sm + ((sizeof(PointTable) + 15) & ~size_t(15)));
-  EnsWarp& W = reinterpret_cast<EnsWarp*>(c + ENS_MAX_SLOTS)[threadIdx.x / 32];
+  double* wb = reinterpret_cast<double*>(c + n_slot) + (size_t)(threadIdx.x / 32) * sc.size;
+  double* pl = wb + sc.pl;
+  double* fr = wb + sc.fac;
+  cplx* whz = reinterpret_cast<cplx*>(wb + sc.hz);  // [q][8]
+  cplx* wz = reinterpret_cast<cplx*>(wb + sc.z);    // [q][8]
+  cplx* wx = reinterpret_cast<cplx*>(wb + sc.x);    // [8]
+  cplx* wyl = reinterpret_cast<cplx*>(wb + sc.yl);  // [12]
+  cplx* wyz = reinterpret_cast<cplx*>(wb + sc.yz);  // [24 NZ]
   __shared__ int tile_id;
   const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
   const int h = lane & 7, part = lane >> 3;
@@ -313,6 +333,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
   const int NR = T.NR, NZ = T.NZ, NS = 6 * NR + 12 * NZ;
   const FactorLayout F{NR, NZ};
   const int nf = F.size(false);
+  float pv[ENS_PV];
+  double fv[ENS_FV];
+  float swv = 0;
+  auto fetch = [&](int64_t e) {
+#pragma unroll
+    for (int i = 0; i < ENS_PV; ++i) {
+      const int j = lane + 32 * i;
+      const float* src = j < SLOT_PP1 ? ev.pp + (size_t)j * ev.n_size
+                                      : (j < SLOT_PP2 ? ev.pp1 + (size_t)(j - SLOT_PP1) * ev.n_size
+                                                      : ev.pp2 + (size_t)(j - SLOT_PP2) * ev.n_size);
+      pv[i] = j < SLOT_PP3 ? __ldg(src + e) : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < ENS_FV; ++i) {
+      const int f = lane + 32 * i;
+      fv[i] = f < nf ? __ldg(fac + (size_t)f * ld + e) : 0.0;
+    }
+    swv = __ldg(ev.sw + e);
+  };
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) tile_id = atomicAdd(next, 1);
@@ -323,23 +362,23 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
     if (!on[tl.t]) continue;
     for (int s = threadIdx.x; s < n_slot; s += WARPS * 32) c[s] = coup[(size_t)tl.t * n_slot + s];
     __syncthreads();
-    cplx acc[ENS_SPL];
+    cplx acc[SPL];
 #pragma unroll
-    for (int j = 0; j < ENS_SPL; ++j) acc[j] = mk(0, 0);
+    for (int j = 0; j < SPL; ++j) acc[j] = mk(0, 0);
     double value = 0;
     unsigned long long nbad = 0;
+    if (tl.e0 + warp < tl.e1) fetch(tl.e0 + warp);
     for (int64_t e = tl.e0 + warp; e < tl.e1; e += WARPS) {
-      // every plane slot of pp, pp1, pp2: a fit moves couplings that are zero at the set-up point too,
-      // so the point table's own staging list (its non-zero helicity slots) is not enough here
-      for (int j = lane; j < SLOT_PP3; j += 32) {
-        const float* src = j < SLOT_PP1 ? ev.pp + (size_t)j * ev.n_size
-                                        : (j < SLOT_PP2 ? ev.pp1 + (size_t)(j - SLOT_PP1) * ev.n_size
-                                                        : ev.pp2 + (size_t)(j - SLOT_PP2) * ev.n_size);
-        W.pl[j] = (double)__ldg(src + e);
-      }
-      for (int f = lane; f < nf; f += 32) W.fac[f] = fac[(size_t)f * ld + e];
+#pragma unroll
+      for (int i = 0; i < ENS_PV; ++i)
+        if (lane + 32 * i < SLOT_PP3) pl[lane + 32 * i] = (double)pv[i];
+#pragma unroll
+      for (int i = 0; i < ENS_FV; ++i)
+        if (lane + 32 * i < nf) fr[lane + 32 * i] = fv[i];
+      const double sw = (double)swv;
       __syncwarp();
-      const EvS E{W.pl};
+      if (e + WARPS < tl.e1) fetch(e + WARPS);  // the next event's loads overlap this event's work
+      const EvS E{pl};
       // H_L[h]: lane (h, part) sums the Lambda* r = part mod 4
       cplx hl = mk(0, 0);
       for (int r = part; r < NR; r += 4) {
@@ -348,7 +387,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
         cplx f = mk(0, 0);
 #pragma unroll
         for (int m = 0; m < 6; ++m) cmac(f, cr[m], E.A(hi, hj, m) * E.DL(sidx, hk, m));
-        cmac(hl, mk(W.fac[F.l() + 2 * r], W.fac[F.l() + 2 * r + 1]), f);
+        cmac(hl, mk(fr[F.l() + 2 * r], fr[F.l() + 2 * r + 1]), f);
       }
       hl += shfl_xor(hl, 8);
       hl += shfl_xor(hl, 16);
@@ -358,26 +397,26 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
         cplx f = mk(0, 0);
 #pragma unroll
         for (int m = 0; m < 12; ++m) cmac(f, cq[m], E.AZ(hi, hj, m) * E.DZ(sidx, hk, m));
-        W.hz[q][h] = f;
+        whz[q * 8 + h] = f;
       }
       __syncwarp();
       double vp = 0;
       if (part == 0) {
         cplx sx = mk(0, 0);
-        for (int q = 0; q < NZ; ++q) cmac(sx, mk(W.fac[F.s1() + 2 * q], W.fac[F.s1() + 2 * q + 1]), W.hz[q][h]);
+        for (int q = 0; q < NZ; ++q) cmac(sx, mk(fr[F.s1() + 2 * q], fr[F.s1() + 2 * q + 1]), whz[q * 8 + h]);
         vp = norm2(hl) + 2.0 * (hl.re * sx.re + hl.im * sx.im);
-        W.x[h] = hl + sx;
+        wx[h] = hl + sx;
       }
       for (int q = part; q < NZ; q += 4) {
         cplx tq = mk(0, 0);
         for (int p = 0; p < NZ; ++p) {
           const int o = F.s2() + 2 * (q <= p ? tri(q, p, NZ) : tri(p, q, NZ));
-          const cplx s2 = q <= p ? mk(W.fac[o], W.fac[o + 1]) : mk(W.fac[o], -W.fac[o + 1]);
-          cmac(tq, s2, W.hz[p][h]);
+          const cplx s2 = q <= p ? mk(fr[o], fr[o + 1]) : mk(fr[o], -fr[o + 1]);
+          cmac(tq, s2, whz[p * 8 + h]);
         }
-        const cplx hz = W.hz[q][h];
+        const cplx hz = whz[q * 8 + h];
         vp += hz.re * tq.re + hz.im * tq.im;
-        W.z[q][h] = conj(mk(W.fac[F.s1() + 2 * q], W.fac[F.s1() + 2 * q + 1])) * hl + tq;
+        wz[q * 8 + h] = conj(mk(fr[F.s1() + 2 * q], fr[F.s1() + 2 * q + 1])) * hl + tq;
       }
       const double v = warp_sum(vp);
       __syncwarp();
@@ -386,34 +425,34 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
         if (t < 12) {
           const int k = t / 6, m = t % 6;
 #pragma unroll
-          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.A(ij >> 1, ij & 1, m)), W.x[(ij << 1) | k]);
-          W.yl[t] = y;
+          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.A(ij >> 1, ij & 1, m)), wx[(ij << 1) | k]);
+          wyl[t] = y;
         } else {
           const int u = t - 12, k = u / (12 * NZ), q = (u / 12) % NZ, m = u % 12;
 #pragma unroll
-          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.AZ(ij >> 1, ij & 1, m)), W.z[q][(ij << 1) | k]);
-          W.yz[u] = y;
+          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.AZ(ij >> 1, ij & 1, m)), wz[q * 8 + ((ij << 1) | k)]);
+          wyz[u] = y;
         }
       }
       __syncwarp();
-      const double sw = (double)__ldg(ev.sw + e);
       const bool good = v > 0 && isfinite(v);
       const double scale = good ? sw / v : 0.0;
 #pragma unroll
-      for (int j = 0; j < ENS_SPL; ++j) {
+      for (int j = 0; j < SPL; ++j) {
         const int s = lane + 32 * j;
-        if (s >= n_slot) break;
-        const int k = s / NS, u = s % NS;
-        cplx g;
-        if (u < 6 * NR) {
-          const int r = u / 6, m = u % 6;
-          const cplx L = mk(W.fac[F.l() + 2 * r], W.fac[F.l() + 2 * r + 1]);
-          g = conj(L * E.DL(T.L[r].sidx, k, m)) * W.yl[k * 6 + m];
-        } else {
-          const int q = (u - 6 * NR) / 12, m = (u - 6 * NR) % 12;
-          g = W.yz[(k * NZ + q) * 12 + m] * E.DZ(T.Z[T.order[q]].sidx, k, m);
+        if (s < n_slot) {
+          const int k = s / NS, u = s % NS;
+          cplx g;
+          if (u < 6 * NR) {
+            const int r = u / 6, m = u % 6;
+            const cplx L = mk(fr[F.l() + 2 * r], fr[F.l() + 2 * r + 1]);
+            g = conj(L * E.DL(T.L[r].sidx, k, m)) * wyl[k * 6 + m];
+          } else {
+            const int q = (u - 6 * NR) / 12, m = (u - 6 * NR) % 12;
+            g = wyz[(k * NZ + q) * 12 + m] * E.DZ(T.Z[T.order[q]].sidx, k, m);
+          }
+          cmac(acc[j], mk(scale, 0), g);
         }
-        cmac(acc[j], mk(scale, 0), g);
       }
       if (lane == 0) {
         value += v > 0 ? log(v) * sw : -1e12;
@@ -422,11 +461,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
       __syncwarp();
     }
 #pragma unroll
-    for (int j = 0; j < ENS_SPL; ++j) {
+    for (int j = 0; j < SPL; ++j) {
       const int s = lane + 32 * j;
-      if (s >= n_slot) break;
-      atomicAdd(&grad[(size_t)tl.t * n_slot + s].re, acc[j].re);
-      atomicAdd(&grad[(size_t)tl.t * n_slot + s].im, acc[j].im);
+      if (s < n_slot) {
+        atomicAdd(&grad[(size_t)tl.t * n_slot + s].re, acc[j].re);
+        atomicAdd(&grad[(size_t)tl.t * n_slot + s].im, acc[j].im);
+      }
     }
     if (lane == 0) {
       atomicAdd(val + tl.t, value);
@@ -770,13 +810,38 @@ int ens_tiles(pwa_ens* s) {
   return PWA_OK;
 }
 
-template <int W>
-cudaError_t launch_data(pwa_ens* s) {
+// Kernel instance for a launch shape and slot count (slots per lane 8, 12, 16 or 21).
+template <int W, int SPL>
+cudaError_t data_t(pwa_ens* s, bool launch, size_t smem, int* occ) {
+  if (!launch) {
+    cudaError_t e = cudaFuncSetAttribute(k_ens_data<W, SPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k_ens_data<W, SPL>, W * 32, smem);
+    return e;
+  }
   const EventSet ev{s->cv.pp, s->cv.pp1, s->cv.pp2, s->cv.sw, s->cv.n_size, s->cv.n, s->cv.nda};
-  const size_t smem = ens_data_smem<W>();
-  k_ens_data<W><<<s->blocks, W * 32, smem, s->st>>>(s->d_T, ev, s->d_fac, s->ld, s->d_tiles, s->n_tiles, s->d_next,
-                                                    s->d_coup, s->d_on, s->n_slot, s->d_val, s->d_grad, s->d_bad);
+  k_ens_data<W, SPL><<<s->blocks, W * 32, smem, s->st>>>(s->d_T, ev, s->d_fac, s->ld, s->d_tiles, s->n_tiles,
+                                                         s->d_next, s->d_coup, s->d_on, s->n_slot,
+                                                         ens_scratch(s->NR, s->NZ), s->d_val, s->d_grad, s->d_bad);
   return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t data_w(pwa_ens* s, bool launch, size_t smem, int* occ) {
+  const int spl = (s->n_slot + 31) / 32;
+  if (spl <= 8) return data_t<W, 8>(s, launch, smem, occ);
+  if (spl <= 12) return data_t<W, 12>(s, launch, smem, occ);
+  if (spl <= 16) return data_t<W, 16>(s, launch, smem, occ);
+  return data_t<W, 21>(s, launch, smem, occ);
+}
+
+// Configures (launch = false: shared-memory size, occupancy into *occ) or launches the data kernel.
+cudaError_t data_kernel(pwa_ens* s, bool launch, int* occ = nullptr) {
+  const size_t smem = ens_data_smem(s->warps, s->n_slot, ens_scratch(s->NR, s->NZ));
+  switch (s->warps) {
+    case 4: return data_w<4>(s, launch, smem, occ);
+    case 8: return data_w<8>(s, launch, smem, occ);
+    default: return data_w<16>(s, launch, smem, occ);
+  }
 }
 
 // Captures one ensemble step (inputs in, both kernels, results out) into a CUDA graph.
@@ -795,7 +860,7 @@ int ens_capture(pwa_ens* s) {
   cudaMemsetAsync(s->d_bad, 0, s->n_toys * sizeof(unsigned long long), s->st);
   cudaMemsetAsync(s->d_grad, 0, nc * sizeof(cplx), s->st);
   cudaMemsetAsync(s->d_next, 0, sizeof(int), s->st);
-  cudaError_t le = s->warps == 4 ? launch_data<4>(s) : launch_data<8>(s);
+  cudaError_t le = data_kernel(s, true);
   k_ens_finish<<<s->n_toys, 256, 0, s->st>>>(s->n_slot, s->d_M, s->d_Mn, s->d_coup, s->d_on, s->d_val, s->d_grad,
                                              s->d_wdata, s->w_mc, s->shift, s->d_out, s->d_gout);
   cudaMemcpyAsync(s->h_out, s->d_out, 4 * s->n_toys * sizeof(double), cudaMemcpyDeviceToHost, s->st);
@@ -947,18 +1012,13 @@ int pwa_ens_gram(const pwa_ens* s, double* h_M, double* h_Mn) {
 }
 
 int pwa_ens_set_launch(pwa_ens* s, int warps, int tile_events) {
-  if (!s || (warps != 4 && warps != 8) || tile_events < 32) return PWA_E_ARG;
+  if (!s || (warps != 4 && warps != 8 && warps != 16) || tile_events < 32) return PWA_E_ARG;
   cudaError_t e = cudaSetDevice(s->cv.device);
   if (e) return cuda_fail(e);
   s->warps = warps;
   s->tile_events = tile_events;
-  const size_t smem = warps == 4 ? ens_data_smem<4>() : ens_data_smem<8>();
-  e = warps == 4 ? cudaFuncSetAttribute(k_ens_data<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                 : cudaFuncSetAttribute(k_ens_data<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 1;
-  if (e == cudaSuccess)
-    e = warps == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_data<4>, 128, smem)
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_data<8>, 256, smem);
+  e = data_kernel(s, false, &occ);
   if (e) return cuda_fail(e);
   s->blocks = s->cv.sm_count * std::max(occ, 1);
   if (s->graph) {

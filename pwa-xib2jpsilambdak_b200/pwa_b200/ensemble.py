@@ -286,7 +286,7 @@ class Ensemble:
 
 
 # ------------------------------------------------------------------ autotuner
-CANDIDATES = [(8, 256), (8, 1024), (8, 4096), (4, 256), (4, 1024), (4, 4096)]
+CANDIDATES = [(16, 256), (16, 1024), (16, 4096), (8, 256), (8, 1024), (8, 4096), (4, 256), (4, 1024)]
 
 
 def _cache_path() -> Path:
