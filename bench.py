@@ -474,6 +474,7 @@ def profile_case(name: str, device: int = 0) -> int:
         ctx.bind_device(ens.sample)
         ctx.set_smearing("gauss", 0.0027, 0.0005, 17)
         E = ensemble.Ensemble(ctx, ens, mdl, vals, ensemble.coupling_names(mdl))
+        ensemble.autotune(E)  # the launch shape the bench uses for this device and ensemble shape
         S = np.repeat(E.s0[None, :], E.n_toys, axis=0)
         for _ in range(3):
             E.eval_slots(S)

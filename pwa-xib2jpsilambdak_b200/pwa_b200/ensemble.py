@@ -246,40 +246,46 @@ class Ensemble:
             V[t] = (U / np.maximum(np.abs(w), floor)) @ U.T
         edm = 0.5 * np.einsum("ti,tij,tj->t", g, V, g)
         it = np.zeros(T, int)
-        conv = edm < 0.002 * tolerance * up
+        crit = 0.002 * tolerance * up
+        conv = edm < crit
         alpha = np.ones(T)
-        D = np.zeros((T, P))
+        D = -np.einsum("tij,tj->ti", V, g)
         busy = active & ~conv
-        for t in np.flatnonzero(busy):
-            D[t] = -V[t] @ g[t]
         while busy.any():
             Xt = X + alpha[:, None] * D
             ft, gt = self.fcn_grad(np.where(busy[:, None], Xt, X), busy)
             calls += 1
             dev_ms += self.last_ms()
-            for t in np.flatnonzero(busy):
-                slope = g[t] @ D[t]
-                if np.isfinite(ft[t]) and ft[t] <= f[t] + 1e-4 * alpha[t] * slope:
-                    s, y = Xt[t] - X[t], gt[t] - g[t]
-                    sy = s @ y
-                    if sy > 1e-300:
-                        rho = 1.0 / sy
-                        Id = np.eye(P)
-                        V[t] = (Id - rho * np.outer(s, y)) @ V[t] @ (Id - rho * np.outer(y, s)) + rho * np.outer(s, s)
-                    X[t], f[t], g[t] = Xt[t], ft[t], gt[t]
-                    it[t] += 1
-                    edm[t] = 0.5 * g[t] @ V[t] @ g[t]
-                    conv[t] = edm[t] < 0.002 * tolerance * up
-                    alpha[t] = 1.0
+            slope = np.einsum("ti,ti->t", g, D)
+            ok = busy & np.isfinite(ft) & (ft <= f + 1e-4 * alpha * slope)
+            fail = busy & ~ok
+            a = np.flatnonzero(ok)
+            if len(a):
+                # BFGS update of the inverse Hessians of the accepted toys, all at once
+                sv, yv = Xt[a] - X[a], gt[a] - g[a]
+                sy = np.einsum("ti,ti->t", sv, yv)
+                upd = sy > 1e-300
+                rho = np.where(upd, 1.0 / np.where(upd, sy, 1.0), 0.0)
+                Va = V[a]
+                Vy = np.einsum("tij,tj->ti", Va, yv)
+                yVy = np.einsum("ti,ti->t", yv, Vy)
+                Va = (Va - rho[:, None, None] * (sv[:, :, None] * Vy[:, None, :] + Vy[:, :, None] * sv[:, None, :])
+                      + (rho * rho * yVy + rho)[:, None, None] * sv[:, :, None] * sv[:, None, :])
+                V[a] = Va
+                X[a], f[a], g[a] = Xt[a], ft[a], gt[a]
+                it[a] += 1
+                edm[a] = 0.5 * np.einsum("ti,tij,tj->t", g[a], V[a], g[a])
+                conv[a] = edm[a] < crit
+                alpha[a] = 1.0
+                D[a] = -np.einsum("tij,tj->ti", V[a], g[a])
+                bad = a[np.einsum("ti,ti->t", g[a], D[a]) >= 0]  # not a descent direction: restart the metric
+                for t in bad:
+                    V[t] = np.diag(np.abs(np.diag(V[t])))
                     D[t] = -V[t] @ g[t]
-                    if g[t] @ D[t] >= 0:  # not a descent direction: restart the metric
-                        V[t] = np.diag(np.abs(np.diag(V[t])))
-                        D[t] = -V[t] @ g[t]
-                else:
-                    alpha[t] *= 0.3
-                    if alpha[t] < 1e-10:  # no descent along the metric: at the precision limit
-                        conv[t] = edm[t] < 1e3 * 0.002 * tolerance * up
-                        it[t] = max_iter
+            alpha[fail] *= 0.3
+            stuck = fail & (alpha < 1e-10)  # no descent along the metric: at the precision limit
+            conv[stuck] = edm[stuck] < 1e3 * crit
+            it[stuck] = max_iter
             busy = active & ~conv & (it < max_iter)
         err = np.sqrt(np.maximum(2 * up * np.einsum("tii->ti", V), 0))
         return EnsembleFit(X, f, err, edm, it, conv & active, calls, dev_ms)
