@@ -305,7 +305,7 @@ int pwa_ens_slots(const float* h_paraList, int para_size, int vamp_size, int spl
                   float FFR, float FFB, double* h_slots);
 /* The Gram matrices M and Mn (non-interference sum), row-major slot x slot complex (Re, Im doubles). */
 int pwa_ens_gram(const pwa_ens* ens, double* h_M, double* h_Mn);
-/* Launch shape of the per-call kernel: warps per block (4, 8 or 16) and events per work item; the
+/* Launch shape of the per-call kernel: warps per block (4, 8, 12 or 16) and events per work item; the
  * project's autotuner (pwa_b200.ensemble.autotune) picks them by timing. */
 int pwa_ens_set_launch(pwa_ens* ens, int warps, int tile_events);
 /* One evaluation of every toy t with on[t] != 0 (on null: all) at its slot vector h_slots[t] ([n_toys]

@@ -297,9 +297,14 @@ inline EnsScratch ens_scratch(int NR, int NZ) {
 constexpr int ENS_PV = (SLOT_PP3 + 31) / 32;  // plane values per lane (prefetch)
 constexpr int ENS_FV = (2 * MAX_LSTAR + 2 * MAX_PC + MAX_PC * (MAX_PC + 1) + 31) / 32;  // factor values per lane
 
-__host__ __device__ inline size_t ens_data_smem(int warps, int n_slot, const EnsScratch& sc) {
+// Index descriptors the data kernel builds once per block: per slot, the plane slot of its angular
+// factor (DL or DZ; bit 30 set for a Pc slot) and its factor-row / y indices; per y entry (12 Lambda*
+// + 24 NZ Pc), the plane slot of A_00m or AZ_00m (bit 30 set for Pc) and the x / z base it contracts.
+__host__ __device__ inline int ens_desc_count(int n_slot, int NZ) { return (n_slot + 12 + 24 * NZ + 1) & ~1; }
+
+__host__ __device__ inline size_t ens_data_smem(int warps, int n_slot, int NZ, const EnsScratch& sc) {
   return ((sizeof(PointTable) + 15) & ~size_t(15)) + (size_t)n_slot * sizeof(cplx) +
-         (size_t)warps * sc.size * sizeof(double);
+         (size_t)ens_desc_count(n_slot, NZ) * sizeof(int2) + (size_t)warps * sc.size * sizeof(double);
 }
 
 // Persistent blocks take tiles from *next; per tile the block loads the toy's slot couplings and each
@@ -318,7 +323,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
   PointTable& T = *reinterpret_cast<PointTable*>(sm);
   load_table<WARPS * 32>(gtab, &T);
   cplx* c = reinterpret_cast<cplx*>(sm + ((sizeof(PointTable) + 15) & ~size_t(15)));
-  double* wb = reinterpret_cast<double*>(c + n_slot) + (size_t)(threadIdx.x / 32) * sc.size;
+  int2* sdesc = reinterpret_cast<int2*>(c + n_slot);  // [n_slot] then the y entries
+  int2* ydesc = sdesc + n_slot;
+  double* wb = reinterpret_cast<double*>(sdesc + ens_desc_count(n_slot, T.NZ)) + (size_t)(threadIdx.x / 32) * sc.size;
   double* pl = wb + sc.pl;
   double* fr = wb + sc.fac;
   cplx* whz = reinterpret_cast<cplx*>(wb + sc.hz);  // [q][8]
@@ -333,6 +340,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
   const int NR = T.NR, NZ = T.NZ, NS = 6 * NR + 12 * NZ;
   const FactorLayout F{NR, NZ};
   const int nf = F.size(false);
+  for (int s = threadIdx.x; s < n_slot; s += WARPS * 32) {
+    const int k = s / NS, u = s % NS;
+    if (u < 6 * NR) {
+      const int r = u / 6, m = u % 6;
+      sdesc[s] = make_int2(51 + T.L[r].sidx * 12 + k * 6 + m, (F.l() + 2 * r) | ((k * 6 + m) << 16));
+    } else {
+      const int q = (u - 6 * NR) / 12, m = (u - 6 * NR) % 12;
+      sdesc[s] = make_int2((SLOT_PP2 + T.Z[T.order[q]].sidx * 24 + k * 12 + m) | (1 << 30), (k * NZ + q) * 12 + m);
+    }
+  }
+  for (int t = threadIdx.x; t < 12 + 24 * NZ; t += WARPS * 32) {
+    if (t < 12) {
+      ydesc[t] = make_int2(3 + 2 * (t % 6), t / 6);
+    } else {
+      const int u = t - 12, k = u / (12 * NZ), q = (u / 12) % NZ, m = u % 12;
+      ydesc[t] = make_int2((SLOT_PP1 + 2 * m) | (1 << 30), q * 8 + k);
+    }
+  }
+  // (made visible by the __syncthreads at the top of the tile loop)
   float pv[ENS_PV];
   double fv[ENS_FV];
   float swv = 0;
@@ -421,18 +447,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
       const double v = warp_sum(vp);
       __syncwarp();
       for (int t = lane; t < 12 + 24 * NZ; t += 32) {
+        // y = sum_ij conj(A_ijm) x[(ij << 1) | k]  (AZ and z_q for a Pc entry); A_ijm at base + 12 ij
+        // (AZ_ijm at base + 24 ij), x / z at xb + 2 ij
+        const int2 d = ydesc[t];
+        const bool pc = d.x >> 30;
+        const int base = d.x & 0xffff, step = pc ? 24 : 12;
+        const cplx* xz = pc ? wz : wx;
         cplx y = mk(0, 0);
-        if (t < 12) {
-          const int k = t / 6, m = t % 6;
 #pragma unroll
-          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.A(ij >> 1, ij & 1, m)), wx[(ij << 1) | k]);
-          wyl[t] = y;
-        } else {
-          const int u = t - 12, k = u / (12 * NZ), q = (u / 12) % NZ, m = u % 12;
-#pragma unroll
-          for (int ij = 0; ij < 4; ++ij) cmac(y, conj(E.AZ(ij >> 1, ij & 1, m)), wz[q * 8 + ((ij << 1) | k)]);
-          wyz[u] = y;
+        for (int ij = 0; ij < 4; ++ij) {
+          const int o = base + step * ij;
+          cmac(y, mk(pl[o], -pl[o + 1]), xz[d.y + 2 * ij]);
         }
+        if (pc)
+          wyz[t - 12] = y;
+        else
+          wyl[t] = y;
       }
       __syncwarp();
       const bool good = v > 0 && isfinite(v);
@@ -441,15 +471,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ens_data(const PointTable* __res
       for (int j = 0; j < SPL; ++j) {
         const int s = lane + 32 * j;
         if (s < n_slot) {
-          const int k = s / NS, u = s % NS;
+          const int2 d = sdesc[s];
+          const double ang = pl[d.x & 0xffff];
           cplx g;
-          if (u < 6 * NR) {
-            const int r = u / 6, m = u % 6;
-            const cplx L = mk(fr[F.l() + 2 * r], fr[F.l() + 2 * r + 1]);
-            g = conj(L * E.DL(T.L[r].sidx, k, m)) * wyl[k * 6 + m];
+          if (d.x >> 30) {
+            g = wyz[d.y] * ang;
           } else {
-            const int q = (u - 6 * NR) / 12, m = (u - 6 * NR) % 12;
-            g = wyz[(k * NZ + q) * 12 + m] * E.DZ(T.Z[T.order[q]].sidx, k, m);
+            const cplx L = mk(fr[d.y & 0xffff], fr[(d.y & 0xffff) + 1]);
+            g = conj(L * ang) * wyl[d.y >> 16];
           }
           cmac(acc[j], mk(scale, 0), g);
         }
@@ -836,10 +865,11 @@ cudaError_t data_w(pwa_ens* s, bool launch, size_t smem, int* occ) {
 
 // Configures (launch = false: shared-memory size, occupancy into *occ) or launches the data kernel.
 cudaError_t data_kernel(pwa_ens* s, bool launch, int* occ = nullptr) {
-  const size_t smem = ens_data_smem(s->warps, s->n_slot, ens_scratch(s->NR, s->NZ));
+  const size_t smem = ens_data_smem(s->warps, s->n_slot, s->NZ, ens_scratch(s->NR, s->NZ));
   switch (s->warps) {
     case 4: return data_w<4>(s, launch, smem, occ);
     case 8: return data_w<8>(s, launch, smem, occ);
+    case 12: return data_w<12>(s, launch, smem, occ);
     default: return data_w<16>(s, launch, smem, occ);
   }
 }
@@ -1012,7 +1042,7 @@ int pwa_ens_gram(const pwa_ens* s, double* h_M, double* h_Mn) {
 }
 
 int pwa_ens_set_launch(pwa_ens* s, int warps, int tile_events) {
-  if (!s || (warps != 4 && warps != 8 && warps != 16) || tile_events < 32) return PWA_E_ARG;
+  if (!s || (warps != 4 && warps != 8 && warps != 12 && warps != 16) || tile_events < 32) return PWA_E_ARG;
   cudaError_t e = cudaSetDevice(s->cv.device);
   if (e) return cuda_fail(e);
   s->warps = warps;

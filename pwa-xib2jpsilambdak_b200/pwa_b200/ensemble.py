@@ -292,7 +292,7 @@ class Ensemble:
 
 
 # ------------------------------------------------------------------ autotuner
-CANDIDATES = [(16, 256), (16, 1024), (16, 4096), (8, 256), (8, 1024), (8, 4096), (4, 256), (4, 1024)]
+CANDIDATES = [(16, 256), (16, 1024), (16, 4096), (12, 256), (12, 1024), (8, 256), (8, 1024), (4, 1024)]
 
 
 def _cache_path() -> Path:
