@@ -226,10 +226,14 @@ class Ensemble:
 
     def fit(self, X0=None, tolerance: float = 0.1, up: float = 0.5, max_iter: int = 300, toys=None) -> EnsembleFit:
         """Minimise every toy's FCN together: quasi-Newton (BFGS on the inverse Hessian) per toy, started
-        from the finite-difference Hessian of the analytic gradient (eigenvalues floored, so that the
-        first steps are Newton steps wherever the FCN is convex), a backtracking line search whose trial
-        points of all toys go into one evaluation, convergence per toy on EDM = g^T V g / 2 < 0.002
-        tolerance up (Migrad's criterion); errors sqrt(2 up V_ii)."""
+        from the finite-difference Hessian of the analytic gradient (eigenvalues floored by modulus, so
+        that the first steps are Newton steps wherever the FCN is convex), a backtracking line search
+        whose trial points of all toys go into one evaluation, convergence per toy on EDM = g^T V g / 2 <
+        0.002 tolerance up (Migrad's criterion); errors sqrt(2 up V_ii).  The toys' inverse Hessians are
+        updated together as one batched tensor (on the GPU when the ensemble has one)."""
+        import torch
+        dev = torch.device("cuda", getattr(self.ctx, "device", 0)) if (getattr(self, "h", None) and
+                                                                      torch.cuda.is_available()) else torch.device("cpu")
         T, P = self.n_toys, len(self.names)
         X = np.repeat(self.x0[None, :], T, axis=0) if X0 is None else np.array(X0, float)
         active = np.zeros(T, bool)
@@ -239,55 +243,65 @@ class Ensemble:
         H, c, ms = self.hessian(X, active)
         calls += c
         dev_ms += ms
-        V = np.zeros((T, P, P))
-        for t in np.flatnonzero(active):
-            w, U = np.linalg.eigh(H[t])
-            floor = 1e-8 * max(float(np.abs(w).max()), 1e-300)
-            V[t] = (U / np.maximum(np.abs(w), floor)) @ U.T
-        edm = 0.5 * np.einsum("ti,tij,tj->t", g, V, g)
-        it = np.zeros(T, int)
+        Ht = torch.as_tensor(H, dtype=torch.float64, device=dev)
+        w, U = torch.linalg.eigh(Ht)
+        floor = 1e-8 * torch.clamp(w.abs().amax(dim=1, keepdim=True), min=1e-300)
+        V = (U / torch.maximum(w.abs(), floor)[:, None, :]) @ U.transpose(1, 2)
+        tX = torch.as_tensor(X, dtype=torch.float64, device=dev)
+        tf = torch.as_tensor(f, dtype=torch.float64, device=dev)
+        tg = torch.as_tensor(g, dtype=torch.float64, device=dev)
+        tact = torch.as_tensor(active, device=dev)
         crit = 0.002 * tolerance * up
+        edm = 0.5 * torch.einsum("ti,tij,tj->t", tg, V, tg)
         conv = edm < crit
-        alpha = np.ones(T)
-        D = -np.einsum("tij,tj->ti", V, g)
-        busy = active & ~conv
-        while busy.any():
-            Xt = X + alpha[:, None] * D
-            ft, gt = self.fcn_grad(np.where(busy[:, None], Xt, X), busy)
+        it = torch.zeros(T, dtype=torch.int64, device=dev)
+        alpha = torch.ones(T, dtype=torch.float64, device=dev)
+        D = -torch.einsum("tij,tj->ti", V, tg)
+        busy = tact & ~conv
+        while bool(busy.any()):
+            Xt = tX + alpha[:, None] * D
+            b_np = busy.cpu().numpy()
+            ft_np, gt_np = self.fcn_grad(torch.where(busy[:, None], Xt, tX).cpu().numpy(), b_np)
             calls += 1
             dev_ms += self.last_ms()
-            slope = np.einsum("ti,ti->t", g, D)
-            ok = busy & np.isfinite(ft) & (ft <= f + 1e-4 * alpha * slope)
+            ft = torch.as_tensor(np.nan_to_num(ft_np, nan=np.inf), dtype=torch.float64, device=dev)
+            gt = torch.as_tensor(gt_np, dtype=torch.float64, device=dev)
+            slope = torch.einsum("ti,ti->t", tg, D)
+            ok = busy & torch.isfinite(ft) & (ft <= tf + 1e-4 * alpha * slope)
             fail = busy & ~ok
-            a = np.flatnonzero(ok)
-            if len(a):
-                # BFGS update of the inverse Hessians of the accepted toys, all at once
-                sv, yv = Xt[a] - X[a], gt[a] - g[a]
-                sy = np.einsum("ti,ti->t", sv, yv)
-                upd = sy > 1e-300
-                rho = np.where(upd, 1.0 / np.where(upd, sy, 1.0), 0.0)
-                Va = V[a]
-                Vy = np.einsum("tij,tj->ti", Va, yv)
-                yVy = np.einsum("ti,ti->t", yv, Vy)
-                Va = (Va - rho[:, None, None] * (sv[:, :, None] * Vy[:, None, :] + Vy[:, :, None] * sv[:, None, :])
-                      + (rho * rho * yVy + rho)[:, None, None] * sv[:, :, None] * sv[:, None, :])
-                V[a] = Va
-                X[a], f[a], g[a] = Xt[a], ft[a], gt[a]
-                it[a] += 1
-                edm[a] = 0.5 * np.einsum("ti,tij,tj->t", g[a], V[a], g[a])
-                conv[a] = edm[a] < crit
-                alpha[a] = 1.0
-                D[a] = -np.einsum("tij,tj->ti", V[a], g[a])
-                bad = a[np.einsum("ti,ti->t", g[a], D[a]) >= 0]  # not a descent direction: restart the metric
-                for t in bad:
-                    V[t] = np.diag(np.abs(np.diag(V[t])))
-                    D[t] = -V[t] @ g[t]
-            alpha[fail] *= 0.3
+            # BFGS update of the accepted toys' inverse Hessians (rho = 0 leaves the others as they are)
+            sv = torch.where(ok[:, None], Xt - tX, torch.zeros_like(tX))
+            yv = torch.where(ok[:, None], gt - tg, torch.zeros_like(tg))
+            sy = torch.einsum("ti,ti->t", sv, yv)
+            rho = torch.where(ok & (sy > 1e-300), 1.0 / torch.where(sy > 1e-300, sy, torch.ones_like(sy)),
+                              torch.zeros_like(sy))
+            Vy = torch.einsum("tij,tj->ti", V, yv)
+            yVy = torch.einsum("ti,ti->t", yv, Vy)
+            V = (V - rho[:, None, None] * (sv[:, :, None] * Vy[:, None, :] + Vy[:, :, None] * sv[:, None, :])
+                 + (rho * rho * yVy + rho)[:, None, None] * sv[:, :, None] * sv[:, None, :])
+            tX = torch.where(ok[:, None], Xt, tX)
+            tf = torch.where(ok, ft, tf)
+            tg = torch.where(ok[:, None], gt, tg)
+            it = it + ok.to(torch.int64)
+            edm_new = 0.5 * torch.einsum("ti,tij,tj->t", tg, V, tg)
+            edm = torch.where(ok, edm_new, edm)
+            conv = conv | (ok & (edm_new < crit))
+            alpha = torch.where(ok, torch.ones_like(alpha), alpha * torch.where(fail, 0.3, 1.0))
+            Dn = -torch.einsum("tij,tj->ti", V, tg)
+            # not a descent direction: restart that toy's metric from its diagonal
+            restart = ok & (torch.einsum("ti,ti->t", tg, Dn) >= 0)
+            if bool(restart.any()):
+                diag = torch.diag_embed(torch.diagonal(V, dim1=1, dim2=2).abs())
+                V = torch.where(restart[:, None, None], diag, V)
+                Dn = -torch.einsum("tij,tj->ti", V, tg)
+            D = torch.where(ok[:, None], Dn, D)
             stuck = fail & (alpha < 1e-10)  # no descent along the metric: at the precision limit
-            conv[stuck] = edm[stuck] < 1e3 * crit
-            it[stuck] = max_iter
-            busy = active & ~conv & (it < max_iter)
-        err = np.sqrt(np.maximum(2 * up * np.einsum("tii->ti", V), 0))
+            conv = conv | (stuck & (edm < 1e3 * crit))
+            it = torch.where(stuck, torch.full_like(it, max_iter), it)
+            busy = tact & ~conv & (it < max_iter)
+        X, f = tX.cpu().numpy(), tf.cpu().numpy()
+        edm, it, conv = edm.cpu().numpy(), it.cpu().numpy(), conv.cpu().numpy()
+        err = np.sqrt(np.maximum(2 * up * torch.diagonal(V, dim1=1, dim2=2).cpu().numpy(), 0))
         return EnsembleFit(X, f, err, edm, it, conv & active, calls, dev_ms)
 
 
