@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the toy-ensemble fit measurement")
+    ap.add_argument("--event-order", choices=["index", "mass"], default="index",
+                    help="walk each MC event class by event index or by m(J/psi p) (pwa_ctx_set_event_order)")
     ap.add_argument("--profile-case", choices=["flow_small", "ensemble_small"],
                     help="run one small case of a kernel for a profiler capture (no bench line)")
     ap.add_argument("--no-full-parity", action="store_true",
@@ -519,6 +521,7 @@ def main():
     if wl["smearing"]:
         ctx.set_smearing(*wl["smearing"])
     ctx.set_lineshape_tables(not args.exact)
+    ctx.set_event_order(args.event_order == "mass")
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     sums = torch.zeros(3, dtype=torch.float64, device=dev)
 
@@ -640,7 +643,8 @@ def main():
                       "parallelism": f"dp{world} event shards, NCCL all-reduce of 3 sums per step",
                       "l2": "inputs larger than L2 (events x 828 B >> 126 MB)", "precision": "plain FP64 path",
                       "lineshapes": "exact K-matrix solves" if args.exact else "FP64 K-matrix tables, exact near "
-                                                                               "thresholds"},
+                                                                               "thresholds",
+                      "event_order": args.event_order},
            "gpu_launches": launches,
            "kernel_shares": shares,
            "segments": {names[k]: {"events": int(n), "deferred_to_exact": int(seg_deferred.get(k, 0)),

@@ -176,6 +176,13 @@ int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double
  * the exact pass (lineshape masses the interpolation tables cannot serve).  No reference counterpart. */
 int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
 
+/* Order in which the kernels walk the MC events of each class under the reference's resolution model
+ * (the 20-offset windows and the unsmeared rest): 0 (default) by event index, so that neighbouring
+ * warps share the 32-byte sectors of the event planes; 1 by m(J/psi p), so that they read neighbouring
+ * nodes of the per-point lineshape tables (the batched gradient's points that move a K-matrix group
+ * each read their own table).  Results differ only by the order of the FP64 sums.  Re-splits the
+ * uploaded events.  No counterpart in the reference. */
+int pwa_ctx_set_event_order(pwa_ctx* ctx, int by_mass);
 /* K-matrix lineshape tables (default on): each evaluation first tabulates the exact FP64 K-matrix
  * outputs on a 10 keV m(J/psi p) grid and interpolates them (6-point Lagrange), evaluating exactly
  * near thresholds, branch switches and pole clamps.  Off: every lookup solves the K-matrix. */

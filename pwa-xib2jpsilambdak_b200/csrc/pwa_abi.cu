@@ -80,6 +80,8 @@ struct pwa_ctx {
   int last_launches = 0;
   // K-matrix lineshape tables (on by default)
   int use_tables = 1;
+  // order of the per-class event lists (MC window / tail): 1 by m(J/psi p), 0 by event index
+  int mass_order = 0;
   void* d_tab = nullptr;  // TAB_BYTES of two-level lineshape tables
   // optional per-segment timing
   int timing = 0;
@@ -210,6 +212,12 @@ int build_reference_segments(pwa_ctx* c, const float* h_mz) {
     const int64_t r0 = f + std::min(wn, std::max<int64_t>(0, c->nda_smr + c->nda_fine));
     for (int64_t e = r0; e < f + wn; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
     for (int64_t e = c->nda; e < n; ++e) (in_window(h_mz[e]) ? lw : lu).push_back((int32_t)e);
+  }
+  if (c->mass_order) {
+    // neighbouring list positions then read neighbouring nodes of the lineshape tables
+    auto by_mass = [&](int32_t x, int32_t y) { return h_mz[x] < h_mz[y]; };
+    std::stable_sort(lw.begin(), lw.end(), by_mass);
+    std::stable_sort(lu.begin(), lu.end(), by_mass);
   }
   const size_t nl = lw.size() + lu.size();
   if (nl) {
@@ -440,6 +448,17 @@ int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int ha
   c->smear_mode = mode;
   if (!c->pp) return PWA_OK;
   // re-split the uploaded events for the new model
+  free_segments(c);
+  std::vector<float> mz((size_t)std::max<int64_t>(c->n, 1));
+  if (c->n) PWA_CUDA(cudaMemcpy(mz.data(), c->pp + c->n_size, c->n * sizeof(float), cudaMemcpyDeviceToHost));
+  return build_segments(c, mz.data());
+}
+
+int pwa_ctx_set_event_order(pwa_ctx* c, int by_mass) {
+  if (!c) return PWA_E_ARG;
+  c->mass_order = by_mass ? 1 : 0;
+  if (!c->pp) return PWA_OK;
+  PWA_CUDA(cudaSetDevice(c->device));
   free_segments(c);
   std::vector<float> mz((size_t)std::max<int64_t>(c->n, 1));
   if (c->n) PWA_CUDA(cudaMemcpy(mz.data(), c->pp + c->n_size, c->n * sizeof(float), cudaMemcpyDeviceToHost));

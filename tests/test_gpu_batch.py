@@ -106,3 +106,20 @@ def test_gradient_batch_with_zcs_entries(ctx):
     # (a Zcs coupling that only fills slots the reference kernel does not read leaves the point equal to
     # the centre, so such points are formed from it as well)
     assert n_zcs > 0 and len(blocks) - n_zcs <= nstruct < len(blocks), (nstruct, len(blocks), n_zcs)
+
+
+def test_mass_ordered_event_lists(ctx):
+    """Walking the MC classes by m(J/psi p) (pwa_ctx_set_event_order) changes only the order of the
+    sums: single points and the gradient batch equal the index-ordered results."""
+    from pwa_b200 import gradient
+    mdl, vals, blk, smp = make_test_sample("kmatrix", 1200, 12000)
+    ctx.upload(smp)
+    labels, blocks = gradient.gradient_blocks(mdl, vals)
+    ref, _ = ctx.eval_nll_batch(blocks)
+    ctx.set_event_order(True)
+    try:
+        res, _ = ctx.eval_nll_batch(blocks)
+        assert np.max(np.abs(np.array([r.nll for r in res]) - [r.nll for r in ref])) < NLL_TOL
+        assert abs(ctx.eval_nll(blk).nll - ref[0].nll) < NLL_TOL
+    finally:
+        ctx.set_event_order(False)
