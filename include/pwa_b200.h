@@ -176,6 +176,18 @@ int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double
  * the exact pass (lineshape masses the interpolation tables cannot serve).  No reference counterpart. */
 int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
 
+/* Coupled-channel K-matrix of the context's evaluations.  PWA_KMATRIX_DEFAULT: 4 channels (J/psi p,
+ * Sigma_c D*, Sigma_c* D*, Sigma_c D; Default_KMatrix, cu_DPFPropogator.cu:588-813).
+ * PWA_KMATRIX_ISOSPIN: the 7-channel isospin split of the reference's ISOSPIN_SIGMACD build
+ * (Isospin_KMatrix, :384-586): charged and neutral partners of each Sigma_c(*) D(*) channel with their
+ * own masses and Sigma_c(*) widths, couplings and scattering terms spread with the isospin factors
+ * sqrt(2/3) and -sqrt(1/3), and poles of channels 1 and 3 shifted by Re(i g^2 (2 rho_charged +
+ * rho_neutral) / 3).  The reference selects it at compile time; here it is a run-time switch of the
+ * context (the allocation-free entry point and the reference-signature functions use the default). */
+#define PWA_KMATRIX_DEFAULT 0
+#define PWA_KMATRIX_ISOSPIN 1
+int pwa_ctx_set_kmatrix(pwa_ctx* ctx, int kmatrix);
+
 /* Order in which the kernels walk the MC events of each class under the reference's resolution model
  * (the 20-offset windows and the unsmeared rest): 0 (default) by event index, so that neighbouring
  * warps share the 32-byte sectors of the event planes; 1 by m(J/psi p), so that they read neighbouring
@@ -201,6 +213,10 @@ int pwa_ctx_last_launches(pwa_ctx* ctx);
  * K-matrix lineshapes. */
 int pwa_host_lineshapes(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
                         int NX, float FFR, float FFB, double mkp, double mz, double* lstar, double* pc);
+/* The same with a K-matrix variant (PWA_KMATRIX_DEFAULT or PWA_KMATRIX_ISOSPIN). */
+int pwa_host_lineshapes_km(const float* h_paraList, int para_size, int vamp_size, int spline_size, int NR, int NZ,
+                           int NX, float FFR, float FFB, int kmatrix, double mkp, double mz, double* lstar,
+                           double* pc);
 
 /* Lambda* lineshape diagnostic on the device (replaces host_store_lineshapeLsKM,
  * RooTDalitz/kernel_calEva.h:27, src/kernel_calEva.cu:1490-1584): for every Lambda* entry r < NR of the

@@ -13,6 +13,10 @@ Recipe (no reference source is copied into the repository; all output goes to or
   The model sizes of ``RooTDalitz/NDefine.h`` are compile-time constants in the reference, so each
   (NR, NZ, NX, max_ikmcount) bucket gets its own generated NDefine.h; every other reference header
   is used in place through symlinks.  The generated source is deleted after compilation.
+* The isospin-split K-matrix is the reference's compile-time switch ``ISOSPIN_SIGMACD``
+  (``RooTDalitz/Resonances.h:17``): its buckets (``libref_iso_*.so``) get a generated Resonances.h with
+  the switch on, and ``cu_DPFPropogator.cu`` is then compiled from a generated translation unit beside
+  it (same text) so that its relative includes find that header.
 * ``oracle/ref_host/driver.cpp`` (this repository's code) adds C entry points.
 
 The result, ``oracle/_ref/libref_<NR>_<NZ>_<NX>_<IKM>.so``, runs the reference's FP32 arithmetic
@@ -49,17 +53,23 @@ CUDA_INC = "/usr/local/cuda/include"
 DEFAULT_BUCKETS = [(6, 0, 0, 6), (6, 12, 0, 6), (14, 3, 0, 6), (3, 4, 0, 6), (2, 2, 0, 6), (2, 1, 2, 6),
                    (5, 5, 0, 6)]
 
+# The isospin-split K-matrix variant is built for the small K-matrix test model's bucket.
+ISOSPIN_BUCKETS = [(3, 4, 0, 6)]
+
 LAUNCH_RE = re.compile(r"(\b\w+)<<<\s*([^,>]+?)\s*,\s*([^>]+?)\s*>>>\s*\(")
 COUPLING_RE = re.compile(
     r"make_cuFloatComplex\(\s*_constant_paraList\[ampcount\+\+\]\s*,\s*_constant_paraList\[ampcount\+\+\]\s*\)")
 
 
-def lib_name(nr: int, nz: int, nx: int, ikm: int) -> str:
-    return f"libref_{nr}_{nz}_{nx}_{ikm}.so"
+def lib_name(nr: int, nz: int, nx: int, ikm: int, isospin: bool = False) -> str:
+    return f"libref_{'iso_' if isospin else ''}{nr}_{nz}_{nx}_{ikm}.so"
 
 
-def lib_path(nr: int, nz: int, nx: int, ikm: int = 6) -> Path:
-    return OUT / lib_name(nr, nz, nx, ikm)
+def lib_path(nr: int, nz: int, nx: int, ikm: int = 6, isospin: bool = False) -> Path:
+    return OUT / lib_name(nr, nz, nx, ikm, isospin)
+
+
+ISOSPIN_RE = re.compile(r"constexpr\s+bool\s+ISOSPIN_SIGMACD\s*=\s*false\s*;")
 
 
 def available() -> bool:
@@ -82,20 +92,32 @@ static constexpr unsigned MYXN = Constant::number_of_Zcs;
 """
 
 
-def build_bucket(nr: int, nz: int, nx: int, ikm: int = 6, verbose: bool = False) -> Path:
+def build_bucket(nr: int, nz: int, nx: int, ikm: int = 6, verbose: bool = False, isospin: bool = False) -> Path:
+    """One model-size bucket.  isospin: the reference's ISOSPIN_SIGMACD build (RooTDalitz/Resonances.h:17
+    set to true in a generated copy of that header, and cu_DPFPropogator.cu compiled from a generated
+    translation unit next to it so that its relative includes find the copy)."""
     reference_tree()
     OUT.mkdir(parents=True, exist_ok=True)
-    target = lib_path(nr, nz, nx, ikm)
-    work = OUT / f"b_{nr}_{nz}_{nx}_{ikm}"
+    target = lib_path(nr, nz, nx, ikm, isospin)
+    work = OUT / f"b_{'iso_' if isospin else ''}{nr}_{nz}_{nx}_{ikm}"
     if work.exists():
         shutil.rmtree(work)
     (work / "src").mkdir(parents=True)
     hdr = work / "RooTDalitz"
     hdr.mkdir()
     for f in (REF / "RooTDalitz").iterdir():
-        if f.name != "NDefine.h":
+        if f.name != "NDefine.h" and not (isospin and f.name == "Resonances.h"):
             (hdr / f.name).symlink_to(f)
     (hdr / "NDefine.h").write_text(_ndefine(nr, nz, nx, ikm))
+    prop_src = REF / "src" / "cu_DPFPropogator.cu"
+    if isospin:
+        res, n_iso = ISOSPIN_RE.subn("constexpr bool ISOSPIN_SIGMACD = true;", (REF / "RooTDalitz" / "Resonances.h").read_text())
+        if n_iso != 1:
+            raise RuntimeError("ISOSPIN_SIGMACD switch not found in Resonances.h; recipe out of date")
+        (hdr / "Resonances.h").write_text(f'#line 1 "{REF / "RooTDalitz" / "Resonances.h"}"\n' + res)
+        prop_src = work / "src" / "cu_DPFPropogator_host.cpp"
+        prop_src.write_text(f'#line 1 "{REF / "src" / "cu_DPFPropogator.cu"}"\n' +
+                            (REF / "src" / "cu_DPFPropogator.cu").read_text())
 
     text = (REF / "src" / "kernel_calEva.cu").read_text()
     text, n_launch = LAUNCH_RE.subn(lambda m: f"ref_host::launch(({m.group(2)}), ({m.group(3)}), {m.group(1)})(", text)
@@ -110,8 +132,7 @@ def build_bucket(nr: int, nz: int, nx: int, ikm: int = 6, verbose: bool = False)
              "-DTHRUST_DEVICE_SYSTEM=THRUST_DEVICE_SYSTEM_CPP", "-include", str(HERE / "ref_host" / "shim.h")]
     objs = []
     cmds = [
-        (["g++", *flags, "-x", "c++", "-c", str(REF / "src" / "cu_DPFPropogator.cu"), "-o", str(work / "prop.o")],
-         work / "prop.o"),
+        (["g++", *flags, "-x", "c++", "-c", str(prop_src), "-o", str(work / "prop.o")], work / "prop.o"),
         (["g++", *flags, "-x", "c++", "-c", str(gen), "-o", str(work / "kern.o")], work / "kern.o"),
         (["g++", "-std=c++17", "-O2", "-fPIC", f"-I{CUDA_INC}", "-c", str(HERE / "ref_host" / "driver.cpp"),
           "-o", str(work / "drv.o")], work / "drv.o"),
@@ -170,6 +191,7 @@ def build_aux(verbose: bool = False) -> Path:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--bucket", action="append", default=[], help="NR,NZ,NX[,IKM]")
+    ap.add_argument("--isospin", action="store_true", help="also build the ISOSPIN_SIGMACD variant of the K-matrix bucket")
     ap.add_argument("-v", action="store_true")
     args = ap.parse_args(argv)
     if not available():
@@ -179,6 +201,8 @@ def main(argv=None) -> int:
     for b in buckets:
         b = tuple(b) + ((6,) if len(b) == 3 else ())
         print("built", build_bucket(*b, verbose=args.v))
+    for b in ISOSPIN_BUCKETS if (args.isospin or not args.bucket) else []:
+        print("built", build_bucket(*b, verbose=args.v, isospin=True))
     print("built", build_aux(verbose=args.v))
     return 0
 

@@ -56,6 +56,7 @@ def lib():
         L.oracle_amp2_x.restype = C.c_int
         L.oracle_amp2_x.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_long, _fp, C.c_int, C.c_int, C.c_int,
                                     C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _dp, C.c_int]
+        L.oracle_set_kmatrix_isospin.argtypes = [C.c_int]
         L.oracle_assemble_nll.restype = C.c_double
         L.oracle_assemble_nll.argtypes = [_dp, _dp, _fp, C.c_long, C.c_long, C.c_double, C.c_double, C.c_double, _dp]
         for f in ("oracle_bw_lstar", "oracle_bw_pc"):
@@ -197,16 +198,22 @@ def nll(sample, block, swap_coupling_parts: bool = False) -> tuple:
 _ref_libs = {}
 
 
-def ref_lib(NR: int, NZ: int, NX: int = 0, ikm: int = 6, build_if_missing: bool = True):
+def set_kmatrix_isospin(on: bool):
+    """The 7-channel isospin-split K-matrix of the reference's ISOSPIN_SIGMACD build (Isospin_KMatrix,
+    src/cu_DPFPropogator.cu:384-586) instead of the 4-channel default, for every later oracle call."""
+    lib().oracle_set_kmatrix_isospin(int(bool(on)))
+
+
+def ref_lib(NR: int, NZ: int, NX: int = 0, ikm: int = 6, build_if_missing: bool = True, isospin: bool = False):
     import importlib.util
     spec = importlib.util.spec_from_file_location("pwa_build_ref", HERE / "build_ref.py")
     br = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(br)
-    path = br.lib_path(NR, NZ, NX, ikm)
+    path = br.lib_path(NR, NZ, NX, ikm, isospin)
     if not path.exists():
         if not (build_if_missing and br.available()):
             return None
-        br.build_bucket(NR, NZ, NX, ikm)
+        br.build_bucket(NR, NZ, NX, ikm, isospin=isospin)
     key = str(path)
     if key not in _ref_libs:
         L = C.CDLL(key)
@@ -227,8 +234,8 @@ def ref_lib(NR: int, NZ: int, NX: int = 0, ikm: int = 6, build_if_missing: bool 
 class RefHost:
     """The reference's host_store_fx on host cores for one sample (SoA buffers set once)."""
 
-    def __init__(self, sample, block):
-        self.L = ref_lib(block.NR, block.NZ, block.NX)
+    def __init__(self, sample, block, isospin: bool = False):
+        self.L = ref_lib(block.NR, block.NZ, block.NX, isospin=isospin)
         if self.L is None:
             raise FileNotFoundError("reference host build unavailable")
         self.s = sample

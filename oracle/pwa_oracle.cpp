@@ -548,9 +548,125 @@ void configure(Model& m) {
   }
 }
 
+// The reference's ISOSPIN_SIGMACD build (RooTDalitz/Resonances.h:17, compile-time there) replaces the
+// 4-channel K-matrix by Isospin_KMatrix; a run-time switch here (oracle_set_kmatrix_isospin).
+static bool g_kmatrix_isospin = false;
+
+// Isospin_KMatrix (cu_DPFPropogator.cu:384-586): 7 channels -- J/psi p and the charged (D- / D*-
+// with Sigma_c++ / Sigma_c*++) and neutral (D0 / D*0 with Sigma_c+ / Sigma_c*+) partners of the three
+// Sigma_c(*) D(*) channels -- with the 4 x 4 couplings and scattering terms spread by the isospin
+// factors sqrt(2/3) (charged) and -sqrt(1/3) (neutral), the poles of channels 1 and 3 shifted by
+// Re(i g^2 / 3 (2 rho_charged + rho_neutral)), a 7 x 7 first-row inverse, and its row folded back onto
+// the 4 production channels.  Same outputs as kmatrix_group.
+int kmatrix_group_isospin(const Model& md, double mpp, int J_r, int P_r, int ik, cd* Mtr) {
+  constexpr double D0 = F(1.86484f), DST0 = F(2.00685f), SCP = F(2.45265f), SCSTP = F(2.5174f);
+  constexpr double SCP_HW = (double)(-2.3f / 1000.f / 2.f), SCSTP_HW = (double)(-17.2f / 1000.f / 2.f);
+  constexpr double DM = F(1.86966f), DSTM = F(2.01026f), SCPP = F(2.45397f), SCSTPP = F(2.51841f);
+  constexpr double SCPP_HW = (double)(-1.89f / 1000.f / 2.f), SCSTPP_HW = (double)(-14.78f / 1000.f / 2.f);
+  const double iso_f[2] = {F(0.816496580927726f), F(-0.5773502691896257f)};
+  const float* pl = md.pl;
+  const double ffb = md.FFB;
+  const int Lna = (P_r == 1) ? 1 : 0;
+  const double s = mpp * mpp;
+  cd rho[7];
+  rho[0] = rho_real(s, M_P, M_JPSI, Lna, ffb);
+  if (J_r == 1 && P_r == -1) {
+    rho[1] = rho_complex(s, cd(DSTM, 0), cd(SCPP, SCPP_HW));
+    rho[2] = rho_complex(s, cd(DST0, 0), cd(SCP, SCP_HW));
+    rho[3] = rho_complex(s, cd(DSTM, 0), cd(SCSTPP, SCSTPP_HW));
+    rho[4] = rho_complex(s, cd(DST0, 0), cd(SCSTP, SCSTP_HW));
+    rho[5] = rho_complex(s, cd(DM, 0), cd(SCPP, SCPP_HW));
+    rho[6] = rho_complex(s, cd(D0, 0), cd(SCP, SCP_HW));
+  } else if (J_r == 3 && P_r == -1) {
+    rho[1] = rho_complex(s, cd(DSTM, 0), cd(SCPP, SCPP_HW));
+    rho[2] = rho_complex(s, cd(DST0, 0), cd(SCP, SCP_HW));
+    rho[3] = rho_complex(s, cd(DSTM, 0), cd(SCSTPP, SCSTPP_HW));
+    rho[4] = rho_complex(s, cd(DST0, 0), cd(SCSTP, SCSTP_HW));
+    rho[5] = rho_complex(s, cd(DM, 0), cd(SCSTPP, SCSTPP_HW));
+    rho[6] = rho_complex(s, cd(D0, 0), cd(SCSTP, SCSTP_HW));
+  } else if (P_r == 1) {
+    rho[1] = rho_real(s, DSTM, SCPP, Lna, ffb);
+    rho[2] = rho_real(s, DST0, SCP, Lna, ffb);
+    rho[3] = rho_real(s, DM, SCPP, Lna, ffb);
+    rho[4] = rho_real(s, D0, SCP, Lna, ffb);
+    rho[5] = rho_real(s, DM, SCSTPP, Lna, ffb);
+    rho[6] = rho_real(s, D0, SCSTP, Lna, ffb);
+  } else {
+    return -1;
+  }
+  const float* g_alpha = &pl[md.kmcount + ik * (NPMAX + NKMC) * NKMC];
+  const float* f_scat = &pl[md.kmcount + NPMAX * NKMC + ik * (NPMAX + NKMC) * NKMC];
+  int Npole = 0, ikm = 1;
+  double ms[NPMAX + 1] = {1, 1, 1, 1, 1};
+  for (int r = md.NR; r < md.NR + md.NZ; ++r) {
+    const double mfit = pl[r * NSET + P_MASS];
+    const int iChannel = (int)pl[r * NSET + P_WIDTH];
+    const int S = (int)pl[r * NSET + P_SPIN];
+    const int type = (int)pl[r * NSET + P_TYPE];
+    const int parity = (int)pl[r * NSET + P_PARITY];
+    if (!(type == T_KMATRIX && S == J_r && parity == P_r && mfit > 0)) continue;
+    if (Npole >= NPMAX) return -2;
+    double m0 = mfit;
+    if (iChannel == 1 || iChannel == 3) {
+      const double mfit2 = mfit * mfit;
+      const cd ra = iChannel == 1 ? rho_complex(mfit2, cd(DSTM, 0), cd(SCPP, SCPP_HW))
+                                  : rho_complex(mfit2, cd(DM, 0), cd(SCPP, SCPP_HW));
+      const cd rb = iChannel == 1 ? rho_complex(mfit2, cd(DST0, 0), cd(SCP, SCP_HW))
+                                  : rho_complex(mfit2, cd(D0, 0), cd(SCP, SCP_HW));
+      const double g = g_alpha[Npole * NKMC + iChannel];
+      const cd shift = cd(0, g * g / 3.0) * (2.0 * ra + rb);
+      m0 = std::sqrt(mfit2 + shift.real());
+    } else if (iChannel != 0) {
+      return -3;  // the reference prints "An unacceptable channel" and uses an unset mass
+    }
+    double denorm = m0 * m0 - s;
+    if (std::fabs(denorm) < F(1e-3f)) denorm = F(1e-3f);
+    ++Npole;
+    ms[0] *= denorm;
+    for (int ip = 1; ip <= NPMAX; ++ip)
+      if (ip != ikm) ms[ip] *= denorm;
+    ++ikm;
+  }
+  double mg[NPMAX][NKMC], fs[NKMC][NKMC], kma[7][7];
+  for (int i = 0; i < Npole; ++i)
+    for (int j = 0; j < NKMC; ++j) mg[i][j] = g_alpha[i * NKMC + j] * ms[i + 1];
+  for (int i = 0; i < NKMC; ++i)
+    for (int j = 0; j < NKMC; ++j) fs[i][j] = f_scat[i * NKMC + j] * ms[0];
+  for (int i = 0; i < 7; ++i) {
+    const double fi = (i == 0) ? 1.0 : iso_f[(i + 1) % 2];
+    const int ip = (i + 1) / 2;
+    for (int j = i; j < 7; ++j) {
+      const double fj = (j == 0) ? 1.0 : iso_f[(j + 1) % 2];
+      const int jp = (j + 1) / 2;
+      double v = fi * fj * fs[ip][jp];
+      for (int k = 0; k < Npole; ++k) v += fi * fj * (double)g_alpha[k * NKMC + ip] * mg[k][jp];
+      kma[i][j] = kma[j][i] = v;
+    }
+  }
+  cd KK[49];
+  for (int i = 0; i < 7; ++i)
+    for (int j = 0; j < 7; ++j) {
+      KK[i * 7 + j] = cd(0, -1) * (kma[i][j] * rho[j]);
+      if (i == j) KK[i * 7 + j] += ms[0];
+    }
+  cd T7[7];
+  first_row_of_inverse(KK, 7, T7);
+  const cd T[NKMC] = {T7[0], iso_f[0] * T7[1] + iso_f[1] * T7[2], iso_f[0] * T7[3] + iso_f[1] * T7[4],
+                      iso_f[0] * T7[5] + iso_f[1] * T7[6]};
+  const double na = (Lna >= 1) ? channel_barrier(s, M_P, M_JPSI, Lna, ffb) : 1.0;
+  for (int p = 0; p < Npole; ++p) {
+    cd acc(0, 0);
+    for (int i = 0; i < NKMC; ++i) acc += T[i] * mg[p][i];
+    Mtr[p] = acc * na;
+  }
+  for (int i = 0; i < NKMC; ++i) Mtr[Npole + i] = T[i] * (ms[0] * na);
+  return Npole + NKMC;
+}
+
 // One J^P group of the coupled-channel Pc K-matrix at invariant mass mpp.  Writes Npole + 4 P-vector
 // outputs (poles first, then the four non-resonant production terms).
 int kmatrix_group(const Model& md, double mpp, int J_r, int P_r, int ik, cd* Mtr) {
+  if (g_kmatrix_isospin) return kmatrix_group_isospin(md, mpp, J_r, P_r, ik, Mtr);
   const float* pl = md.pl;
   const double ffb = md.FFB;
   const int Lna = (P_r == 1) ? 1 : 0;
@@ -890,6 +1006,8 @@ bool in_mc_smear_window(float mz) { return (mz > 4.4 && mz < 4.48) || (mz > 4.27
 }  // namespace
 
 extern "C" {
+
+void oracle_set_kmatrix_isospin(int on) { g_kmatrix_isospin = on != 0; }
 
 // Per-event |A|^2 with the reference's band dispatch (kernel_calEva.cu:819-961):
 //   [0, nda_smr)                     30-offset smearing

@@ -82,6 +82,8 @@ struct pwa_ctx {
   int use_tables = 1;
   // order of the per-class event lists (MC window / tail): 1 by m(J/psi p), 0 by event index
   int mass_order = 0;
+  // build_point_table flags (K-matrix variant)
+  int build_flags = 0;
   void* d_tab = nullptr;  // TAB_BYTES of two-level lineshape tables
   // optional per-segment timing
   int timing = 0;
@@ -240,7 +242,8 @@ int build_reference_segments(pwa_ctx* c, const float* h_mz) {
 int pwa::ctx_view(const pwa_ctx* c, CtxView* v) {
   if (!c || !v) return PWA_E_ARG;
   *v = CtxView{c->device, c->sm_count, c->st, c->pp, c->pp1, c->pp2, c->sw, c->pp3, c->pp4, c->n, c->n_size,
-               c->nda, c->smear_mode == PWA_SMEAR_GAUSS ? 1 : 0, c->d_grid, c->grid_nb, c->use_tables};
+               c->nda, c->smear_mode == PWA_SMEAR_GAUSS ? 1 : 0, c->d_grid, c->grid_nb, c->use_tables,
+               c->build_flags};
   return c->pp ? PWA_OK : PWA_E_STATE;
 }
 
@@ -454,6 +457,13 @@ int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int ha
   return build_segments(c, mz.data());
 }
 
+int pwa_ctx_set_kmatrix(pwa_ctx* c, int kmatrix) {
+  if (!c) return PWA_E_ARG;
+  if (kmatrix != PWA_KMATRIX_DEFAULT && kmatrix != PWA_KMATRIX_ISOSPIN) return PWA_E_ARG;
+  c->build_flags = kmatrix == PWA_KMATRIX_ISOSPIN ? BUILD_KM_ISOSPIN : 0;
+  return PWA_OK;
+}
+
 int pwa_ctx_set_event_order(pwa_ctx* c, int by_mass) {
   if (!c) return PWA_E_ARG;
   c->mass_order = by_mass ? 1 : 0;
@@ -555,7 +565,7 @@ int pwa_ctx_eval_nll(pwa_ctx* c, const float* pl, int para_size, int vamp_size, 
                      pwa_result* out, double* h_fx) {
   if (!c || !pl || !out) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table, c->build_flags);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
   if (h_fx && c->fx_cap < c->n) {
@@ -634,7 +644,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   std::vector<PointTable> H(npoints);
   for (int p = 0; p < npoints; ++p) {
     const int rc = build_point_table(pls + (size_t)p * block_stride, para_size, vamp_size, spline_size, NR, NZ, NX,
-                                     FFR, FFB, &H[p]);
+                                     FFR, FFB, &H[p], c->build_flags);
     if (rc) return rc;
   }
   // structured points (relative to point 0) and points for the single-point path
@@ -798,7 +808,7 @@ int pwa_ctx_amp2(pwa_ctx* c, const float* pl, int para_size, int vamp_size, int 
                  float FFR, float FFB, double* h_amp2) {
   if (!c || !pl || !h_amp2) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table, c->build_flags);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
   if (c->fx_cap < c->n) {
@@ -825,7 +835,7 @@ int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_siz
                         int NX, float FFR, float FFB, double* integral) {
   if (!c || !pl || !integral) return PWA_E_ARG;
   if (!c->pp) return PWA_E_STATE;
-  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table);
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, c->h_table, c->build_flags);
   if (rc) return rc;
   PWA_CUDA(cudaSetDevice(c->device));
   if (c->fx_cap < c->n) {
@@ -852,9 +862,17 @@ int pwa_ctx_mc_integral(pwa_ctx* c, const float* pl, int para_size, int vamp_siz
 
 int pwa_host_lineshapes(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
                         float FFR, float FFB, double mkp, double mz, double* lstar, double* pc) {
+  return pwa_host_lineshapes_km(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, PWA_KMATRIX_DEFAULT, mkp,
+                                mz, lstar, pc);
+}
+
+int pwa_host_lineshapes_km(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
+                           float FFR, float FFB, int kmatrix, double mkp, double mz, double* lstar, double* pc) {
   if (!pl || !lstar || !pc) return PWA_E_ARG;
+  if (kmatrix != PWA_KMATRIX_DEFAULT && kmatrix != PWA_KMATRIX_ISOSPIN) return PWA_E_ARG;
   PointTable* T = new PointTable();
-  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, T);
+  int rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, T,
+                             kmatrix == PWA_KMATRIX_ISOSPIN ? BUILD_KM_ISOSPIN : 0);
   if (!rc) host_lineshapes(*T, mkp, mz, reinterpret_cast<cplx*>(lstar), reinterpret_cast<cplx*>(pc));
   delete T;
   return rc;

@@ -171,9 +171,83 @@ __host__ __device__ inline cplx x_lineshape(const XEntry& X, const XKin& k) {
   return mk(de2 * f, gm * f) * (FB * ipow(k.pBm, X.LB));
 }
 
+// One J^P group of the 7-channel isospin-split K-matrix (Isospin_KMatrix, cu_DPFPropogator.cu:
+// 384-586): J/psi p and the charged / neutral partners of the three Sigma_c(*) D(*) channels, the
+// 4 x 4 couplings and scattering terms spread over them with the isospin factors, a 7 x 7 solve, and
+// the first row folded back onto the 4 production channels.  Outputs as km_solve's.  Kept out of line:
+// only the isospin build calls it, and the default kernels keep their register allocation.
+static __host__ __device__ __noinline__ void km_solve_iso(const KmGroup& G, double mz, double ffb, cplx* out) {
+  const double s = mz * mz;
+  cplx rho[7];
+  rho[0] = rho_real(s, M_P, M_JPSI, G.Lna, ffb);
+  const cplx dstm = mk(KMI_DSTM, 0), dst0 = mk(KMI_DST0, 0), dm = mk(KMI_DM, 0), d0 = mk(KMI_D0, 0);
+  const cplx scpp = mk(KMI_SCPP, KMI_SCPP_HW), scp = mk(KMI_SCP, KMI_SCP_HW);
+  const cplx scstpp = mk(KMI_SCSTPP, KMI_SCSTPP_HW), scstp = mk(KMI_SCSTP, KMI_SCSTP_HW);
+  if (G.P == -1) {
+    rho[1] = rho_complex(s, dstm, scpp);
+    rho[2] = rho_complex(s, dst0, scp);
+    rho[3] = rho_complex(s, dstm, scstpp);
+    rho[4] = rho_complex(s, dst0, scstp);
+    rho[5] = rho_complex(s, dm, G.J2 == 1 ? scpp : scstpp);
+    rho[6] = rho_complex(s, d0, G.J2 == 1 ? scp : scstp);
+  } else {
+    rho[1] = rho_real(s, KMI_DSTM, KMI_SCPP, G.Lna, ffb);
+    rho[2] = rho_real(s, KMI_DST0, KMI_SCP, G.Lna, ffb);
+    rho[3] = rho_real(s, KMI_DM, KMI_SCPP, G.Lna, ffb);
+    rho[4] = rho_real(s, KMI_D0, KMI_SCP, G.Lna, ffb);
+    rho[5] = rho_real(s, KMI_DM, KMI_SCSTPP, G.Lna, ffb);
+    rho[6] = rho_real(s, KMI_D0, KMI_SCSTP, G.Lna, ffb);
+  }
+  double ms[NPMAX + 1] = {1, 1, 1, 1, 1};
+  for (int p = 0; p < G.npole; ++p) {
+    double den = G.m0sq[p] - s;
+    if (fabs(den) < KM_DENORM_MIN) den = KM_DENORM_MIN;
+    ms[0] *= den;
+#pragma unroll
+    for (int ip = 1; ip <= NPMAX; ++ip)
+      if (ip != p + 1) ms[ip] *= den;
+  }
+  double mg[NPMAX][NKMC];
+  for (int p = 0; p < G.npole; ++p)
+#pragma unroll
+    for (int j = 0; j < NKMC; ++j) mg[p][j] = G.g[p][j] * ms[p + 1];
+  // channel i >= 1 is production channel (i + 1) / 2 with isospin factor ISO0 (odd i) or ISO1
+  auto iso = [](int i) { return i == 0 ? 1.0 : ((i + 1) % 2 == 0 ? KMI_ISO0 : KMI_ISO1); };
+  cplx S[7][7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i)
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      const int a = i < j ? i : j, b = i < j ? j : i;  // the reference fills the upper triangle
+      const int ap = (a + 1) / 2, bp = (b + 1) / 2;
+      const double f = iso(a) * iso(b);
+      double v = f * (G.f[ap][bp] * ms[0]);
+      for (int p = 0; p < G.npole; ++p) v += f * G.g[p][ap] * mg[p][bp];
+      S[i][j] = mk(v * rho[j].im, -v * rho[j].re);
+      if (i == j) S[i][j].re += ms[0];
+    }
+  cplx T7[7];
+  first_row_inverse<7>(S, T7);
+  const cplx T[NKMC] = {T7[0], T7[1] * KMI_ISO0 + T7[2] * KMI_ISO1, T7[3] * KMI_ISO0 + T7[4] * KMI_ISO1,
+                        T7[5] * KMI_ISO0 + T7[6] * KMI_ISO1};
+  const double na = (G.Lna >= 1) ? channel_barrier(s, M_P, M_JPSI, G.Lna, ffb) : 1.0;
+  for (int p = 0; p < G.npole; ++p) {
+    cplx acc = mk(0, 0);
+#pragma unroll
+    for (int i = 0; i < NKMC; ++i) acc += T[i] * mg[p][i];
+    out[p] = acc * na;
+  }
+#pragma unroll
+  for (int i = 0; i < NKMC; ++i) out[G.npole + i] = T[i] * (ms[0] * na);
+}
+
 // One J^P group of the coupled-channel K-matrix at mass mz (Default_KMatrix,
 // cu_DPFPropogator.cu:588-813): P-vector outputs, npole poles first then 4 production terms.
 __host__ __device__ inline void km_solve(const KmGroup& G, double mz, double ffb, cplx* out) {
+  if (G.iso) {
+    km_solve_iso(G, mz, ffb, out);
+    return;
+  }
   const double s = mz * mz;
   cplx rho[NKMC];
   rho[0] = rho_real(s, M_P, M_JPSI, G.Lna, ffb);

@@ -947,7 +947,7 @@ int pwa_ens_create(pwa_ctx* ctx, const float* pl, int para_size, int vamp_size, 
     ens_free(s);
     return cuda_fail(e);
   }
-  if ((rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, s->h_T))) {
+  if ((rc = build_point_table(pl, para_size, vamp_size, spline_size, NR, NZ, NX, FFR, FFB, s->h_T, cv.build_flags))) {
     ens_free(s);
     return rc;
   }

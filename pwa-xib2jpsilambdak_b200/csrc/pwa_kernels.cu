@@ -17,6 +17,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "pwa_device.cuh"
@@ -713,13 +714,26 @@ static int G_valid_check(const KmGroup& G) { return (G.npole <= NPMAX) ? 0 : 1; 
 // Masses in the table range where the reference's complex square root (csqrt_branch) changes branch
 // for one of the complex-mass channels (D* Sigma_c, D* Sigma_c*, D Sigma_c, D Sigma_c*): the lineshape
 // jumps there, so interpolation must not straddle them.  Scan plus bisection, computed once.
-static const std::vector<double>& complex_branch_masses() {
-  static std::vector<double> out;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    const cplx ch[4][2] = {{mk(KM_DST, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_DST, 0), mk(KM_SCST, KM_SCST_HW)},
-                           {mk(KM_D, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_D, 0), mk(KM_SCST, KM_SCST_HW)}};
-    for (auto& c : ch) {
+// Masses where the reference's complex square root switches branch in the complex-mass channels of
+// the K-matrix (the 4-channel default, or the 7-channel isospin split).
+static const std::vector<double>& complex_branch_masses(bool isospin = false) {
+  static std::vector<double> out[2];
+  static std::once_flag once[2];
+  std::call_once(once[isospin ? 1 : 0], [isospin] {
+    std::vector<double>& res = out[isospin ? 1 : 0];
+    std::vector<std::pair<cplx, cplx>> ch;
+    if (!isospin) {
+      ch = {{mk(KM_DST, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_DST, 0), mk(KM_SCST, KM_SCST_HW)},
+            {mk(KM_D, 0), mk(KM_SC, KM_SC_HW)}, {mk(KM_D, 0), mk(KM_SCST, KM_SCST_HW)}};
+    } else {
+      const cplx dstm = mk(KMI_DSTM, 0), dst0 = mk(KMI_DST0, 0), dm = mk(KMI_DM, 0), d0 = mk(KMI_D0, 0);
+      const cplx scpp = mk(KMI_SCPP, KMI_SCPP_HW), scp = mk(KMI_SCP, KMI_SCP_HW);
+      const cplx scstpp = mk(KMI_SCSTPP, KMI_SCSTPP_HW), scstp = mk(KMI_SCSTP, KMI_SCSTP_HW);
+      ch = {{dstm, scpp}, {dst0, scp}, {dstm, scstpp}, {dst0, scstp}, {dm, scpp}, {d0, scp}, {dm, scstpp},
+            {d0, scstp}};
+    }
+    for (auto& cc : ch) {
+      const cplx c[2] = {cc.first, cc.second};
       auto state = [&](double m) {
         const double s = m * m;
         const cplx a = c[0] + c[1], b = c[0] - c[1];
@@ -738,14 +752,14 @@ static const std::vector<double>& complex_branch_masses() {
             const double c2 = 0.5 * (a + b);
             (state(c2) == prev ? a : b) = c2;
           }
-          out.push_back(0.5 * (a + b));
+          res.push_back(0.5 * (a + b));
           prev = st;
         }
         prev_m = m;
       }
     }
   });
-  return out;
+  return out[isospin ? 1 : 0];
 }
 
 static bool nonzero_host(cplx c) { return c.re != 0.0 || c.im != 0.0; }
@@ -754,7 +768,8 @@ static bool nonzero_host(cplx c) { return c.re != 0.0 || c.im != 0.0; }
 // coupling offsets of cuda_configure_ampcount, kernel_calEva.cu:1014-1098; K-matrix output slots
 // of cuda_configure_Pc_KMatrix, :978-1010) and hoists every parameter-only constant.
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
-                      float ffr, float ffb, PointTable* T) {
+                      float ffr, float ffb, PointTable* T, int flags) {
+  const bool isospin = (flags & BUILD_KM_ISOSPIN) != 0;
   std::memset(T, 0, sizeof(PointTable));
   if (NR > MAX_LSTAR || NZ > MAX_PC || NX > MAX_ZCS || NR < 0 || NZ < 0 || NX < 0) return 4;  // PWA_E_SIZE
   if (para_size != NSET * (NR + NZ + NX)) return 3;                                           // PWA_E_LAYOUT
@@ -1026,6 +1041,7 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
     G.J2 = (ik == 1 || ik == 3) ? 3 : 1;
     G.P = (ik >= 2) ? 1 : -1;
     G.Lna = (G.P == 1) ? 1 : 0;
+    G.iso = isospin ? 1 : 0;
     const float* g_alpha = pl + kmcount + ik * (NPMAX + NKMC) * NKMC;
     const float* f_scat = g_alpha + NPMAX * NKMC;
     for (int i = 0; i < NKMC; ++i)
@@ -1038,7 +1054,24 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
       const double mfit = q[0];
       const int ich = (int)q[1];
       double m0 = mfit;
-      if (ich > 0) {
+      if (ich > 0 && isospin) {
+        // Isospin_KMatrix (cu_DPFPropogator.cu:455-489): channels 1 and 3 only, the shift
+        // Re(i g^2 / 3 (2 rho_charged + rho_neutral))
+        const double mfit2 = mfit * mfit;
+        cplx ra, rb;
+        if (ich == 1) {
+          ra = rho_complex(mfit2, mk(KMI_DSTM, 0), mk(KMI_SCPP, KMI_SCPP_HW));
+          rb = rho_complex(mfit2, mk(KMI_DST0, 0), mk(KMI_SCP, KMI_SCP_HW));
+        } else if (ich == 3) {
+          ra = rho_complex(mfit2, mk(KMI_DM, 0), mk(KMI_SCPP, KMI_SCPP_HW));
+          rb = rho_complex(mfit2, mk(KMI_D0, 0), mk(KMI_SCP, KMI_SCP_HW));
+        } else {
+          return 6;  // the reference prints "An unacceptable channel" and reads an unset mass
+        }
+        const double g = g_alpha[np * NKMC + ich];
+        const cplx shift = mk(0, g * g / 3.0) * (ra * 2.0 + rb);
+        m0 = std::sqrt(mfit2 + shift.re);
+      } else if (ich > 0) {
         const double mfit2 = mfit * mfit;
         cplx rch;
         if (ich == 1)
@@ -1191,13 +1224,21 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
       guard(std::sqrt(b), step);
     }
   }
-  if (pos_parity) {  // real-mass channel thresholds of the positive-parity groups
+  if (pos_parity && !isospin) {  // real-mass channel thresholds of the positive-parity groups
     guard(KM_DST + KM_SC, cusp);
     guard(KM_D + KM_SC, cusp);
     guard(KM_D + KM_SCST, cusp);
   }
+  if (pos_parity && isospin) {
+    guard(KMI_DSTM + KMI_SCPP, cusp);
+    guard(KMI_DST0 + KMI_SCP, cusp);
+    guard(KMI_DM + KMI_SCPP, cusp);
+    guard(KMI_D0 + KMI_SCP, cusp);
+    guard(KMI_DM + KMI_SCSTPP, cusp);
+    guard(KMI_D0 + KMI_SCSTP, cusp);
+  }
   if (neg_parity)
-    for (double m : complex_branch_masses()) guard(m, step);
+    for (double m : complex_branch_masses(isospin)) guard(m, step);
   // spline waves drop to zero outside their domain
   bool pc_spline = false;
   for (int i = 0; i < NZ; ++i) pc_spline |= (T->Z[i].type == LT_SPLINE);

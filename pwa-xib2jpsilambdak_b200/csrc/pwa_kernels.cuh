@@ -86,12 +86,15 @@ struct CtxView {
   const double* grid;
   int grid_nb;
   int use_tables;
+  int build_flags;  // build_point_table flags (K-matrix variant)
 };
 int ctx_view(const pwa_ctx* c, CtxView* v);
 
-// Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.
+// Builds the point table from a float parameter block; returns 0 or a PWA_E_* code.  flags:
+// BUILD_KM_ISOSPIN selects the 7-channel isospin-split K-matrix (the reference's ISOSPIN_SIGMACD).
+constexpr int BUILD_KM_ISOSPIN = 1;
 int build_point_table(const float* pl, int para_size, int vamp_size, int spline_size, int NR, int NZ, int NX,
-                      float ffr, float ffb, PointTable* out);
+                      float ffr, float ffb, PointTable* out, int flags = 0);
 
 // Launches one segment; partials written at out[0 .. segment_parts).  fx_out (optional) receives
 // per-event fx (weighted by w for MC, like the reference's d_fx).  With the lineshape tables on, defer

@@ -158,49 +158,64 @@ __host__ __device__ __forceinline__ double tanh_eff_mass(double m, double mmin, 
 constexpr int NKMC = 4;
 constexpr int NPMAX = 4;
 
-// First row of inv(S), S complex 4x4 row-major, by an unpivoted LU of S^T solved against e0
-// (RooTDalitz/cuSolve4x4.h:278-353).
-__host__ __device__ __forceinline__ void first_row_inverse4(const cplx (&S)[4][4], cplx (&T)[4]) {
+// First row of inv(S), S complex N x N row-major, by an unpivoted LU of S^T solved against e0
+// (RooTDalitz/cuSolve4x4.h:278-353 for N = 4, solve_7x7 :463 for N = 7).
+template <int N>
+__host__ __device__ __forceinline__ void first_row_inverse(const cplx (&S)[N][N], cplx (&T)[N]) {
   // A = S^T: A[r][c] = S[c][r]
-  cplx U[4][4], L[4][4], invU[4];
+  cplx U[N][N], L[N][N], invU[N];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < N; ++i) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < N; ++c) {
       if (c < i) continue;
       cplx u = S[c][i];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < N; ++k)
         if (k < i) u -= L[i][k] * U[k][c];
       U[i][c] = u;
     }
     invU[i] = recip(U[i][i]);
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < N; ++r) {
       if (r <= i) continue;
       cplx l = S[i][r];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < N; ++k)
         if (k < i) l -= L[r][k] * U[k][i];
       L[r][i] = l * invU[i];
     }
   }
-  cplx y[4];
+  cplx y[N];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < N; ++i) {
     y[i] = (i == 0) ? mk(1, 0) : mk(0, 0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < N; ++j)
       if (j < i) y[i] -= L[i][j] * y[j];
   }
 #pragma unroll
-  for (int i = 3; i >= 0; --i) {
+  for (int i = N - 1; i >= 0; --i) {
     cplx x = y[i];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < N; ++j)
       if (j > i) x -= U[i][j] * T[j];
     T[i] = invU[i] * x;
   }
 }
+__host__ __device__ __forceinline__ void first_row_inverse4(const cplx (&S)[4][4], cplx (&T)[4]) {
+  first_row_inverse<4>(S, T);
+}
+
+// Isospin-split channels of the 7-channel K-matrix (Isospin_KMatrix, cu_DPFPropogator.cu:384-586,
+// the reference's ISOSPIN_SIGMACD build): charged and neutral D(*) and Sigma_c(*) masses, the
+// Sigma_c(*) half-widths as complex masses, and the isospin factors sqrt(2/3), -sqrt(1/3) (floats).
+constexpr double KMI_D0 = PWA_F(1.86484f), KMI_DST0 = PWA_F(2.00685f);
+constexpr double KMI_SCP = PWA_F(2.45265f), KMI_SCSTP = PWA_F(2.5174f);
+constexpr double KMI_SCP_HW = (double)(-2.3f / 1000.f / 2.f), KMI_SCSTP_HW = (double)(-17.2f / 1000.f / 2.f);
+constexpr double KMI_DM = PWA_F(1.86966f), KMI_DSTM = PWA_F(2.01026f);
+constexpr double KMI_SCPP = PWA_F(2.45397f), KMI_SCSTPP = PWA_F(2.51841f);
+constexpr double KMI_SCPP_HW = (double)(-1.89f / 1000.f / 2.f), KMI_SCSTPP_HW = (double)(-14.78f / 1000.f / 2.f);
+constexpr double KMI_ISO0 = PWA_F(0.816496580927726f), KMI_ISO1 = PWA_F(-0.5773502691896257f);
 
 }  // namespace pwa

@@ -90,6 +90,7 @@ struct XEntry {
 
 struct KmGroup {
   int J2, P, Lna, npole;
+  int iso, pad;           // 1: the 7-channel isospin-split K-matrix (the reference's ISOSPIN_SIGMACD build)
   double m0sq[NPMAX];     // pole mass^2 after the near-threshold shift
   double g[NPMAX][NKMC];  // pole couplings
   double f[NKMC][NKMC];   // scattering matrix

@@ -18,8 +18,8 @@ LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().pare
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
             "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing", "pwa_ctx_select_data",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
-            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_set_event_order", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
-            "pwa_host_lineshapes", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_events_from_unit",
+            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_set_event_order", "pwa_ctx_set_kmatrix", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
+            "pwa_host_lineshapes", "pwa_host_lineshapes_km", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_events_from_unit",
             "pwa_unit_flat", "pwa_flow_create", "pwa_flow_destroy", "pwa_flow_param_count", "pwa_flow_get_params",
             "pwa_flow_set_params", "pwa_flow_train_step", "pwa_flow_gradients", "pwa_flow_log_density",
             "pwa_flow_sample", "pwa_flow_fit_premap", "pwa_flow_get_premap", "pwa_flow_set_premap",
@@ -100,6 +100,8 @@ def load() -> C.CDLL:
         L.pwa_ctx_stream.argtypes = [C.c_void_p]
         L.pwa_host_lineshapes.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                           C.c_float, C.c_double, C.c_double, _dp, _dp]
+        L.pwa_host_lineshapes_km.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                             C.c_float, C.c_int, C.c_double, C.c_double, _dp, _dp]
         L.pwa_lineshapes_lstar_km.argtypes = [C.c_int, _fp, C.c_int, C.c_int, C.c_float, _fp, C.c_int, _dp, _dp,
                                               _dp, _dp]
         L.pwa_generate_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
@@ -262,6 +264,10 @@ class Context:
                                   block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp)), "pwa_ctx_amp2")
         return out
 
+    def set_kmatrix(self, isospin: bool):
+        """Coupled-channel K-matrix: the 7-channel isospin split (True) or the 4-channel default."""
+        check(self.L.pwa_ctx_set_kmatrix(self.h, int(bool(isospin))), "pwa_ctx_set_kmatrix")
+
     def set_event_order(self, by_mass: bool):
         """Walk each MC event class by m(J/psi p) (True) or by event index (False, the default)."""
         check(self.L.pwa_ctx_set_event_order(self.h, int(bool(by_mass))), "pwa_ctx_set_event_order")
@@ -309,15 +315,16 @@ class Context:
         return self.L.pwa_ctx_last_launches(self.h)
 
 
-def host_lineshapes(block, mkp: float, mz: float):
-    """Decoded Lambda* and Pc lineshapes (times production barriers) evaluated on the host."""
+def host_lineshapes(block, mkp: float, mz: float, isospin: bool = False):
+    """Decoded Lambda* and Pc lineshapes (times production barriers) evaluated on the host; isospin: the
+    7-channel isospin-split K-matrix."""
     L = load()
     pl = np.ascontiguousarray(block.data, np.float32)
     ls = np.zeros(2 * max(block.NR, 1))
     pc = np.zeros(2 * max(block.NZ, 1))
-    check(L.pwa_host_lineshapes(_f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR, block.NZ,
-                                block.NX, block.ffr, block.ffb, mkp, mz, ls.ctypes.data_as(_dp),
-                                pc.ctypes.data_as(_dp)), "pwa_host_lineshapes")
+    check(L.pwa_host_lineshapes_km(_f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR, block.NZ,
+                                   block.NX, block.ffr, block.ffb, int(bool(isospin)), mkp, mz,
+                                   ls.ctypes.data_as(_dp), pc.ctypes.data_as(_dp)), "pwa_host_lineshapes_km")
     return ls[0::2][:block.NR] + 1j * ls[1::2][:block.NR], pc[0::2][:block.NZ] + 1j * pc[1::2][:block.NZ]
 
 
