@@ -70,4 +70,4 @@ def loss_and_grads(params, x: np.ndarray, w: np.ndarray, emulate_bf16: bool = Tr
     wt = torch.as_tensor(w, dtype=torch.float64)
     loss = -(wt * lq).sum() / wt.sum()
     loss.backward()
-    return float(loss), [(W.grad.numpy(), b.grad.numpy()) for W, b in ts]
+    return float(loss.detach()), [(W.grad.numpy(), b.grad.numpy()) for W, b in ts]
