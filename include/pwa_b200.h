@@ -329,7 +329,8 @@ int pwa_ens_slots(const float* h_paraList, int para_size, int vamp_size, int spl
 /* The Gram matrices M and Mn (non-interference sum), row-major slot x slot complex (Re, Im doubles). */
 int pwa_ens_gram(const pwa_ens* ens, double* h_M, double* h_Mn);
 /* Launch shape of the per-call kernel: warps per block (4, 8, 12 or 16) and events per work item; the
- * project's autotuner (pwa_b200.ensemble.autotune) picks them by timing. */
+ * project's autotuner (pwa_b200.ensemble.autotune) picks them by timing.  A shape whose shared memory
+ * exceeds one block's (large models at 16 warps) returns PWA_E_SIZE and the current shape stays. */
 int pwa_ens_set_launch(pwa_ens* ens, int warps, int tile_events);
 /* One evaluation of every toy t with on[t] != 0 (on null: all) at its slot vector h_slots[t] ([n_toys]
  * [slots] x (Re, Im)), as one CUDA-graph launch (captured at the first call and after a launch-shape or

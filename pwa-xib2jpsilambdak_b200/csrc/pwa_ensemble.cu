@@ -1045,11 +1045,22 @@ int pwa_ens_set_launch(pwa_ens* s, int warps, int tile_events) {
   if (!s || (warps != 4 && warps != 8 && warps != 12 && warps != 16) || tile_events < 32) return PWA_E_ARG;
   cudaError_t e = cudaSetDevice(s->cv.device);
   if (e) return cuda_fail(e);
+  // a shape whose shared memory does not fit one block is refused and the current shape kept
+  int max_smem = 0;
+  if ((e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->cv.device)))
+    return cuda_fail(e);
+  if (ens_data_smem(warps, s->n_slot, s->NZ, ens_scratch(s->NR, s->NZ)) > (size_t)max_smem) return PWA_E_SIZE;
+  const int old_warps = s->warps, old_tile = s->tile_events;
   s->warps = warps;
   s->tile_events = tile_events;
   int occ = 1;
   e = data_kernel(s, false, &occ);
-  if (e) return cuda_fail(e);
+  if (e) {
+    s->warps = old_warps;
+    s->tile_events = old_tile;
+    cudaGetLastError();
+    return cuda_fail(e);
+  }
   s->blocks = s->cv.sm_count * std::max(occ, 1);
   if (s->graph) {
     cudaGraphExecDestroy(s->graph);

@@ -343,7 +343,10 @@ def autotune(ens: Ensemble, cache: str | Path | None = None, reps: int = 3, forc
     S = np.repeat(ens.s0[None, :], ens.n_toys, axis=0)
     timings = []
     for w, te in CANDIDATES:
-        ens.set_launch(w, te)
+        try:
+            ens.set_launch(w, te)
+        except lib.PwaError:
+            continue  # the shape does not fit this model (shared memory per block)
         ens.eval_slots(S)
         ms = []
         for _ in range(reps):
