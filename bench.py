@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--plain-only", action="store_true", help="skip the batched (Minuit gradient) measurement")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the toy-ensemble fit measurement")
+    ap.add_argument("--no-batch-tune", action="store_true",
+                    help="keep one wave of blocks per event class for the batched passes (no autotuning)")
     ap.add_argument("--event-order", choices=["index", "mass"], default="index",
                     help="walk each MC event class by event index or by m(J/psi p) (pwa_ctx_set_event_order)")
     ap.add_argument("--profile-case", choices=["flow_small", "ensemble_small"],
@@ -578,6 +580,10 @@ def main():
                 dist.all_reduce(bsums)
             return res, ns
 
+        tune = None
+        if not args.no_batch_tune:
+            from pwa_b200 import autotune
+            tune = autotune.tune_batch(ctx, gblocks)  # waves per event class, timed or from the cache
         for _ in range(max(args.warmup, 3)):
             bres, nstruct = bstep()
         if world > 1:
@@ -606,7 +612,7 @@ def main():
         idx = [0] + [labels.index((n, +1)) for n in probe if (n, +1) in labels]
         dmax = max(abs(bres[i].nll - ctx.eval_nll(gblocks[i]).nll) for i in idx)
         bat = dict(npts=npts, nstruct=nstruct, dev_ms=bdev_ms, e2e_ms=be2e_ms, launches=blaunch, dnll=dmax,
-                   nprobe=len(idx), seg=bseg, labels=labels, blocks=gblocks, res=bres)
+                   nprobe=len(idx), seg=bseg, labels=labels, blocks=gblocks, res=bres, tune=tune)
     clocks = clk.stop()
     if world > 1:
         t = torch.tensor([dev_ms, e2e_ms, bat["dev_ms"] if bat else 0.0, bat["e2e_ms"] if bat else 0.0],
@@ -747,7 +753,11 @@ def batched_line(plain: dict, bat: dict, args, world: int, sample, req_b: int, h
                   "points_one_by_one": npts - bat["nstruct"],
                   "max_abs_dnll_vs_single_point": bat["dnll"], "probed_points": bat["nprobe"],
                   "step": "the 2N+1 parameter points of Minuit's numerical gradient (centre, +-h per parameter) "
-                          "in one pwa_ctx_eval_nll_batch call; every point's NLL is computed in FP64"},
+                          "in one pwa_ctx_eval_nll_batch call; every point's NLL is computed in FP64",
+                  "waves_per_class": ({bnames[int(k)]: w for k, w in bat["tune"]["waves"].items()}
+                                      if bat.get("tune") else "1 (not tuned)"),
+                  "tune_ms": ({bnames[int(k)]: v for k, v in bat["tune"]["ms"].items()}
+                              if bat.get("tune") and "ms" in bat["tune"] else None)},
         "kernel_shares": {bnames[k]: round(t / tot, 4) for k, (t, n) in seg.items()},
         "segments": {bnames[k]: {"events": int(n), "ms_per_step": round(t / args.steps, 3)}
                      for k, (t, n) in seg.items()},

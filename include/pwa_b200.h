@@ -176,6 +176,13 @@ int pwa_ctx_segment_info(pwa_ctx* ctx, int i, int* kind, int64_t* events, double
  * the exact pass (lineshape masses the interpolation tables cannot serve).  No reference counterpart. */
 int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
 
+/* Launch shape of the batched evaluation's passes over one event class (the kind pwa_ctx_segment_info
+ * reports: 0 unsmeared, 1/2/3 the 20/30/150-offset classes, 4 the weighted grid): grid = min(blocks
+ * for its events, waves x SMs x resident blocks per SM), waves 1..16 (default 1).  More waves than
+ * one balance uneven per-event work at the cost of more block starts; the batch autotuner
+ * (pwa_b200.autotune.tune_batch) picks them per class by timing and caches the choice. */
+int pwa_ctx_set_batch_waves(pwa_ctx* ctx, int kind, int waves);
+
 /* Coupled-channel K-matrix of the context's evaluations.  PWA_KMATRIX_DEFAULT: 4 channels (J/psi p,
  * Sigma_c D*, Sigma_c* D*, Sigma_c D; Default_KMatrix, cu_DPFPropogator.cu:588-813).
  * PWA_KMATRIX_ISOSPIN: the 7-channel isospin split of the reference's ISOSPIN_SIGMACD build

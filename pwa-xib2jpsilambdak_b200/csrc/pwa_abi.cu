@@ -84,6 +84,8 @@ struct pwa_ctx {
   int mass_order = 0;
   // build_point_table flags (K-matrix variant)
   int build_flags = 0;
+  // launch shape of the batched passes per event class (Smear kind): waves of resident blocks
+  int batch_waves[SMEAR_KINDS] = {1, 1, 1, 1, 1};
   void* d_tab = nullptr;  // TAB_BYTES of two-level lineshape tables
   // optional per-segment timing
   int timing = 0;
@@ -457,6 +459,12 @@ int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int ha
   return build_segments(c, mz.data());
 }
 
+int pwa_ctx_set_batch_waves(pwa_ctx* c, int kind, int waves) {
+  if (!c || kind < 0 || kind >= SMEAR_KINDS || waves < 1 || waves > 16) return PWA_E_ARG;
+  c->batch_waves[kind] = waves;
+  return PWA_OK;
+}
+
 int pwa_ctx_set_kmatrix(pwa_ctx* c, int kmatrix) {
   if (!c) return PWA_E_ARG;
   if (kmatrix != PWA_KMATRIX_DEFAULT && kmatrix != PWA_KMATRIX_ISOSPIN) return PWA_E_ARG;
@@ -740,7 +748,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     size_t rows = 0;
     for (auto& sg : c->segs) {
       row_off.push_back(rows);
-      rows += batch_segment_rows(sg, T0, gm, nc, c->sm_count, tables);
+      rows += batch_segment_rows(sg, T0, gm, nc, c->sm_count, tables, c->batch_waves[sg.kind]);
     }
     if (rows * nc > c->bparts_cap) {
       cudaFree(c->d_bparts);
@@ -755,7 +763,8 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
       int* dcnt = tables ? c->d_defer_cnt + i : nullptr;
       if (c->timing) PWA_CUDA(cudaEventRecord(c->bseg_ev[2 * i], c->st));
       PWA_CUDA(launch_batch_segment(ev, c->segs[i], c->d_table, T0, gm, c->d_bpts, nc,
-                                    c->d_bparts + row_off[i] * nc, dq, dcnt, c->sm_count, c->st));
+                                    c->d_bparts + row_off[i] * nc, dq, dcnt, c->sm_count, c->st,
+                                    c->batch_waves[c->segs[i].kind]));
       if (c->timing) PWA_CUDA(cudaEventRecord(c->bseg_ev[2 * i + 1], c->st));
       launches += tables ? 2 : 1;
     }

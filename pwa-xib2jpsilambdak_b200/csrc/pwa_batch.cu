@@ -22,6 +22,7 @@
 // evaluates the centre (Lambda* terms, Pc angular amplitudes HZ_q[h], the entry lineshapes R at up to
 // 32 masses per round and S_b[h] = sum_q R_q(m_b) HZ_q[h]), then each lane takes one parameter point.
 // Per-point results go to per-block FP64 sums; a finalize kernel reduces them per point.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -477,7 +478,11 @@ static int batch_nb(int kind) {
   return kind == SMEAR_20 ? 20 : kind == SMEAR_30 ? 30 : kind == SMEAR_150 ? 150 : kind == SMEAR_GRID ? -1 : 0;
 }
 
-static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count) {
+// Blocks of a batched pass: one per BATCH_WARPS events (BU_THREADS for the unsmeared kernel), at most
+// `waves` x the resident blocks (sm_count x occupancy); waves > 1 trades block start-up cost for a
+// finer balance of uneven per-event work (the batch autotuner picks it per event class).
+static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count,
+                      int waves) {
   const int64_t n = s.end - s.begin;
   int occ = 1;
   int64_t b;
@@ -496,15 +501,15 @@ static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMa
     }
   }
   if (occ < 1) occ = 1;
-  const int64_t cap = (int64_t)sm_count * occ;
+  const int64_t cap = (int64_t)sm_count * occ * std::max(1, waves);
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (int)b;
 }
 
 int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count,
-                       bool deferred) {
-  const int g = batch_grid(s, T0, gm, npts, sm_count);
+                       bool deferred, int waves) {
+  const int g = batch_grid(s, T0, gm, npts, sm_count, waves);
   return deferred ? 2 * g : g;
 }
 
@@ -538,7 +543,7 @@ static void launch_batch_nb(int nb, const EventSet& ev, int64_t begin, int64_t e
 
 cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
                                  const BatchGroupMap& gm, const BatchPoint* d_pts, int npts, Partial* out,
-                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st) {
+                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st, int waves) {
   if (seg.end <= seg.begin) return cudaSuccess;
   if (npts < 1 || npts > BATCH_MAX_POINTS) return cudaErrorInvalidValue;
   const int nb = batch_nb(seg.kind);
@@ -546,7 +551,7 @@ cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const P
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
   const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, T0.NX, gm.max_slots, npts).total
                               : batch_layout(T0.NR, T0.NZ, npts).total;
-  const int grid = batch_grid(seg, T0, gm, npts, sm_count);
+  const int grid = batch_grid(seg, T0, gm, npts, sm_count, waves);
   if (defer) {
     launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, defer,
                     defer_count, false, grid, smem, st, seg);

@@ -157,13 +157,14 @@ constexpr int BATCH_MAX_POINTS = 384;
 // Partial rows a segment of a batched evaluation writes (its pass, plus the deferred pass when
 // deferred is true); each row holds npts partials.
 int batch_segment_rows(const Segment& s, const PointTable& T0, const BatchGroupMap& gm, int npts, int sm_count,
-                       bool deferred);
+                       bool deferred, int waves = 1);
 
 // Launches the batched passes over one segment: partial rows out[0 .. batch_segment_rows) x npts.
 // The points with kind BP_PCG must come first in d_pts.
 cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const PointTable* d_T0, const PointTable& T0,
                                  const BatchGroupMap& gm, const BatchPoint* d_pts, int npts, Partial* out,
-                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st);
+                                 int32_t* defer, int* defer_count, int sm_count, cudaStream_t st,
+                                 int waves = 1);
 
 // Reduces rows x npts partials (row-major) into npts results.
 cudaError_t launch_finalize_points(const Partial* parts, int rows, int npts, double sum_w_mc, double sum_w_data,

@@ -18,7 +18,7 @@ LIB_PATH = Path(os.environ.get("PWA_B200_LIB", str(Path(__file__).resolve().pare
 EXPORTED = ["pwa_ctx_create", "pwa_ctx_destroy", "pwa_ctx_upload_events", "pwa_ctx_upload_events_unsorted", "pwa_band_order", "pwa_ctx_set_device_events",
             "pwa_ctx_upload_zcs_events", "pwa_ctx_set_device_zcs_events", "pwa_ctx_set_smearing", "pwa_ctx_select_data",
             "pwa_ctx_eval_nll", "pwa_ctx_eval_nll_batch", "pwa_ctx_last_batch_ms", "pwa_ctx_batch_segment_ms", "pwa_ctx_amp2", "pwa_ctx_mc_integral", "pwa_ctx_last_kernel_ms", "pwa_ctx_last_launches", "pwa_ctx_stream",
-            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_set_event_order", "pwa_ctx_set_kmatrix", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
+            "pwa_ctx_set_timing", "pwa_ctx_set_lineshape_tables", "pwa_ctx_set_event_order", "pwa_ctx_set_kmatrix", "pwa_ctx_set_batch_waves", "pwa_ctx_segment_count", "pwa_ctx_segment_info", "pwa_ctx_segment_deferred", "pwa_point_table_bytes",
             "pwa_host_lineshapes", "pwa_host_lineshapes_km", "pwa_lineshapes_lstar_km", "pwa_generate_events", "pwa_events_from_unit",
             "pwa_unit_flat", "pwa_flow_create", "pwa_flow_destroy", "pwa_flow_param_count", "pwa_flow_get_params",
             "pwa_flow_set_params", "pwa_flow_train_step", "pwa_flow_gradients", "pwa_flow_log_density",
@@ -263,6 +263,10 @@ class Context:
         check(self.L.pwa_ctx_amp2(self.h, _f(pl), block.para_size, block.vamp_size, block.spline_size, block.NR,
                                   block.NZ, block.NX, block.ffr, block.ffb, out.ctypes.data_as(_dp)), "pwa_ctx_amp2")
         return out
+
+    def set_batch_waves(self, kind: int, waves: int):
+        """Waves of resident blocks for the batched passes over event class `kind`."""
+        check(self.L.pwa_ctx_set_batch_waves(self.h, int(kind), int(waves)), "pwa_ctx_set_batch_waves")
 
     def set_kmatrix(self, isospin: bool):
         """Coupled-channel K-matrix: the 7-channel isospin split (True) or the 4-channel default."""

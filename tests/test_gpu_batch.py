@@ -123,3 +123,33 @@ def test_mass_ordered_event_lists(ctx):
         assert abs(ctx.eval_nll(blk).nll - ref[0].nll) < NLL_TOL
     finally:
         ctx.set_event_order(False)
+
+
+def test_batch_waves_and_tuner(ctx, tmp_path):
+    """Wider grids (more waves of blocks per event class) only change the order of the sums; the batch
+    tuner picks one per class, caches it, and a second call takes the cache."""
+    from pwa_b200 import autotune, gradient
+    mdl, vals, blk, smp = make_test_sample("small_kmatrix", 1500, 15000)
+    ctx.upload(smp)
+    labels, blocks = gradient.gradient_blocks(mdl, vals)
+    kinds = sorted({k for k, _, _ in ctx.segments()})
+    ref, _ = ctx.eval_nll_batch(blocks)
+    for w in (2, 4, 16):
+        for k in kinds:
+            ctx.set_batch_waves(k, w)
+        res, _ = ctx.eval_nll_batch(blocks)
+        diff = np.array([r.nll - o.nll for r, o in zip(res, ref)])
+        assert np.max(np.abs(diff)) < NLL_TOL, (w, np.max(np.abs(diff)))
+    with pytest.raises(Exception):
+        ctx.set_batch_waves(kinds[0], 0)
+    cache = tmp_path / "tune.json"
+    first = autotune.tune_batch(ctx, blocks, cache=cache, reps=1)
+    assert not first["cached"] and set(first["waves"]) == {str(k) for k in kinds}
+    assert all(int(w) in autotune.BATCH_WAVES for w in first["waves"].values())
+    second = autotune.tune_batch(ctx, blocks, cache=cache)
+    assert second["cached"] and second["waves"] == first["waves"]
+    res, _ = ctx.eval_nll_batch(blocks)
+    assert max(abs(r.nll - o.nll) for r, o in zip(res, ref)) < NLL_TOL
+    ctx.set_timing(False)
+    for k in kinds:
+        ctx.set_batch_waves(k, 1)
