@@ -76,6 +76,8 @@ def parse():
                     help="walk each MC event class by event index or by m(J/psi p) (pwa_ctx_set_event_order)")
     ap.add_argument("--profile-case", choices=["flow_small", "ensemble_small"],
                     help="run one small case of a kernel for a profiler capture (no bench line)")
+    ap.add_argument("--ens-shape", help="ensemble_small profile case: launch shape 'warps,tile_events' "
+                                         "instead of the autotuned one")
     ap.add_argument("--no-full-parity", action="store_true",
                     help="skip the FP64 oracle check of the whole sample (centre and one point per batch kind)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kmatrix",
@@ -456,11 +458,12 @@ def ensemble_bench(device: int, hbm: float) -> dict:
 
 
 # ------------------------------------------------------------------------------ profiler cases
-def profile_case(name: str, device: int = 0) -> int:
+def profile_case(name: str, device: int = 0, ens_shape: str | None = None) -> int:
     """Small runs of one kernel family for ncu captures (inputs above L2, a few GB on the device at
     most): flow_small = 12 training steps of the proposal network on 16,384-event batches (k_gemm);
     ensemble_small = an 8-toy ensemble of the full BW model (8 x 40k data events, 100k MC) and three
-    ensemble steps (k_ens_data)."""
+    ensemble steps (k_ens_data), at the launch shape `ens_shape` ("warps,tile_events") or the autotuned
+    one."""
     import torch
     from pwa_b200 import configs, ensemble, flow, lib, model as M, toys
     if name == "flow_small":
@@ -478,7 +481,10 @@ def profile_case(name: str, device: int = 0) -> int:
         ctx.bind_device(ens.sample)
         ctx.set_smearing("gauss", 0.0027, 0.0005, 17)
         E = ensemble.Ensemble(ctx, ens, mdl, vals, ensemble.coupling_names(mdl))
-        ensemble.autotune(E)  # the launch shape the bench uses for this device and ensemble shape
+        if ens_shape:
+            E.set_launch(*(int(v) for v in ens_shape.split(",")))
+        else:
+            ensemble.autotune(E)  # the launch shape the bench uses for this device and ensemble shape
         S = np.repeat(E.s0[None, :], E.n_toys, axis=0)
         for _ in range(3):
             E.eval_slots(S)
@@ -493,7 +499,7 @@ def profile_case(name: str, device: int = 0) -> int:
 def main():
     args = parse()
     if args.profile_case:
-        return profile_case(args.profile_case)
+        return profile_case(args.profile_case, ens_shape=args.ens_shape)
     if args.impl == "reference":
         return reference_arm(args)
     import torch

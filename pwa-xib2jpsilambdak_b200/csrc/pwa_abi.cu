@@ -699,7 +699,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
   }
   while (tables && (int)c->bt_tabs.size() < std::min(ntab, BATCH_MAX_TABLES)) {
     void* t = nullptr;
-    PWA_CUDA(cudaMalloc(&t, TAB_BYTES));
+    PWA_CUDA(cudaMalloc(&t, TAB_BYTES_GROUP));
     c->bt_tabs.push_back(t);
   }
   int launches = 0, rc = 0;
@@ -727,7 +727,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     for (int j = 0; j < nc; ++j) {
       const int p = sidx[c0 + j];
       dt[j] = H[p];  // keeps the point's own guard intervals; tables stay off unless attached here
-      if (bp[p].kind == BP_PCG && tables) attach_tables(&dt[j], c->bt_tabs[tab_slot++]);
+      if (bp[p].kind == BP_PCG && tables) attach_group_table(&dt[j], bp[p].group, c->bt_tabs[tab_slot++]);
       dp[j] = bp[p];
       dp[j].T = c->d_btables + j;
       dp[j].dc = c->d_bdc + (size_t)j * 8 * 24;
@@ -740,7 +740,7 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
     PWA_CUDA(cudaMemcpyAsync(c->d_bdc, dcc.data(), dcc.size() * sizeof(cplx), cudaMemcpyHostToDevice, c->st));
     for (int j = 0; j < nc; ++j)
       if (dt[j].tab.enabled) {
-        PWA_CUDA(launch_build_tables(c->d_btables + j, TAB_NODES, c->sm_count, c->st));
+        PWA_CUDA(launch_build_tables(c->d_btables + j, dt[j].tab.n_nodes, c->sm_count, c->st));
         launches += 4;
       }
     // partial rows of all segments

@@ -12,8 +12,6 @@ namespace pwa {
 // Resolution offsets in units of the mass resolution (reference data, Resonances.h:31-54).
 #include "smear_tables.inc"
 
-constexpr int MAX_GROUP_ENTRIES = 8;
-
 __device__ __forceinline__ double ldf(const float* p, int64_t i) { return (double)__ldg(p + i); }
 
 // ------------------------------------------------------------------------------- lineshapes
@@ -389,8 +387,8 @@ __device__ __forceinline__ cplx tab_get(const TabAt& a, int stride, int pos) {
   return acc;
 }
 
-// All Pc entry lineshapes at mass m into out[order position] from the table; false (and zeros) when
-// the table cannot serve m.
+// All Pc entry lineshapes at mass m into out[order position] from a table of every group; false
+// (and zeros) when the table cannot serve m.
 __device__ __forceinline__ bool lookup_table(const PointTable& T, double m, cplx* out) {
   TabAt ta;
   const bool ok = tab_at(T.tab, m, ta);

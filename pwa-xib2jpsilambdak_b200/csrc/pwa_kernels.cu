@@ -366,7 +366,7 @@ __global__ void k_build_tables(const PointTable* __restrict__ T, int n_nodes) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_nodes; j += gridDim.x * blockDim.x) {
     cplx* dst = const_cast<cplx*>(T->tab.data) + (size_t)j * T->tab.stride;
     const PcKin kin = pc_kin(*T, T->tab.m_lo + j * T->tab.h);
-    for (int g = 0; g < T->ngroups; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first);
+    for (int g = T->tab.g_lo; g < T->tab.g_hi; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first - T->tab.pos0);
   }
 }
 
@@ -380,14 +380,14 @@ __device__ bool interval_ok(const PointTable& T, const cplx* base, int stride, d
     double w[6];
     lagrange6(ts[pt], w);
     const PcKin kin = pc_kin(T, m0 + ts[pt] * step);
-    for (int g = 0; g < T.ngroups; ++g) {
+    for (int g = T.tab.g_lo; g < T.tab.g_hi; ++g) {
       const PcGroup& gr = T.grp[g];
       cplx ex[MAX_PC];
       pc_group_exact(T, g, kin, ex);
       double emax = 0, vmax = 0;
       for (int q = 0; q < gr.count; ++q) {
         cplx acc = mk(0, 0);
-        for (int n = 0; n < 6; ++n) acc += base[n * stride + gr.first + q] * w[n];
+        for (int n = 0; n < 6; ++n) acc += base[n * stride + gr.first - T.tab.pos0 + q] * w[n];
         // written so that a non-finite node or exact value propagates (fmax would drop a NaN)
         const double e = sqrt(norm2(acc - ex[q])), v = sqrt(norm2(ex[q]));
         if (!(e <= emax)) emax = e;
@@ -446,7 +446,7 @@ __global__ void k_build_sub(const PointTable* __restrict__ T) {
     const double m = tab.m_lo + tab.block_interval[b] * tab.h + (s - 2) * hs;
     cplx* dst = const_cast<cplx*>(tab.sub) + ((size_t)b * TAB_SUB_NODES + s) * tab.stride;
     const PcKin kin = pc_kin(*T, m);
-    for (int g = 0; g < T->ngroups; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first);
+    for (int g = tab.g_lo; g < tab.g_hi; ++g) pc_group_exact(*T, g, kin, dst + T->grp[g].first - tab.pos0);
   }
 }
 
@@ -488,6 +488,26 @@ void attach_tables(PointTable* T, void* d_mem) {
   tb.block_interval = tb.nblocks + 1;
   tb.stride = T->NZ > 0 ? T->NZ : 1;
   tb.enabled = (T->NZ > 0 && d_mem) ? 1 : 0;
+}
+
+void attach_group_table(PointTable* T, int g, void* d_mem) {
+  LineTables& tb = T->tab;
+  unsigned char* p = static_cast<unsigned char*>(d_mem);
+  tb.data = reinterpret_cast<const cplx*>(p);
+  p += TAB_BYTES_GROUP_DATA;
+  tb.cell = reinterpret_cast<const int*>(p);
+  p += TAB_BYTES_CELL;
+  tb.sub = reinterpret_cast<const cplx*>(p);
+  p += TAB_BYTES_GROUP_SUB;
+  tb.sub_bad = p;
+  p += TAB_BYTES_SUB_BAD;
+  tb.nblocks = reinterpret_cast<int*>(p);
+  tb.block_interval = tb.nblocks + 1;
+  tb.g_lo = g;
+  tb.g_hi = g + 1;
+  tb.pos0 = T->grp[g].first;
+  tb.stride = T->grp[g].count;
+  tb.enabled = (g >= 0 && g < T->ngroups && d_mem) ? 1 : 0;
 }
 
 // ------------------------------------------------------------------------------- finalize
@@ -1201,6 +1221,9 @@ int build_point_table(const float* pl, int para_size, int vamp_size, int spline_
   tb.m_lo = TAB_M_LO;
   tb.h = TAB_H;
   tb.inv_h = 1.0 / TAB_H;
+  tb.g_lo = 0;
+  tb.g_hi = ng;
+  tb.pos0 = 0;
   tb.nguard = 0;
   auto guard = [&](double m, double half) {
     if (tb.nguard < MAX_GUARDS && m > TAB_M_LO - 1e-3 && m < TAB_M_HI + 1e-3) {

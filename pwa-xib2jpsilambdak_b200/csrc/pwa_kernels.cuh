@@ -111,6 +111,11 @@ cudaError_t launch_build_tables(const PointTable* d_table, int n_nodes, int sm_c
 // table: enables interpolation of the Pc lineshapes.
 void attach_tables(PointTable* T, void* d_mem);
 
+// Attaches TAB_BYTES_GROUP of device memory to a host point table for a table of Pc group g alone
+// (the grid of attach_tables, stride = the group's entry count): the table of a batch point that
+// moves only that group's lineshape.
+void attach_group_table(PointTable* T, int g, void* d_mem);
+
 // Reduces nparts partials and assembles the NLL.
 cudaError_t launch_finalize(const Partial* parts, int nparts, double sum_w_mc, double sum_w_data,
                             double nll_shift, EvalResult* res, cudaStream_t st);

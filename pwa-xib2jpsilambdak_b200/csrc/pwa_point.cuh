@@ -116,6 +116,8 @@ struct PcGroup {
 // flagged and refined.  Lookups that neither level can serve, and those near the grid ends, evaluate
 // the lineshapes exactly.
 constexpr int MAX_GUARDS = 48;
+// Entries of one Pc group (a K-matrix J^P group shares one solve).
+constexpr int MAX_GROUP_ENTRIES = 8;
 // Intervals that fail the check are refined: each gets a block of TAB_SUB sub-intervals (step
 // h / TAB_SUB) with TAB_SUB + 5 nodes (the 6-point stencils of all sub-intervals), verified the same
 // way.  Up to TAB_MAX_BLOCKS intervals are refined per point; the others and sub-intervals that fail
@@ -125,7 +127,11 @@ constexpr int TAB_SUB_NODES = TAB_SUB + 5;
 constexpr int TAB_MAX_BLOCKS = 4096;
 struct LineTables {
   int enabled;
-  int n_nodes, stride;  // stride: complex values per node (= NZ, entries in group order)
+  int n_nodes, stride;  // stride: complex values per node (entries in group order)
+  // The table holds groups [g_lo, g_hi), whose entries start at order position pos0: every group
+  // for a context's table (stride NZ), one group for a batch point that moves only that group's
+  // lineshape (stride = its entry count, on the coarser group grid below).
+  int g_lo, g_hi, pos0;
   double m_lo, h, inv_h;
   int nguard;
   double guard_lo[MAX_GUARDS], guard_hi[MAX_GUARDS];
@@ -148,6 +154,12 @@ constexpr size_t TAB_BYTES_SUB_BAD = tab_align((size_t)TAB_MAX_BLOCKS * TAB_SUB)
 constexpr size_t TAB_BYTES_BLOCKS = tab_align((size_t)(TAB_MAX_BLOCKS + 1) * 4);
 constexpr size_t TAB_BYTES =
     TAB_BYTES_DATA + TAB_BYTES_CELL + TAB_BYTES_SUB + TAB_BYTES_SUB_BAD + TAB_BYTES_BLOCKS;
+// A table of one Pc group (a batch point that moves only that group's lineshape): the same grid,
+// stride = the group's entry count.
+constexpr size_t TAB_BYTES_GROUP_DATA = tab_align((size_t)TAB_NODES * MAX_GROUP_ENTRIES * 16);
+constexpr size_t TAB_BYTES_GROUP_SUB = tab_align((size_t)TAB_MAX_BLOCKS * TAB_SUB_NODES * MAX_GROUP_ENTRIES * 16);
+constexpr size_t TAB_BYTES_GROUP = TAB_BYTES_GROUP_DATA + TAB_BYTES_CELL + TAB_BYTES_GROUP_SUB +
+                                   TAB_BYTES_SUB_BAD + TAB_BYTES_BLOCKS;
 
 // Plane slots of one event staged in shared memory (as doubles): pp 111, pp1 96, pp2 96, pp3 97, pp4 96.
 constexpr int SLOT_PP = 0, SLOT_PP1 = 111, SLOT_PP2 = 207, SLOT_PP3 = 303, SLOT_PP4 = 400, SLOT_ALL = 496;
