@@ -44,11 +44,11 @@ CPU_FRAC = 10  # the bounded CPU sample: 1/CPU_FRAC of the bench sample's data a
 # ncu captures of the 50k data + 500k MC case (DRAM read + write of the table-only and the
 # exact-capable pass of the window segment); the traffic of a launch scales with its events.
 DRAM_BYTES_PER_EVENT = {1: 3120.0}
-BATCH_DRAM_BYTES_PER_EVENT = {1: 210900.0}
+BATCH_DRAM_BYTES_PER_EVENT = {1: 38200.0}
 # The resource that binds the FP64 kernels: FP64 pipe utilisation of the dominant kernel (ncu,
 # sm__pipe_fp64_cycles_active as % of peak, small case of the same kernel), with its summary file.
 FP64_PIPE = {("plain", 1): (0.186, "profiles/k_smeared20_kmatrix_50k_500k.md"),
-             ("batch", 1): (0.126, "profiles/k_batch20_kmatrix_50k_500k.md")}
+             ("batch", 1): (0.112, "profiles/k_batch20_kmatrix_50k_500k.md")}
 
 
 def fp64_pipe(kind: str, seg: int):
