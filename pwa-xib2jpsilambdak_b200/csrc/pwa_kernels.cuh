@@ -135,7 +135,7 @@ struct BatchPoint {
   int ldc;                 // BP_LSTAR: 1 when dc holds the coupling differences of the lcmask resonances
                            // (in r order, 12 used of each 24), 0 when more than 8 changed
   int group;               // BP_PCG: Pc group whose lineshapes changed
-  int nq;                  // BP_PCC: Pc entries whose couplings changed (at most 8)
+  int nq;                  // BP_PCC: Pc entries whose couplings changed (at most BATCH_MAXQ_PC = 4)
   int qpos[8], qsidx[8];   // their order positions and d-function spin indices
   const cplx* dc;          // BP_PCC: coupling differences point - centre, [nq][24] (device)
   const PointTable* T;     // device copy of the point's table (BP_LSTAR, BP_PCG)

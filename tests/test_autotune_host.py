@@ -46,14 +46,15 @@ def fake_device(monkeypatch):
 
 
 def test_picks_fastest_per_class_and_caches(tmp_path):
-    cost = {0: {1: 2.0, 2: 1.0, 4: 3.0}, 1: {1: 1.0, 2: 1.5, 4: 0.9}, 4: {1: 0.5, 2: 0.6, 4: 0.7}}
+    cost = {0: {1: 2.0, 2: 1.0, 4: 3.0, 8: 3.5}, 1: {1: 1.0, 2: 1.5, 4: 0.9, 8: 1.2},
+            4: {1: 0.5, 2: 0.6, 4: 0.7, 8: 0.8}}
     ctx = FakeCtx(cost)
     cache = tmp_path / "t.json"
     out = autotune.tune_batch(ctx, [FakeBlock()] * 5, cache=cache, reps=2)
     # kind 1 has two segments: their times add up (2 x 0.9 at 4 waves beats 2 x 1.0 at 1)
     assert out["waves"] == {"0": 2, "1": 4, "4": 1}
     assert ctx.waves == {0: 2, 1: 4, 4: 1}
-    assert ctx.calls == 3 * 3  # one warm-up and two timed calls per candidate
+    assert ctx.calls == 3 * len(autotune.BATCH_WAVES)  # one warm-up and two timed calls per candidate
     table = json.loads(cache.read_text())
     (key,) = table
     assert "FakeGPU" in key and "NR=3" in key and "points=5" in key
@@ -61,13 +62,13 @@ def test_picks_fastest_per_class_and_caches(tmp_path):
     again = autotune.tune_batch(ctx2, [FakeBlock()] * 5, cache=cache)
     assert again["cached"] and ctx2.calls == 0 and ctx2.waves == {0: 2, 1: 4, 4: 1}
     forced = autotune.tune_batch(ctx2, [FakeBlock()] * 5, cache=cache, force=True, reps=1)
-    assert not forced["cached"] and ctx2.calls == 3 * 2
+    assert not forced["cached"] and ctx2.calls == 2 * len(autotune.BATCH_WAVES)
 
 
 def test_unreadable_cache_is_ignored(tmp_path):
     cache = tmp_path / "t.json"
     cache.write_text("{not json")
-    cost = {k: {1: 1.0, 2: 2.0, 4: 3.0} for k in (0, 1, 4)}
+    cost = {k: {1: 1.0, 2: 2.0, 4: 3.0, 8: 4.0} for k in (0, 1, 4)}
     out = autotune.tune_batch(FakeCtx(cost), [FakeBlock()], cache=cache, reps=1)
     assert out["waves"] == {"0": 1, "1": 1, "4": 1} and not out["cached"]
     assert json.loads(cache.read_text())
