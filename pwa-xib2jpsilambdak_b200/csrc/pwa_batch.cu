@@ -492,7 +492,8 @@ static int batch_grid(const Segment& s, const PointTable& T0, const BatchGroupMa
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_un<false, false>, BU_THREADS, smem);
   } else {
     b = (n + BATCH_WARPS - 1) / BATCH_WARPS;
-    const size_t smem = batch_layout(T0.NR, T0.NZ, npts, batch_moments(batch_nb(s.kind))).total;
+    const int nb = batch_nb(s.kind);
+    const size_t smem = batch_layout(T0.NR, T0.NZ, npts, batch_moments(nb), batch_row_cap(nb)).total;
     switch (batch_nb(s.kind)) {
       case 20: occ = batch_occupancy_20(smem); break;
       case 30: occ = batch_occupancy_30(smem); break;
@@ -550,7 +551,7 @@ cudaError_t launch_batch_segment(const EventSet& ev, const Segment& seg, const P
   if (nb < 0 && (!seg.grid || seg.grid_nb < 1 || seg.grid_nb > GRID_MAX_NB)) return cudaErrorInvalidValue;
   const int band = (seg.kind == SMEAR_30 || seg.kind == SMEAR_150) ? 1 : 0;
   const size_t smem = nb == 0 ? batch_un_layout(T0.NR, T0.NZ, T0.NX, gm.max_slots, npts).total
-                              : batch_layout(T0.NR, T0.NZ, npts, batch_moments(nb)).total;
+                              : batch_layout(T0.NR, T0.NZ, npts, batch_moments(nb), batch_row_cap(nb)).total;
   const int grid = batch_grid(seg, T0, gm, npts, sm_count, waves);
   if (defer) {
     launch_batch_nb(nb, ev, seg.begin, seg.end, seg.list, nullptr, d_T0, gm, d_pts, npts, out, band, defer,

@@ -27,8 +27,11 @@ __host__ __device__ inline size_t bal16(size_t x) { return (x + 15) & ~size_t(15
 // the row loops measured faster, and without the moment buffers the blocks leave more of the unified
 // L1 to the table lookups.
 __host__ __device__ constexpr bool batch_moments(int nb) { return nb > 0 && nb + 1 <= 32; }
+// Offset rows a round holds: the lookups of one event (with the row at the event mass) for 20 and 30
+// offsets, a full round of 32 otherwise.
+__host__ __device__ constexpr int batch_row_cap(int nb) { return nb > 0 && nb + 1 <= 32 ? nb + 1 : 32; }
 
-__host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts, bool moments) {
+__host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts, bool moments, int row_cap) {
   BatchLayout L;
   L.nzp = (NZ + 3) & ~3;
   L.rs = L.nzp + 1;
@@ -52,9 +55,9 @@ __host__ __device__ inline BatchLayout batch_layout(int NR, int NZ, int npts, bo
   L.hz = o;
   o = bal16(o + (size_t)(L.nzp > 0 ? L.nzp : 1) * 8 * sizeof(cplx));
   L.R = o;
-  o = bal16(o + (size_t)32 * L.rs * sizeof(cplx));
+  o = bal16(o + (size_t)row_cap * L.rs * sizeof(cplx));
   L.S0 = o;
-  o = bal16(o + (size_t)32 * 9 * sizeof(cplx));
+  o = bal16(o + (size_t)row_cap * 9 * sizeof(cplx));
   // moments of the centre's offset rows (coupling points): G triangle, P [q][h], R1, Y, row 0
   const size_t nq = moments ? (size_t)(L.nzp > 0 ? L.nzp : 1) : 0;
   L.G = o;
@@ -184,7 +187,8 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   const PointTable& T0 = *T0p;
   const int NR = T0.NR, NZ = T0.NZ;
   constexpr bool has_x = ZCS;  // Zcs entries (their amplitudes join the centre's H_L)
-  const BatchLayout Ly = batch_layout(NR, NZ, npts, batch_moments(NB));
+  constexpr int RC = batch_row_cap(NB);  // rows held per round
+  const BatchLayout Ly = batch_layout(NR, NZ, npts, batch_moments(NB), RC);
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
   unsigned char* wb = sm + warp * Ly.warp_bytes;
   double* bs = reinterpret_cast<double*>(wb + Ly.bs);
@@ -296,23 +300,27 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     // one round of centre rows: R[b][q] at lookup l0 + b, S0[b][h]; the centre's smeared sums
     auto centre_round = [&](int l0, bool sums) {
       const int l = l0 + lane;
-      cplx* row = R + lane * rs;
-      if (l < nlook) {
-        const double m = row_mass(l, mz, mres);
-        if (FIX)
-          lookup_entries(T0, m, row);
-        else
-          fail |= !lookup_table(T0, m, row);
-      } else {
-        for (int q = 0; q < NZ; ++q) row[q] = mk(0, 0);
+      cplx* row = R + lane * rs;  // rows past RC are past nlook too and are never read
+      if (lane < RC) {
+        if (l < nlook) {
+          const double m = row_mass(l, mz, mres);
+          if (FIX)
+            lookup_entries(T0, m, row);
+          else
+            fail |= !lookup_table(T0, m, row);
+        } else {
+          for (int q = 0; q < NZ; ++q) row[q] = mk(0, 0);
+        }
+        for (int q = NZ; q < nzp; ++q) row[q] = mk(0, 0);
       }
-      for (int q = NZ; q < nzp; ++q) row[q] = mk(0, 0);
       __syncwarp();
+      if (lane < RC) {
 #pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        cplx s = mk(0, 0);
-        for (int q = 0; q < NZ; ++q) cmac(s, row[q], hz[q * 8 + h]);
-        S0[lane * 9 + h] = s;
+        for (int h = 0; h < 8; ++h) {
+          cplx s = mk(0, 0);
+          for (int q = 0; q < NZ; ++q) cmac(s, row[q], hz[q * 8 + h]);
+          S0[lane * 9 + h] = s;
+        }
       }
       __syncwarp();
       if (sums) {

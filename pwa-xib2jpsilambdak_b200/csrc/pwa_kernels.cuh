@@ -157,7 +157,7 @@ BatchGroupMap batch_group_map(const PointTable& T0);
 bool classify_point(const PointTable& T0, const PointTable& Tp, BatchPoint* bp, cplx* dc_host);
 
 // Largest number of points one batched launch takes (shared memory holds per-point sums).
-constexpr int BATCH_MAX_POINTS = 384;
+constexpr int BATCH_MAX_POINTS = 512;
 
 // Partial rows a segment of a batched evaluation writes (its pass, plus the deferred pass when
 // deferred is true); each row holds npts partials.
