@@ -334,7 +334,7 @@ def proposal_bench(device: int, bf16_peak: float) -> dict:
     exp_q = 1.05 * float(wq.max()) / float(wq.mean())
     exp_f = 1.05 * float(a2f.max()) / float(a2f.mean())
     q999 = float(torch.quantile(wq[:1 << 24].float(), 0.999)) / float(wq.mean())
-    # weighted toys (every candidate kept with weight |A|^2 flat / q, the exact amplitude as judge): the
+    # weighted toys (every candidate kept with weight |A|^2 flat / q, the exact amplitude deciding): the
     # amplitude evaluations per effective event, n / ESS = mean(w^2) / mean(w)^2, against the
     # evaluations per accepted event of flat hit-or-miss at the same statistical power
     per_eff_q = float((wq ** 2).mean()) / float(wq.mean()) ** 2

@@ -21,7 +21,7 @@ FP32 accumulation.
 
 Used (i) for toys: candidates drawn from q, each weighted by |A|^2 flat / q and accepted against the
 largest weight (hit-or-miss on the weights), and (ii) for normalisation integrals: the mean of
-|A|^2 flat / q over q-samples.  The exact amplitude judges every event, so neither use is biased;
+|A|^2 flat / q over q-samples.  The exact amplitude decides every event, so neither use is biased;
 flat phase space stays available (`flat_unit`).  No counterpart in the reference, whose toys are flat
 hit-or-miss (gen_toys/create_efficiency/hit_and_reject.py:40-50).
 """
