@@ -732,6 +732,23 @@ int pwa_ctx_eval_nll_batch(pwa_ctx* c, const float* pls, int npoints, int block_
       dp[j].T = c->d_btables + j;
       dp[j].dc = c->d_bdc + (size_t)j * 8 * 24;
     }
+    // neighbouring points that move the same couplings (Minuit's +h and -h of one coupling) are paired
+    auto same_couplings = [](const BatchPoint& x, const BatchPoint& y) {
+      if (x.kind != y.kind) return false;
+      if (x.kind == BP_LSTAR)
+        return x.lsmask == 0 && y.lsmask == 0 && x.ldc && y.ldc && x.lmask == y.lmask && x.lcmask == x.lmask &&
+               y.lcmask == y.lmask;
+      if (x.kind == BP_PCC)
+        return x.nq == y.nq && std::memcmp(x.qpos, y.qpos, sizeof(int) * x.nq) == 0 &&
+               std::memcmp(x.qsidx, y.qsidx, sizeof(int) * x.nq) == 0;
+      return false;
+    };
+    for (int j = 0; j < nc;) {
+      const bool pr = j + 1 < nc && same_couplings(dp[j], dp[j + 1]);
+      dp[j].pair = pr ? 1 : 0;
+      if (pr) dp[j + 1].pair = 0;
+      j += pr ? 2 : 1;
+    }
     PWA_CUDA(cudaMemcpyAsync(c->d_btables, dt.data(), nc * sizeof(PointTable), cudaMemcpyHostToDevice, c->st));
     PWA_CUDA(cudaMemcpyAsync(c->d_bpts, dp.data(), nc * sizeof(BatchPoint), cudaMemcpyHostToDevice, c->st));
     std::vector<cplx> dcc((size_t)nc * 8 * 24);

@@ -104,6 +104,47 @@ __device__ __forceinline__ void pc_acc(const cplx* c, int sx, const Ev& E, cplx 
   }
 }
 
+// Two points that move the same Lambda* couplings (differences ca, cb) from one pass over the planes:
+// outa / outb as lstar_acc with ca / cb.
+__device__ __forceinline__ void lstar_acc2(const cplx* ca, const cplx* cb, int sx, const Ev& E, cplx q, cplx* outa,
+                                           cplx* outb) {
+#pragma unroll 3
+  for (int m = 0; m < 6; ++m) {
+    const cplx a0 = ca[m], a1 = ca[6 + m], b0 = cb[m], b1 = cb[6 + m];
+    if (!nonzero(a0) && !nonzero(a1) && !nonzero(b0) && !nonzero(b1)) continue;
+    const double dl0 = E.DL(sx, 0, m), dl1 = E.DL(sx, 1, m);
+    const cplx wa0 = (q * a0) * dl0, wa1 = (q * a1) * dl1, wb0 = (q * b0) * dl0, wb1 = (q * b1) * dl1;
+#pragma unroll
+    for (int ij = 0; ij < 4; ++ij) {
+      const cplx a = E.A(ij >> 1, ij & 1, m);
+      cmac(outa[2 * ij], a, wa0);
+      cmac(outa[2 * ij + 1], a, wa1);
+      cmac(outb[2 * ij], a, wb0);
+      cmac(outb[2 * ij + 1], a, wb1);
+    }
+  }
+}
+
+// Two points that move the same Pc entry's couplings: outa / outb as pc_acc with ca / cb.
+__device__ __forceinline__ void pc_acc2(const cplx* ca, const cplx* cb, int sx, const Ev& E, cplx q, cplx* outa,
+                                        cplx* outb) {
+#pragma unroll 4
+  for (int m = 0; m < 12; ++m) {
+    const cplx a0 = ca[m], a1 = ca[12 + m], b0 = cb[m], b1 = cb[12 + m];
+    if (!nonzero(a0) && !nonzero(a1) && !nonzero(b0) && !nonzero(b1)) continue;
+    const double dz0 = E.DZ(sx, 0, m), dz1 = E.DZ(sx, 1, m);
+    const cplx wa0 = (q * a0) * dz0, wa1 = (q * a1) * dz1, wb0 = (q * b0) * dz0, wb1 = (q * b1) * dz1;
+#pragma unroll
+    for (int ij = 0; ij < 4; ++ij) {
+      const cplx a = E.AZ(ij >> 1, ij & 1, m);
+      cmac(outa[2 * ij], a, wa0);
+      cmac(outa[2 * ij + 1], a, wa1);
+      cmac(outb[2 * ij], a, wb0);
+      cmac(outb[2 * ij + 1], a, wb1);
+    }
+  }
+}
+
 // ZCS: the model has Zcs entries (instantiated apart so that the common kernel stays as it was)
 template <bool FIX, bool ZCS>
 __global__ void __launch_bounds__(BU_THREADS)
@@ -205,12 +246,74 @@ __global__ void __launch_bounds__(BU_THREADS)
     const double swe = (live && is_data) ? (double)__ldg(ev.sw + E.e) : 0.0;
     int cur_group = -1;
     __syncwarp();
+    // |A|^2 of point pi from its amplitude change d (to H_L for Lambda* points, to H_Z otherwise), and
+    // the warp's sums of it into the block's per-point sums
+    auto finish = [&](int pi, int kind, const cplx(&d)[8]) {
+      const bool to_hl = kind == BP_LSTAR;
+      double v = 0, vn = 0;
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const cplx hl = to_hl ? HL0[h] + d[h] : HL0[h], hz = to_hl ? HZ0[h] : HZ0[h] + d[h];
+        v += norm2(hl + hz);
+        if (has_x) {
+          const cplx hx = hxs[h * 32 + lane];
+          vn += norm2(hl - hx) + norm2(hx) + norm2(hz);
+        } else {
+          vn += norm2(hl) + norm2(hz);
+        }
+      }
+      const double fxe = data_w ? v : v * (double)wf;
+      double a0 = 0, a1 = 0, a2 = 0;
+      bool bad = false;
+      if (live) {
+        bad = !(fxe > 0) || !isfinite(fxe);
+        if (is_data) {
+          a0 = (fxe > 0) ? log(fxe) * swe : -1e12;
+        } else {
+          a1 = fxe;
+          a2 = data_w ? 0.0 : vn * (double)wf;
+        }
+      }
+      a0 = warp_sum(a0);
+      a1 = warp_sum(a1);
+      a2 = warp_sum(a2);
+      const int nbad = __popc(__ballot_sync(0xffffffffu, bad));
+      if (lane == 0) {
+        double* a = acc + pi * 4;
+        atomicAdd(a + 0, a0);
+        atomicAdd(a + 1, a1);
+        atomicAdd(a + 2, a2);
+        if (nbad) atomicAdd(a + 3, (double)nbad);
+      }
+    };
     for (int pi = 0; pi < npts; ++pi) {
       const BatchPoint& bp = pts[pi];
       const int kind = bp.kind;
       cplx d[8];  // change of H_L (Lambda* points) or of H_Z (Pc points)
 #pragma unroll
       for (int h = 0; h < 8; ++h) d[h] = mk(0, 0);
+      if (bp.pair) {
+        // this point and the next move the same couplings: one pass over the planes for both
+        const BatchPoint& bq = pts[pi + 1];
+        cplx d2[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) d2[h] = mk(0, 0);
+        if (kind == BP_LSTAR) {
+          int u = 0;
+          for (int r = 0; r < NR; ++r) {
+            if (!(bp.lmask >> r & 1)) continue;
+            lstar_acc2(bp.dc + 24 * u, bq.dc + 24 * u, T0.L[r].sidx, E, q0s[r * 32 + lane], d, d2);
+            ++u;
+          }
+        } else {
+          for (int u = 0; u < bp.nq; ++u)
+            pc_acc2(bp.dc + u * 24, bq.dc + u * 24, bp.qsidx[u], E, r0s[bp.qpos[u] * 32 + lane], d, d2);
+        }
+        finish(pi, kind, d);
+        finish(pi + 1, kind, d2);
+        ++pi;
+        continue;
+      }
       if (kind == BP_LSTAR) {
         const PointTable& Tp = *bp.T;
         const unsigned lm = bp.lmask, lsm = bp.lsmask, lcm = bp.lcmask;
@@ -278,42 +381,7 @@ __global__ void __launch_bounds__(BU_THREADS)
           for (int h = 0; h < 8; ++h) cmac(d[h], dsl[sl], hzg[(sl * 8 + h) * 32 + lane]);
         }
       }
-      const bool to_hl = kind == BP_LSTAR;
-      double v = 0, vn = 0;
-#pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        const cplx hl = to_hl ? HL0[h] + d[h] : HL0[h], hz = to_hl ? HZ0[h] : HZ0[h] + d[h];
-        v += norm2(hl + hz);
-        if (has_x) {
-          const cplx hx = hxs[h * 32 + lane];
-          vn += norm2(hl - hx) + norm2(hx) + norm2(hz);
-        } else {
-          vn += norm2(hl) + norm2(hz);
-        }
-      }
-      const double fxe = data_w ? v : v * (double)wf;
-      double a0 = 0, a1 = 0, a2 = 0;
-      bool bad = false;
-      if (live) {
-        bad = !(fxe > 0) || !isfinite(fxe);
-        if (is_data) {
-          a0 = (fxe > 0) ? log(fxe) * swe : -1e12;
-        } else {
-          a1 = fxe;
-          a2 = data_w ? 0.0 : vn * (double)wf;
-        }
-      }
-      a0 = warp_sum(a0);
-      a1 = warp_sum(a1);
-      a2 = warp_sum(a2);
-      const int nbad = __popc(__ballot_sync(0xffffffffu, bad));
-      if (lane == 0) {
-        double* a = acc + pi * 4;
-        atomicAdd(a + 0, a0);
-        atomicAdd(a + 1, a1);
-        atomicAdd(a + 2, a2);
-        if (nbad) atomicAdd(a + 3, (double)nbad);
-      }
+      finish(pi, kind, d);
     }
     __syncwarp();
   }

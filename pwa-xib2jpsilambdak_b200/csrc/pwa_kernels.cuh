@@ -139,6 +139,8 @@ struct BatchPoint {
   int qpos[8], qsidx[8];   // their order positions and d-function spin indices
   const cplx* dc;          // BP_PCC: coupling differences point - centre, [nq][24] (device)
   const PointTable* T;     // device copy of the point's table (BP_LSTAR, BP_PCG)
+  int pair;                // 1: the next point moves the same couplings (Lambda* couplings only, or the
+                           // same Pc entries); the unsmeared kernel forms both from one pass over the planes
 };
 
 // Per Pc group of the batch centre: entries with identical couplings (the non-resonant K-matrix
