@@ -21,7 +21,6 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import json
-import os
 from pathlib import Path
 
 import numpy as np
@@ -310,10 +309,8 @@ CANDIDATES = [(16, 256), (16, 1024), (16, 4096), (12, 256), (12, 1024), (8, 256)
 
 
 def _cache_path() -> Path:
-    base = os.environ.get("PWA_B200_TUNE_CACHE")
-    if base:
-        return Path(base)
-    return Path(os.environ.get("XDG_CACHE_HOME", str(Path.home() / ".cache"))) / "pwa_b200" / "ensemble_tune.json"
+    from .autotune import cache_path
+    return cache_path("ensemble_tune.json")
 
 
 def tune_key(ens: Ensemble) -> str:
