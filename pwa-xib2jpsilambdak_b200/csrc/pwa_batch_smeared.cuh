@@ -219,8 +219,8 @@ __global__ void __launch_bounds__(BATCH_THREADS)
   __syncthreads();
   // The lineshape points' table lookups decide whether an event is deferred (FIX = false): the values
   // of the passes up to the last lineshape point wait in vbuf until then, later passes go straight to
-  // the sums, and a deferred event stops there.  A batch whose lineshape points outside the buffer's
-  // reach (not produced by the host) defers every event to the exact pass.
+  // the sums, and a deferred event stops there.  A batch with lineshape points beyond the buffer's
+  // reach (the host never builds one) defers every event to the exact pass.
   const int pcg_end = FIX ? 0 : (s_npcg + 31) & ~31;
   const bool vb_overflow = !FIX && min(pcg_end, npts) > BATCH_VBUF;
 
