@@ -178,7 +178,7 @@ int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
 
 /* Launch shape of the batched evaluation's passes over one event class (the kind pwa_ctx_segment_info
  * reports: 0 unsmeared, 1/2/3 the 20/30/150-offset classes, 4 the weighted grid): grid = min(blocks
- * for its events, waves x SMs x resident blocks per SM), waves 1..16 (default 1).  More waves than
+ * for its events, waves x SMs x resident blocks per SM), waves 1..64 (default 1).  More waves than
  * one balance uneven per-event work at the cost of more block starts; the batch autotuner
  * (pwa_b200.autotune.tune_batch) picks them per class by timing and caches the choice. */
 int pwa_ctx_set_batch_waves(pwa_ctx* ctx, int kind, int waves);

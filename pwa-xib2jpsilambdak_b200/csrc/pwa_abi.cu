@@ -460,7 +460,7 @@ int pwa_ctx_set_smearing(pwa_ctx* c, int mode, double sigma, double step, int ha
 }
 
 int pwa_ctx_set_batch_waves(pwa_ctx* c, int kind, int waves) {
-  if (!c || kind < 0 || kind >= SMEAR_KINDS || waves < 1 || waves > 16) return PWA_E_ARG;
+  if (!c || kind < 0 || kind >= SMEAR_KINDS || waves < 1 || waves > 64) return PWA_E_ARG;
   c->batch_waves[kind] = waves;
   return PWA_OK;
 }

@@ -134,7 +134,7 @@ def test_batch_waves_and_tuner(ctx, tmp_path):
     labels, blocks = gradient.gradient_blocks(mdl, vals)
     kinds = sorted({k for k, _, _ in ctx.segments()})
     ref, _ = ctx.eval_nll_batch(blocks)
-    for w in (2, 4, 16):
+    for w in (2, 4, 64):
         for k in kinds:
             ctx.set_batch_waves(k, w)
         res, _ = ctx.eval_nll_batch(blocks)
