@@ -180,7 +180,8 @@ int pwa_ctx_segment_deferred(pwa_ctx* ctx, int i, int64_t* deferred);
  * reports: 0 unsmeared, 1/2/3 the 20/30/150-offset classes, 4 the weighted grid): grid = min(blocks
  * for its events, waves x SMs x resident blocks per SM), waves 1..64 (default 1).  More waves than
  * one balance uneven per-event work at the cost of more block starts; the batch autotuner
- * (pwa_b200.autotune.tune_batch) picks them per class by timing and caches the choice. */
+ * (pwa_b200.autotune.tune_batch) picks them per class by timing and caches the choice.  No reference
+ * counterpart (the reference launches one fixed shape). */
 int pwa_ctx_set_batch_waves(pwa_ctx* ctx, int kind, int waves);
 
 /* Coupled-channel K-matrix of the context's evaluations.  PWA_KMATRIX_DEFAULT: 4 channels (J/psi p,
