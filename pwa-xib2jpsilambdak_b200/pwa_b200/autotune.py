@@ -15,7 +15,7 @@ from pathlib import Path
 
 import numpy as np
 
-BATCH_WAVES = (1, 2, 4, 8, 16, 32)
+BATCH_WAVES = (1, 2, 4, 8, 16, 32, 64)
 
 
 def cache_path(name: str = "tune.json") -> Path:

@@ -46,9 +46,9 @@ def fake_device(monkeypatch):
 
 
 def test_picks_fastest_per_class_and_caches(tmp_path):
-    cost = {0: {1: 2.0, 2: 1.0, 4: 3.0, 8: 3.5, 16: 3.6, 32: 3.7},
-            1: {1: 1.0, 2: 1.5, 4: 0.9, 8: 1.2, 16: 1.3, 32: 1.4},
-            4: {1: 0.5, 2: 0.6, 4: 0.7, 8: 0.8, 16: 0.9, 32: 1.0}}
+    cost = {0: {1: 2.0, 2: 1.0, 4: 3.0, 8: 3.5, 16: 3.6, 32: 3.7, 64: 3.8},
+            1: {1: 1.0, 2: 1.5, 4: 0.9, 8: 1.2, 16: 1.3, 32: 1.4, 64: 1.5},
+            4: {1: 0.5, 2: 0.6, 4: 0.7, 8: 0.8, 16: 0.9, 32: 1.0, 64: 1.1}}
     ctx = FakeCtx(cost)
     cache = tmp_path / "t.json"
     out = autotune.tune_batch(ctx, [FakeBlock()] * 5, cache=cache, reps=2)
@@ -69,7 +69,7 @@ def test_picks_fastest_per_class_and_caches(tmp_path):
 def test_unreadable_cache_is_ignored(tmp_path):
     cache = tmp_path / "t.json"
     cache.write_text("{not json")
-    cost = {k: {1: 1.0, 2: 2.0, 4: 3.0, 8: 4.0, 16: 5.0, 32: 6.0} for k in (0, 1, 4)}
+    cost = {k: {1: 1.0, 2: 2.0, 4: 3.0, 8: 4.0, 16: 5.0, 32: 6.0, 64: 7.0} for k in (0, 1, 4)}
     out = autotune.tune_batch(FakeCtx(cost), [FakeBlock()], cache=cache, reps=1)
     assert out["waves"] == {"0": 1, "1": 1, "4": 1} and not out["cached"]
     assert json.loads(cache.read_text())
